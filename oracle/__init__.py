@@ -1,0 +1,231 @@
+"""CPU oracle for QUICK's direct-SCF two-electron path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline / reference legs, never by the quick_b200 package.
+
+Two checkers live here:
+  * ``liboracle.so`` (oracle.c): this project's plain-C restatement of the
+    reference's algorithm;
+  * ``libquickref.so`` (build_ref.py): QUICK's own CUDA bridge and kernels
+    (src/cuda/gpu.cu, gpu_get2e.cu, gpu_getxc.cu) compiled as host code and
+    driven through QUICK's own ``gpu_*_`` entry points, in the call order of
+    src/main.f90:81-177 and src/hfoperator.f90:76-104.
+"""
+import contextlib
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(HERE, "_ref")
+
+_P = C.c_void_p
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_P)
+
+
+class _OBasis(C.Structure):
+    _fields_ = [("natom", C.c_int), ("nbasis", C.c_int), ("nshell", C.c_int), ("jbasis", C.c_int),
+                ("xyz", _P), ("kstart", _P), ("katom", _P), ("kprim", _P), ("Ksumtype", _P),
+                ("Qstart", _P), ("Qfinal", _P), ("Qsbasis", _P), ("Qfbasis", _P), ("KLMN", _P),
+                ("gccoeff", _P), ("gcexpo", _P), ("cons", _P)]
+
+
+def build_oracle():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(LIBDIR, "liboracle.so")
+        if not os.path.exists(path):
+            build_oracle()
+        _lib = C.CDLL(path)
+        _lib.oracle_fock.restype = C.c_long
+        _lib.oracle_shell_quartet.restype = C.c_long
+    return _lib
+
+
+class OracleInputs:
+    """Keeps the numpy arrays alive behind the C struct."""
+
+    def __init__(self, basis, xyz_bohr):
+        b = basis
+        self.keep = dict(
+            xyz=np.asfortranarray(xyz_bohr, dtype=np.float64),
+            kstart=np.ascontiguousarray(b.kstart, dtype=np.int32),
+            katom=np.ascontiguousarray(b.katom, dtype=np.int32),
+            kprim=np.ascontiguousarray(b.kprim, dtype=np.int32),
+            Ksumtype=np.ascontiguousarray(b.Ksumtype, dtype=np.int32),
+            Qstart=np.ascontiguousarray(b.Qstart, dtype=np.int32),
+            Qfinal=np.ascontiguousarray(b.Qfinal, dtype=np.int32),
+            Qsbasis=np.asfortranarray(b.Qsbasis, dtype=np.int32),
+            Qfbasis=np.asfortranarray(b.Qfbasis, dtype=np.int32),
+            KLMN=np.asfortranarray(b.KLMN, dtype=np.int32),
+            gccoeff=np.asfortranarray(b.gccoeff),
+            gcexpo=np.asfortranarray(b.gcexpo),
+            cons=np.ascontiguousarray(b.cons))
+        k = self.keep
+        self.s = _OBasis(b.natom, b.nbasis, b.nshell, b.jbasis, *[_ptr(k[n]) for n in (
+            "xyz", "kstart", "katom", "kprim", "Ksumtype", "Qstart", "Qfinal", "Qsbasis",
+            "Qfbasis", "KLMN", "gccoeff", "gcexpo", "cons")])
+        self.basis = basis
+
+
+def boys(mmax, T):
+    F = np.zeros(mmax + 1)
+    lib().oracle_boys(C.c_int(mmax), C.c_double(T), _ptr(F))
+    return F
+
+
+def schwarz(basis, xyz_bohr):
+    """YCutoff (nshell x nshell) and cutPrim (jbasis x jbasis), Fortran order."""
+    inp = OracleInputs(basis, xyz_bohr)
+    Y = np.zeros((basis.nshell, basis.nshell), order="F")
+    cp = np.zeros((basis.jbasis, basis.jbasis), order="F")
+    lib().oracle_schwarz(C.byref(inp.s), _ptr(Y), _ptr(cp))
+    return Y, cp
+
+
+def cutmatrix(basis, dense):
+    cm = np.zeros((basis.nshell, basis.nshell), order="F")
+    inp = OracleInputs(basis, np.zeros((3, basis.natom), order="F"))
+    d = np.asfortranarray(dense)
+    lib().oracle_cutmatrix(C.byref(inp.s), _ptr(d), _ptr(cm))
+    return cm
+
+
+def fock(basis, xyz_bohr, YCutoff, cutPrim, cutMatrix, dense, integral_cutoff, prim_limit,
+         hybrid=1.0, O=None):
+    """O + G(D) as QUICK's get2e returns it; also the quartet counts."""
+    inp = OracleInputs(basis, xyz_bohr)
+    n = basis.nbasis
+    O = np.zeros((n, n), order="F") if O is None else np.array(O, order="F", dtype=np.float64)
+    Y, cp, cm, d = (np.asfortranarray(a, dtype=np.float64) for a in (YCutoff, cutPrim, cutMatrix, dense))
+    npq, nint = C.c_long(0), C.c_long(0)
+    nq = lib().oracle_fock(C.byref(inp.s), _ptr(Y), _ptr(cp), _ptr(cm), _ptr(d),
+                           C.c_double(integral_cutoff), C.c_double(prim_limit), C.c_double(hybrid),
+                           _ptr(O), C.byref(npq), C.byref(nint))
+    return O, dict(quartets=int(nq), prim_quartets=int(npq.value), integrals=int(nint.value))
+
+
+def shell_quartet(basis, xyz_bohr, ii, jj, kk, ll, I, J, K, L):
+    """Contracted (ab|cd) block (0-based shells) without screening."""
+    inp = OracleInputs(basis, xyz_bohr)
+    out = np.zeros(10 ** 4)
+    lib().oracle_shell_quartet(C.byref(inp.s), ii, jj, kk, ll, I, J, K, L, C.c_double(-1.0), None,
+                               C.c_double(0.0), -1, _ptr(out))
+    return out
+
+
+# ------------------------------------------------------------ QUICK itself
+_ref = None
+
+
+def ref_available():
+    return os.path.exists(os.path.join(LIBDIR, "libquickref.so"))
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = C.CDLL(os.path.join(LIBDIR, "libquickref.so"))
+    return _ref
+
+
+@contextlib.contextmanager
+def _quiet():
+    """QUICK's bridge prints every pair it sorts; silence fd 1 meanwhile."""
+    import sys
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        yield
+    finally:
+        C.CDLL(None).fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+
+
+def _i(v):
+    return C.byref(C.c_int(int(v)))
+
+
+def _d(v):
+    return C.byref(C.c_double(float(v)))
+
+
+def ref_upload_molecule(mol, basis, YCutoff, cutPrim, threads=None):
+    """QUICK's start-up upload sequence (src/main.f90:84-177)."""
+    r = ref_lib()
+    if threads:
+        r.qref_set_threads(int(threads))
+    b = basis
+    keep = []
+
+    def arr(a, dt):
+        x = np.asfortranarray(a, dtype=dt)
+        keep.append(x)
+        return _ptr(x)
+
+    with _quiet():
+        r.qref_reset()
+        r.gpu_init_()
+        r.gpu_setup_(_i(mol.natom), _i(b.nbasis), _i(mol.n_electrons), _i(mol.mult), _i(mol.charge),
+                     _i(len(set(mol.symbols))))
+        r.gpu_upload_xyz_(arr(mol.xyz_bohr, np.float64))
+        r.gpu_upload_atom_and_chg_(arr(mol.atomic_numbers, np.int32),
+                                   arr(mol.atomic_numbers.astype(np.float64), np.float64))
+        I32, F64 = np.int32, np.float64
+        r.gpu_upload_basis_(_i(b.nshell), _i(b.nprim), _i(b.jshell), _i(b.jbasis), _i(b.maxcontract),
+                            arr(b.ncontract, I32), arr(b.itype, I32), arr(b.aexp, F64), arr(b.dcoeff, F64),
+                            arr(b.first_basis_function, I32), arr(b.last_basis_function, I32),
+                            arr(b.first_shell_basis_function, I32), arr(b.last_shell_basis_function, I32),
+                            arr(b.ncenter, I32), arr(b.kstart, I32), arr(b.katom, I32), arr(b.ktype, I32),
+                            arr(b.kprim, I32), arr(b.kshell, I32), arr(b.Ksumtype, I32), arr(b.Qnumber, I32),
+                            arr(b.Qstart, I32), arr(b.Qfinal, I32), arr(b.Qsbasis, I32), arr(b.Qfbasis, I32),
+                            arr(b.gccoeff, F64), arr(b.cons, F64), arr(b.gcexpo, F64), arr(b.KLMN, I32))
+        r.gpu_upload_cutoff_matrix_(arr(YCutoff, F64), arr(cutPrim, F64))
+    return keep
+
+
+def ref_pairlist():
+    r = ref_lib()
+    cap = 1 << 24
+    xy = np.zeros(2 * cap, dtype=np.int32)
+    f, ff = C.c_int(0), C.c_int(0)
+    n = r.qref_pairlist(_ptr(xy), cap, C.byref(f), C.byref(ff))
+    q = np.zeros(1 << 20, dtype=np.int32)
+    qn = np.zeros(1 << 20, dtype=np.int32)
+    nq = r.qref_sorted_q(_ptr(q), _ptr(qn), 1 << 20)
+    return dict(pairs=xy[:2 * n].reshape(n, 2).copy(), fStart=f.value, ffStart=ff.value,
+                sorted_Q=q[:nq].copy(), sorted_Qnumber=qn[:nq].copy())
+
+
+def ref_get2e(O, dense, cutMatrix, integral_cutoff, prim_limit, method=0):
+    """One QUICK Fock build: upload_method/calculated/cutoff + gpu_get2e_
+    (src/hfoperator.f90:76-98).  Returns the new O."""
+    r = ref_lib()
+    n = O.shape[0]
+    o = np.array(O, order="F", dtype=np.float64)
+    co = np.zeros((n, n), order="F")
+    vec = np.zeros((n, n), order="F")
+    d = np.array(dense, order="F", dtype=np.float64)
+    cm = np.array(cutMatrix, order="F", dtype=np.float64)
+    with _quiet():
+        r.gpu_upload_method_(_i(method))
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(vec), _ptr(d))
+        r.gpu_upload_cutoff_(_ptr(cm), _d(integral_cutoff), _d(prim_limit), None)
+        r.gpu_get2e_(_ptr(o))
+    return o

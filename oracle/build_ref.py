@@ -1,0 +1,69 @@
+"""Build ``oracle/_ref/libquickref.so``: QUICK's own CUDA bridge and kernels
+compiled as host code, used only as the checker for this package.
+
+The sources are read where they lie in the QUICK tree (``src/cuda``); the
+shim in ``oracle/ref_shim`` supplies a host stand-in for the CUDA runtime and
+the launch geometry.  Build outputs go to ``oracle/_ref`` only.
+
+    python oracle/build_ref.py [--quick-root /root/reference] [--spdf]
+"""
+import argparse
+import os
+import re
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SHIM = os.path.join(HERE, "ref_shim")
+OUT = os.path.join(HERE, "_ref")
+CUDA_INC = "/usr/local/cuda/include"
+
+
+def build(quick_root, spdf=False, jobs=8, opt="-O2"):
+    src = os.path.join(quick_root, "src", "cuda")
+    if not os.path.isdir(src):
+        raise FileNotFoundError("QUICK sources not found at %s" % src)
+    os.makedirs(os.path.join(OUT, "inc"), exist_ok=True)
+    # QUICK's headers include "../config.h" relative to src/cuda; with
+    # -I_ref/inc that resolves to _ref/config.h.
+    with open(os.path.join(SHIM, "config.h")) as fh:
+        cfg = fh.read()
+    if spdf:
+        cfg += "#define CUDA_SPDF\n"
+    with open(os.path.join(OUT, "config.h"), "w") as fh:
+        fh.write(cfg)
+    # gpu_getxc.cu: replace its one bare kernel launch (see ref_xc.cpp)
+    with open(os.path.join(src, "gpu_getxc.cu")) as fh:
+        xc = fh.read()
+    xc, n = re.subn(r"getxc_kernel<<<[^;]*?>>>\(\);", 'qref_launch("getxc_kernel<<<>>>");', xc)
+    assert n == 1, "expected one getxc_kernel launch"
+    with open(os.path.join(OUT, "gpu_getxc_host.cu"), "w") as fh:
+        fh.write(xc)
+    flags = [opt, "-fPIC", "-std=c++17", "-w", "-include", os.path.join(SHIM, "qref_shim.h"),
+             "-I" + SHIM, "-I" + os.path.join(OUT, "inc"), "-I" + OUT, "-I" + src, "-I" + CUDA_INC]
+    units = ["ref_bridge", "ref_kernels", "ref_type", "ref_xc"]
+    objs = []
+
+    def cc(u):
+        o = os.path.join(OUT, u + ".o")
+        cmd = ["g++"] + flags + ["-c", os.path.join(SHIM, u + ".cpp"), "-o", o]
+        subprocess.run(cmd, check=True)
+        return o
+
+    with ThreadPoolExecutor(jobs) as ex:
+        objs = list(ex.map(cc, units))
+    fo = os.path.join(OUT, "fake_cudart.o")
+    subprocess.run(["g++", opt, "-fPIC", "-std=c++17", "-I" + CUDA_INC, "-c",
+                    os.path.join(SHIM, "fake_cudart.cpp"), "-o", fo], check=True)
+    lib = os.path.join(OUT, "libquickref.so")
+    subprocess.run(["g++", "-shared", "-o", lib] + objs + [fo, "-lpthread"], check=True)
+    return lib
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--quick-root", default="/root/reference")
+    ap.add_argument("--spdf", action="store_true")
+    a = ap.parse_args()
+    print(build(a.quick_root, a.spdf))
