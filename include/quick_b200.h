@@ -1,0 +1,114 @@
+/*
+ * quick_b200 C ABI.
+ *
+ * Part 1 is a drop-in for the Fortran-callable bridge of QUICK's CUDA build
+ * (src/cuda/gpu.h:16-58, implemented in src/cuda/gpu.cu).  Same symbol names
+ * (lower case + trailing underscore), every argument by pointer (Fortran
+ * by-reference), arrays column-major, indices stored inside arrays 1-based,
+ * void return.  The call order QUICK's Fortran uses is kept:
+ *   start-up   gpu_startup_ -> gpu_set_device_ -> gpu_init_ -> gpu_setup_
+ *              -> gpu_upload_xyz_ -> gpu_upload_atom_and_chg_
+ *              -> gpu_upload_basis_ -> gpu_upload_cutoff_matrix_
+ *   per SCF    gpu_upload_method_ -> gpu_upload_calculated_
+ *              -> gpu_upload_cutoff_ -> gpu_get2e_        (src/hfoperator.f90:76-98)
+ *   gradient   gpu_upload_calculated_ -> gpu_upload_cutoff_ -> gpu_upload_grad_
+ *              -> gpu_grad_                               (src/gradient.f90:279-286)
+ *   DFT        ... -> gpu_getxc_                          (src/dft.f90:893-899)
+ * Where QUICK prints and exits on a fault, these print to stderr and record
+ * a sticky error that qb_status() returns.
+ *
+ * Part 2 adds entry points QUICK does not have (int status return, 0 = ok).
+ */
+#ifndef QUICK_B200_H
+#define QUICK_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- Part 1: QUICK's gpu_* bridge ------------------------------------ */
+/* src/cuda/gpu.cu:29 */
+void gpu_startup_(void);
+/* src/cuda/gpu.cu:18 */
+void gpu_set_device_(int* gpu_dev_id);
+/* src/cuda/gpu.cu:43-173 */
+void gpu_init_(void);
+/* src/cuda/gpu.cu:206-215 */
+void gpu_shutdown_(void);
+/* src/cuda/gpu.cu:175-201 (device count, id, memory MB, SM count, clock GHz, name, name length, major, minor) */
+void gpu_get_device_info_(int* gpu_dev_count, int* gpu_dev_id, int* gpu_dev_mem, int* gpu_num_proc,
+                          double* gpu_core_freq, char* gpu_dev_name, int* name_len, int* majorv, int* minorv);
+/* src/cuda/gpu.cu:221-267 */
+void gpu_setup_(int* natom, int* nbasis, int* nElec, int* imult, int* molchg, int* iAtomType);
+/* src/cuda/gpu.cu:269-278: 0 HF, 1 B3LYP (exchange 0.2), 2 DFT (no exchange) */
+void gpu_upload_method_(int* quick_method);
+/* src/cuda/gpu.cu:283-328: xyz(3, natom) in bohr */
+void gpu_upload_xyz_(double* atom_xyz);
+/* src/cuda/gpu.cu:334-349 */
+void gpu_upload_atom_and_chg_(int* atom, double* atom_chg);
+/* src/cuda/gpu.cu:1070-1390 */
+void gpu_upload_basis_(int* nshell, int* nprim, int* jshell, int* jbasis, int* maxcontract,
+                       int* ncontract, int* itype, double* aexp, double* dcoeff,
+                       int* first_basis_function, int* last_basis_function,
+                       int* first_shell_basis_function, int* last_shell_basis_function,
+                       int* ncenter, int* kstart, int* katom, int* ktype, int* kprim, int* kshell,
+                       int* Ksumtype, int* Qnumber, int* Qstart, int* Qfinal, int* Qsbasis, int* Qfbasis,
+                       double* gccoeff, double* cons, double* gcexpo, int* KLMN);
+/* src/cuda/gpu.cu:401-1003: YCutoff(nshell, nshell), cutPrim(jbasis, jbasis); builds the
+   shell-pair list in QUICK's exact order */
+void gpu_upload_cutoff_matrix_(double* YCutoff, double* cutPrim);
+/* src/cuda/gpu.cu:1008-1065: O(nbasis, nbasis) holds the one-electron operator, dense the density */
+void gpu_upload_calculated_(double* o, double* co, double* vec, double* dense);
+/* src/cuda/gpu.cu:356-394.  Fortran callers pass three arguments
+   (src/hfoperator.f90:81); the fourth is never read, DMCutoff is 1e-9 as in QUICK. */
+void gpu_upload_cutoff_(double* cutMatrix, double* integralCutoff, double* primLimit, double* DMCutoff);
+/* src/cuda/gpu.cu:1806-1864: o <- o + J - (h/2) K, symmetric */
+void gpu_get2e_(double* o);
+/* src/cuda/gpu.cu:1393-1444: grad(3 natom) accumulates, gradCutoff */
+void gpu_upload_grad_(double* grad, double* gradCutoff);
+/* src/cuda/gpu.cu:1481-1551: grad <- grad + two-electron gradient */
+void gpu_grad_(double* grad);
+/* src/cuda/gpu.cu:1866-1975 */
+void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double* belec, double* o);
+/* src/cuda/gpu.cu:1446-1479 */
+void gpu_cleanup_(void);
+/* src/cuda/gpu.cu:1559-1801, 1991-2237: the conventional (stored-integral) path is not built;
+   these report that and record an error. */
+void gpu_aoint_(double* leastIntegralCutoff, double* maxIntegralCutoff, int* intNum, char* intFileName);
+void gpu_addint_(double* o, int* intindex, char* intFileName);
+
+/* ---- Part 2: additions ---------------------------------------------- */
+/* Sticky status of the bridge: 0 ok, else an error code; message via qb_last_error. */
+int qb_status(void);
+const char* qb_last_error(void);
+void qb_clear_error(void);
+
+/* Run subsequent work on this CUDA stream (a cudaStream_t), 0 = the bridge's own stream. */
+int qb_set_stream(void* stream);
+
+/* QUICK's shell-pair list as gpu_upload_cutoff_matrix_ built it: xy[2*i], xy[2*i+1] are the
+   sorted-Qshell indices of pair i (QUICK's sorted_YCutoffIJ, gpu.cu:447-647); also the sorted
+   shell order (sorted_Q, sorted_Qnumber, gpu.cu:1191-1218) and fStart / ffStart.
+   Returns the number of pairs (or -1 if cap is too small). */
+int qb_get_pairlist(int* xy, int cap, int* sorted_Q, int* sorted_Qnumber, int qcap, int* fStart, int* ffStart);
+
+/* Host-only: QUICK's pair-list construction on given inputs, without a GPU (for tests).
+   sorted_Q, sorted_Qnumber, kprim are 0-based Qshell data; YCutoff is (nshell, nshell). */
+int qb_build_pairlist_host(int Qshell, const int* sorted_Q, const int* sorted_Qnumber, const int* kprim,
+                           int nshell, const double* YCutoff, int* xy_out, int cap, int* fStart, int* ffStart);
+
+/* Schwarz bounds on the GPU from the uploaded basis and coordinates, in QUICK's definition
+   (src/schwarz.f90:12-548): YCutoff(nshell, nshell), cutPrim(jbasis, jbasis). */
+int gpu_schwarz_(double* YCutoff, double* cutPrim);
+
+/* Fock build on device-resident data: D (nbasis^2, device pointer), O_in and O_out (device
+   pointers, may alias).  Uses the cutoffs and density screen from the last gpu_upload_cutoff_. */
+int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out);
+
+/* Statistics of the last Fock build: shell quartets (QUICK's iclass-call count),
+   device time of the class kernels in ms, device time of the screening in ms. */
+int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

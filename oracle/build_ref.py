@@ -57,7 +57,7 @@ def build(quick_root, spdf=False, jobs=8, opt="-O2"):
     subprocess.run(["g++", opt, "-fPIC", "-std=c++17", "-I" + CUDA_INC, "-c",
                     os.path.join(SHIM, "fake_cudart.cpp"), "-o", fo], check=True)
     lib = os.path.join(OUT, "libquickref.so")
-    subprocess.run(["g++", "-shared", "-o", lib] + objs + [fo, "-lpthread"], check=True)
+    subprocess.run(["g++", "-shared", "-Wl,-Bsymbolic", "-o", lib] + objs + [fo, "-lpthread"], check=True)
     return lib
 
 

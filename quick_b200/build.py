@@ -1,0 +1,86 @@
+"""Build ``quick_b200/_lib/libquickb200.so`` (sm_100a) in-tree.
+
+Generates the per-class kernels (csrc/gen_eri.py), compiles every CUDA
+source with nvcc for sm_100a in parallel and links one shared library with
+the CUDA runtime linked statically.  Rebuilds only what changed.
+
+    python -m quick_b200.build [--lmax 2] [--jobs 8]
+"""
+import argparse
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+GEN = os.path.join(CSRC, "gen")
+OBJ = os.path.join(HERE, "_build")
+LIBDIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIBDIR, "libquickb200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "-I" + CSRC, "-I" + os.path.join(HERE, "..", "include")]
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(lmax=2, jobs=None, verbose=False):
+    jobs = jobs or max(2, os.cpu_count() or 2)
+    subprocess.run([sys.executable, os.path.join(CSRC, "gen_eri.py"), GEN, "--lmax", str(lmax)],
+                   check=True, stdout=subprocess.DEVNULL)
+    os.makedirs(OBJ, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
+    headers += [os.path.join(GEN, "eri_classes.h"), os.path.join(HERE, "..", "include", "quick_b200.h")]
+    srcs = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
+    srcs += [os.path.join(GEN, f) for f in sorted(os.listdir(GEN)) if f.endswith(".cu")]
+    # drop generated classes beyond lmax (left over from an earlier build)
+    keep = []
+    for s in srcs:
+        b = os.path.basename(s)
+        if b.startswith("eri_") and b[4:8].isdigit() and max(int(ch) for ch in b[4:8]) > lmax:
+            continue
+        keep.append(s)
+    srcs = keep
+    objs = []
+    todo = []
+    for s in srcs:
+        o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
+        objs.append(o)
+        if _newer(o, [s] + headers):
+            todo.append((s, o))
+
+    def cc(so):
+        s, o = so
+        cmd = [NVCC] + ARCH + FLAGS + ["-c", s, "-o", o]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed on %s:\n%s" % (s, r.stderr[-4000:]))
+        if verbose and r.stderr.strip():
+            print(r.stderr)
+        return o
+
+    # longest compiles first
+    todo.sort(key=lambda so: -os.path.getsize(so[0]))
+    with ThreadPoolExecutor(jobs) as ex:
+        list(ex.map(cc, todo))
+    if todo or not os.path.exists(LIB):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lpthread"]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--lmax", type=int, default=2)
+    ap.add_argument("--jobs", type=int, default=None)
+    ap.add_argument("-v", action="store_true")
+    a = ap.parse_args()
+    print(build(a.lmax, a.jobs, a.v))

@@ -1,0 +1,169 @@
+"""ctypes binding of ``libquickb200.so`` (the C ABI in include/quick_b200.h).
+
+The call sequence mirrors QUICK's Fortran host: ``upload_molecule`` is the
+start-up part of src/main.f90:84-177, ``get2e`` one Fock build of
+src/hfoperator.f90:76-98.  Every call checks the bridge's sticky status and
+raises ``QuickB200Error`` with its message; there is no fallback path.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libquickb200.so")
+
+_P = C.c_void_p
+
+
+class QuickB200Error(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise QuickB200Error("libquickb200.so not built: run `python -m quick_b200.build` "
+                                 "(expected at %s)" % LIB_PATH)
+        _lib = C.CDLL(LIB_PATH)
+        _lib.qb_last_error.restype = C.c_char_p
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_P)
+
+
+def _i(v):
+    return C.byref(C.c_int(int(v)))
+
+
+def _d(v):
+    return C.byref(C.c_double(float(v)))
+
+
+def check():
+    r = lib()
+    st = r.qb_status()
+    if st:
+        msg = r.qb_last_error().decode()
+        r.qb_clear_error()
+        raise QuickB200Error("quick_b200 error %d: %s" % (st, msg))
+
+
+class Session:
+    """One molecule resident on the GPU behind QUICK's gpu_* entry points."""
+
+    def __init__(self, device=0):
+        r = lib()
+        r.qb_clear_error()
+        r.gpu_startup_()
+        r.gpu_set_device_(_i(device))
+        r.gpu_init_()
+        check()
+        self._keep = []
+        self.nbasis = 0
+
+    def _arr(self, a, dt):
+        x = np.asfortranarray(a, dtype=dt)
+        self._keep.append(x)
+        return _ptr(x)
+
+    def upload_molecule(self, mol, basis, YCutoff=None, cutPrim=None):
+        """Start-up uploads; YCutoff / cutPrim default to the GPU Schwarz kernel."""
+        r = lib()
+        b = basis
+        self.basis = b
+        self.nbasis = b.nbasis
+        self.nshell = b.nshell
+        I32, F64 = np.int32, np.float64
+        r.gpu_setup_(_i(mol.natom), _i(b.nbasis), _i(mol.n_electrons), _i(mol.mult), _i(mol.charge),
+                     _i(len(set(mol.symbols))))
+        r.gpu_upload_xyz_(self._arr(mol.xyz_bohr, F64))
+        r.gpu_upload_atom_and_chg_(self._arr(mol.atomic_numbers, I32),
+                                   self._arr(mol.atomic_numbers.astype(F64), F64))
+        r.gpu_upload_basis_(_i(b.nshell), _i(b.nprim), _i(b.jshell), _i(b.jbasis), _i(b.maxcontract),
+                            self._arr(b.ncontract, I32), self._arr(b.itype, I32), self._arr(b.aexp, F64),
+                            self._arr(b.dcoeff, F64), self._arr(b.first_basis_function, I32),
+                            self._arr(b.last_basis_function, I32), self._arr(b.first_shell_basis_function, I32),
+                            self._arr(b.last_shell_basis_function, I32), self._arr(b.ncenter, I32),
+                            self._arr(b.kstart, I32), self._arr(b.katom, I32), self._arr(b.ktype, I32),
+                            self._arr(b.kprim, I32), self._arr(b.kshell, I32), self._arr(b.Ksumtype, I32),
+                            self._arr(b.Qnumber, I32), self._arr(b.Qstart, I32), self._arr(b.Qfinal, I32),
+                            self._arr(b.Qsbasis, I32), self._arr(b.Qfbasis, I32), self._arr(b.gccoeff, F64),
+                            self._arr(b.cons, F64), self._arr(b.gcexpo, F64), self._arr(b.KLMN, I32))
+        check()
+        if YCutoff is None:
+            YCutoff, cutPrim = self.schwarz()
+        r.gpu_upload_cutoff_matrix_(self._arr(YCutoff, F64), self._arr(cutPrim, F64))
+        check()
+        self.YCutoff, self.cutPrim = YCutoff, cutPrim
+
+    def schwarz(self):
+        b = self.basis
+        Y = np.zeros((b.nshell, b.nshell), order="F")
+        cp = np.zeros((b.jbasis, b.jbasis), order="F")
+        lib().gpu_schwarz_(_ptr(Y), _ptr(cp))
+        check()
+        return Y, cp
+
+    def get2e(self, O, dense, cutMatrix, integral_cutoff, prim_limit, method=0):
+        """O + G(dense): QUICK's upload_method / calculated / cutoff + gpu_get2e_."""
+        r = lib()
+        n = self.nbasis
+        o = np.array(O, order="F", dtype=np.float64)
+        co = np.zeros((1,), dtype=np.float64)
+        d = np.asfortranarray(dense, dtype=np.float64)
+        cm = np.asfortranarray(cutMatrix, dtype=np.float64)
+        r.gpu_upload_method_(_i(method))
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(co), _ptr(d))
+        r.gpu_upload_cutoff_(_ptr(cm), _d(integral_cutoff), _d(prim_limit), None)
+        r.gpu_get2e_(_ptr(o))
+        check()
+        return o
+
+    def fock_stats(self):
+        q, a, b = C.c_longlong(0), C.c_double(0), C.c_double(0)
+        lib().qb_last_fock_stats(C.byref(q), C.byref(a), C.byref(b))
+        return dict(quartets=q.value, ms_eri=a.value, ms_screen=b.value)
+
+    def pairlist(self):
+        cap = 1 << 24
+        xy = np.zeros(2 * cap, dtype=np.int32)
+        q = np.zeros(1 << 20, dtype=np.int32)
+        qn = np.zeros(1 << 20, dtype=np.int32)
+        f, ff = C.c_int(0), C.c_int(0)
+        n = lib().qb_get_pairlist(_ptr(xy), cap, _ptr(q), _ptr(qn), 1 << 20, C.byref(f), C.byref(ff))
+        check()
+        nq = sum(int(self.basis.Qfinal[s] - self.basis.Qstart[s] + 1) for s in range(self.basis.nshell))
+        return dict(pairs=xy[:2 * n].reshape(n, 2).copy(), fStart=f.value, ffStart=ff.value,
+                    sorted_Q=q[:nq].copy(), sorted_Qnumber=qn[:nq].copy())
+
+    def close(self):
+        lib().gpu_shutdown_()
+
+
+def build_pairlist_host(basis, YCutoff):
+    """QUICK's pair-list construction on the host (no GPU needed)."""
+    sq, sqn = [], []
+    for L in range(4):
+        for s in range(basis.nshell):
+            if basis.Qstart[s] <= L <= basis.Qfinal[s]:
+                sq.append(s)
+                sqn.append(L)
+    sq = np.array(sq, dtype=np.int32)
+    sqn = np.array(sqn, dtype=np.int32)
+    kp = np.ascontiguousarray(basis.kprim, dtype=np.int32)
+    Y = np.asfortranarray(YCutoff, dtype=np.float64)
+    cap = len(sq) * len(sq)
+    xy = np.zeros(2 * cap, dtype=np.int32)
+    f, ff = C.c_int(0), C.c_int(0)
+    n = lib().qb_build_pairlist_host(len(sq), _ptr(sq), _ptr(sqn), _ptr(kp), basis.nshell, _ptr(Y), _ptr(xy), cap,
+                                     C.byref(f), C.byref(ff))
+    return dict(pairs=xy[:2 * n].reshape(n, 2).copy(), fStart=f.value, ffStart=ff.value,
+                sorted_Q=sq, sorted_Qnumber=sqn)

@@ -1,0 +1,835 @@
+// Host side of the C ABI: QUICK's gpu_* bridge (src/cuda/gpu.cu) rebuilt
+// around device-resident, class-sorted shell-pair tables.
+//
+// Differences from QUICK's bridge, by design:
+//  * device buffers are allocated once per geometry and reused every SCF
+//    iteration (QUICK re-allocates o, dense and oULL per call);
+//  * the Fock matrix accumulates in FP64 with device atomics after per-thread
+//    and per-warp reduction, not as 64-bit fixed point with one atomic per
+//    integral;
+//  * quartets are screened into per-class work lists instead of testing all
+//    sqrQshell^2 pair-pairs in every thread.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/quick_b200.h"
+#include "gen/eri_classes.h"
+#include "qb_internal.h"
+
+namespace qb {
+
+constexpr int MAXPRIM = 10;                                  // src/modules/quick_size_module.f90:37
+constexpr double X0 = 5.9149671727956128778234784350536;    // sqrt(2 pi^2.5), gpu_common.h:196
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count)
+    {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        n = count;
+        return cudaMalloc((void**)&p, std::max<size_t>(count, 1) * sizeof(T));
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct Context {
+    int dev_id = -1;
+    bool inited = false;
+    int nsm = 148;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    // molecule
+    int natom = 0, nbasis = 0, nelec = 0, imult = 1, molchg = 0, iAtomType = 0;
+    int method = 0;
+    std::vector<double> xyz;
+    std::vector<int> iattype;
+    std::vector<double> chg;
+    // basis (QUICK arrays)
+    int nshell = 0, nprim = 0, jshell = 0, jbasis = 0, maxcontract = 0;
+    std::vector<int> kstart, katom, kprim, Ksumtype, Qnumber, Qstart, Qfinal, Qsbasis, Qfbasis, KLMN;
+    std::vector<double> gccoeff, gcexpo, cons;
+    bool have_basis = false;
+    int Qshell = 0, maxL = 0;
+    std::vector<int> sorted_Q, sorted_Qnumber;
+    // QUICK's pair list
+    std::vector<int> ref_xy;
+    int fStart = 0, ffStart = 0;
+    std::vector<double> YCutoff, cutPrim;
+    bool have_pairs = false;
+    // our pair table
+    int npair = 0;
+    std::vector<int> type_begin, type_end;
+    // device tables
+    DevBuf<double4> d_prim;
+    DevBuf<double> d_cut_prim, d_pair_Y, d_boys, d_dense, d_dense_raw, d_cons, d_fock, d_cut_matrix, d_o_in, d_o_out;
+    DevBuf<int4> d_pair_bf, d_pair_sh;
+    DevBuf<double4> d_pair_AB;
+    DevBuf<ScreenClass> d_screen_cls;
+    DevBuf<unsigned long long> d_counts;
+    DevBuf<int> d_class_count, d_overflow;
+    DevBuf<long long> d_class_offset;
+    DevBuf<int2> d_quartets;
+    std::vector<ScreenClass> screen_cls;
+    // per-iteration
+    std::vector<double> o_host;          // O as uploaded (one-electron part)
+    std::vector<double> dense_host;
+    bool have_calc = false;
+    double integralCutoff = 1e-7, primLimit = 1e-7, DMCutoff = 1e-9, gradCutoff = 1e-7;
+    std::vector<double> cutMatrix;
+    bool have_cutoff = false;
+    // stats
+    long long last_quartets = 0;
+    double last_ms_eri = 0, last_ms_screen = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+static Context* g = nullptr;
+static int g_status = 0;
+static std::string g_err;
+
+static void set_error(int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (!g_status) {
+        g_status = code;
+        g_err = buf;
+    }
+    fprintf(stderr, "quick_b200: %s\n", buf);
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            set_error(2, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return 2;                                                                     \
+        }                                                                                 \
+    } while (0)
+
+static int require(bool cond, const char* what)
+{
+    if (!cond) {
+        set_error(1, "%s", what);
+        return 1;
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------ Boys table
+// F_m(k/32) for the device table, summed as a long-double series
+// F_m(T) = e^-T sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)) at the top m, then
+// downward recursion, which is stable.
+static void boys_table(std::vector<double>& tab)
+{
+    tab.assign((size_t)kBoysPoints * kBoysCols, 0.0);
+    for (int k = 0; k < kBoysPoints; k++) {
+        long double T = (long double)k / kBoysPerUnit;
+        int mmax = kBoysCols - 1;
+        long double term = 1.0L / (2 * mmax + 1), sum = term;
+        for (int j = 1; j < 2000; j++) {
+            term *= 2.0L * T / (2 * mmax + 2 * j + 1);
+            sum += term;
+            if (term < sum * 1e-22L) break;
+        }
+        long double e = expl(-T);
+        long double f = e * sum;
+        tab[(size_t)k * kBoysCols + mmax] = (double)f;
+        for (int m = mmax - 1; m >= 0; m--) {
+            f = (2.0L * T * f + e) / (2 * m + 1);
+            tab[(size_t)k * kBoysCols + m] = (double)f;
+        }
+    }
+}
+
+// ------------------------------------------------------------- pair list
+// QUICK's shell-pair list (gpu.cu:401-1003, sort_method 0), restated with
+// stable sorts.  QUICK bubble-sorts each (q,p) class with strict
+// comparisons, which leaves equal keys in insertion order; a stable sort on
+// the same key gives the identical sequence.
+//   band 1: YCutoff > 1e-4, ordered by kprim(x)*kprim(y) descending, ties by
+//           kprim(x) descending (gpu.cu:447-531);
+//   band 2: 1e-10 < YCutoff <= 1e-4, ordered by YCutoff descending, then
+//           stably by the same kprim key (gpu.cu:532-636).
+// fStart / ffStart mark the first (d,f) and the first (p+q = 6) class.
+static int build_pairlist(int Qshell, const int* sQ, const int* sQn, const int* kprim, int nshell,
+                          const double* Y, std::vector<int>& xy, int& fStart, int& ffStart)
+{
+    xy.clear();
+    fStart = 0;
+    ffStart = 0;
+    const double cut1 = 1e-10, cut2 = 1e-4;
+    auto yv = [&](int x, int y) { return Y[(size_t)sQ[x] + (size_t)sQ[y] * nshell]; };
+    auto kp = [&](int x) { return kprim[sQ[x]]; };
+    for (int band = 0; band < 2; band++) {
+        for (int qp = 0; qp <= 6; qp++)
+            for (int q = 0; q <= 3; q++)
+                for (int p = 0; p <= 3; p++) {
+                    if (p + q != qp) continue;
+                    std::vector<std::pair<int, int>> blk;
+                    for (int i = 0; i < Qshell; i++)
+                        for (int j = 0; j < Qshell; j++) {
+                            if (sQn[i] != q || sQn[j] != p || sQ[i] > sQ[j]) continue;
+                            double v = yv(i, j);
+                            bool in = band == 0 ? (v > cut2) : (v <= cut2 && v > cut1);
+                            if (in) blk.push_back({i, j});
+                        }
+                    if (band == 1)
+                        std::stable_sort(blk.begin(), blk.end(), [&](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+                            return yv(a.first, a.second) > yv(b.first, b.second);
+                        });
+                    std::stable_sort(blk.begin(), blk.end(), [&](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+                        long pa = (long)kp(a.first) * kp(a.second), pb = (long)kp(b.first) * kp(b.second);
+                        if (pa != pb) return pa > pb;
+                        return kp(a.first) > kp(b.first);
+                    });
+                    int a_before = (int)xy.size() / 2;
+                    for (auto& e : blk) {
+                        xy.push_back(e.first);
+                        xy.push_back(e.second);
+                    }
+                    if (!blk.empty()) {
+                        if (q == 2 && p == 3 && (band == 0 || fStart == 0)) fStart = a_before;
+                        if (p + q == 6 && (band == 0 || ffStart == 0)) ffStart = a_before;
+                    }
+                }
+    }
+    int a = (int)xy.size() / 2;
+    if (ffStart == 0) ffStart = a;
+    if (fStart == 0) fStart = a;
+    return a;
+}
+
+// Shells sorted by angular momentum, stable in shell order (gpu.cu:1165-1218).
+static void sort_qshells(Context& c)
+{
+    c.Qshell = 0;
+    for (int i = 0; i < c.nshell; i++) c.Qshell += c.Qfinal[i] - c.Qstart[i] + 1;
+    c.sorted_Q.clear();
+    c.sorted_Qnumber.clear();
+    for (int L = 0; L <= 3; L++)
+        for (int s = 0; s < c.nshell; s++)
+            if (c.Qstart[s] <= L && L <= c.Qfinal[s]) {
+                c.sorted_Q.push_back(s);
+                c.sorted_Qnumber.push_back(L);
+            }
+    c.maxL = 0;
+    for (int v : c.sorted_Qnumber) c.maxL = std::max(c.maxL, v);
+}
+
+static inline double ccoef(const Context& c, int sh, int L, int p)
+{
+    return c.gccoeff[(size_t)p + (size_t)(c.Ksumtype[sh] - 1 + L) * MAXPRIM];
+}
+static inline double cexpo(const Context& c, int sh, int p)
+{
+    return c.gcexpo[(size_t)p + (size_t)(c.Ksumtype[sh] - 1) * MAXPRIM];
+}
+static inline int bf_first(const Context& c, int sh, int L)
+{
+    return c.Ksumtype[sh] - 1 + c.Qsbasis[(size_t)sh + (size_t)L * c.nshell];
+}
+static inline const double* center(const Context& c, int sh) { return c.xyz.data() + 3 * (c.katom[sh] - 1); }
+
+static int pair_type_index(int la, int lb)
+{
+    for (int t = 0; t < kNumPairTypes; t++)
+        if (kPairTypeL[t][0] == la && kPairTypeL[t][1] == lb) return t;
+    return -1;
+}
+
+// Our pair table from QUICK's list: drop the (p,s) copies of an sp shell's
+// self-pair (QUICK lists both (s,p) and (p,s); its basis-function filter
+// discards every integral of the second), orient each pair with the higher
+// angular momentum first, group by pair type and sort by Schwarz bound.
+static int build_tables(Context& c)
+{
+    struct Rec {
+        int type, shA, shB, LA, LB, ref, key;
+        double Y, w;
+    };
+    std::vector<Rec> recs;
+    int npref = (int)c.ref_xy.size() / 2;
+    for (int r = 0; r < npref; r++) {
+        int x = c.ref_xy[2 * r], y = c.ref_xy[2 * r + 1];
+        int sx = c.sorted_Q[x], sy = c.sorted_Q[y], Lx = c.sorted_Qnumber[x], Ly = c.sorted_Qnumber[y];
+        if (sx == sy && x != y && Lx > Ly) continue;
+        Rec e;
+        e.ref = r;
+        e.Y = c.YCutoff[(size_t)sx + (size_t)sy * c.nshell];
+        e.w = (x == y) ? 0.5 : 1.0;
+        e.key = sx * 4 + Lx;
+        if (Lx >= Ly) { e.shA = sx; e.LA = Lx; e.shB = sy; e.LB = Ly; }
+        else { e.shA = sy; e.LA = Ly; e.shB = sx; e.LB = Lx; }
+        e.type = pair_type_index(e.LA, e.LB);
+        if (e.type < 0) return set_error(1, "angular momentum (%d,%d) beyond this build", e.LA, e.LB), 1;
+        recs.push_back(e);
+    }
+    std::stable_sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) {
+        if (a.type != b.type) return a.type < b.type;
+        return a.Y > b.Y;
+    });
+    c.npair = (int)recs.size();
+    c.type_begin.assign(kNumPairTypes, 0);
+    c.type_end.assign(kNumPairTypes, 0);
+    for (int t = 0, i = 0; t < kNumPairTypes; t++) {
+        c.type_begin[t] = i;
+        while (i < c.npair && recs[i].type == t) i++;
+        c.type_end[t] = i;
+    }
+    std::vector<int4> pbf(c.npair), psh(c.npair);
+    std::vector<double> pY(c.npair);
+    std::vector<double4> pAB(c.npair);
+    std::vector<double4> prim;
+    std::vector<double> cprim;
+    for (int i = 0; i < c.npair; i++) {
+        const Rec& e = recs[i];
+        const double *A = center(c, e.shA), *B = center(c, e.shB);
+        double AB2 = 0;
+        for (int k = 0; k < 3; k++) AB2 += (A[k] - B[k]) * (A[k] - B[k]);
+        int off = (int)cprim.size();
+        // QUICK's own orientation (first Qshell x) indexes cutPrim
+        int x = c.ref_xy[2 * e.ref], y = c.ref_xy[2 * e.ref + 1];
+        int sx = c.sorted_Q[x], sy = c.sorted_Q[y];
+        for (int pa = 0; pa < c.kprim[e.shA]; pa++)
+            for (int pb = 0; pb < c.kprim[e.shB]; pb++) {
+                double a = cexpo(c, e.shA, pa), b = cexpo(c, e.shB, pb), p = a + b;
+                double X = exp(-a * b / p * AB2) / p;
+                double K = X0 * X * ccoef(c, e.shA, e.LA, pa) * ccoef(c, e.shB, e.LB, pb);
+                double P[3], PA[3];
+                for (int k = 0; k < 3; k++) {
+                    P[k] = (A[k] * a + B[k] * b) / p;
+                    PA[k] = P[k] - A[k];
+                }
+                prim.push_back(make_double4(p, K, P[0], P[1]));
+                prim.push_back(make_double4(P[2], PA[0], PA[1], PA[2]));
+                int px = (e.shA == sx && (sx != sy || e.LA == c.sorted_Qnumber[x])) ? pa : pb;
+                int py = (px == pa) ? pb : pa;
+                cprim.push_back(c.cutPrim[(size_t)(c.kstart[sx] - 1 + px) + (size_t)(c.kstart[sy] - 1 + py) * c.jbasis]);
+            }
+        pbf[i] = make_int4(bf_first(c, e.shA, e.LA), bf_first(c, e.shB, e.LB), off, (int)cprim.size() - off);
+        psh[i] = make_int4(e.shA, e.shB, e.key, e.ref);
+        pY[i] = e.Y;
+        pAB[i] = make_double4(A[0] - B[0], A[1] - B[1], A[2] - B[2], e.w);
+    }
+    CK(c.d_prim.alloc(prim.size()));
+    CK(c.d_cut_prim.alloc(cprim.size()));
+    CK(c.d_pair_bf.alloc(c.npair));
+    CK(c.d_pair_sh.alloc(c.npair));
+    CK(c.d_pair_Y.alloc(c.npair));
+    CK(c.d_pair_AB.alloc(c.npair));
+    CK(cudaMemcpy(c.d_prim.p, prim.data(), prim.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.d_cut_prim.p, cprim.data(), cprim.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.d_pair_bf.p, pbf.data(), pbf.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.d_pair_sh.p, psh.data(), psh.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.d_pair_Y.p, pY.data(), pY.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.d_pair_AB.p, pAB.data(), pAB.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    // screening classes
+    c.screen_cls.assign(kNumClasses, ScreenClass{});
+    for (int k = 0; k < kNumClasses; k++) {
+        int tb = pair_type_index(kClassL[k][0], kClassL[k][1]);
+        int tk = pair_type_index(kClassL[k][2], kClassL[k][3]);
+        ScreenClass& s = c.screen_cls[k];
+        s.bra_begin = c.type_begin[tb];
+        s.bra_end = c.type_end[tb];
+        s.ket_begin = c.type_begin[tk];
+        s.ket_end = c.type_end[tk];
+        s.same_type = tb == tk;
+        s.out_offset = 0;
+        s.capacity = 0;
+    }
+    return 0;
+}
+
+static FockParams fock_params(Context& c)
+{
+    FockParams P;
+    P.prim = c.d_prim.p;
+    P.cut_prim = c.d_cut_prim.p;
+    P.pair_bf = c.d_pair_bf.p;
+    P.pair_sh = c.d_pair_sh.p;
+    P.pair_Y = c.d_pair_Y.p;
+    P.pair_AB = c.d_pair_AB.p;
+    P.quartets = c.d_quartets.p;
+    P.class_offset = c.d_class_offset.p;
+    P.class_count = c.d_class_count.p;
+    P.dense = c.d_dense.p;
+    P.fock = c.d_fock.p;
+    P.cut_matrix = c.d_cut_matrix.p;
+    P.boys = c.d_boys.p;
+    P.nbasis = c.nbasis;
+    P.nshell = c.nshell;
+    P.prim_limit = c.primLimit;
+    P.hybrid = c.method == 0 ? 1.0 : (c.method == 1 ? 0.2 : 0.0);
+    P.integral_cutoff = c.integralCutoff;
+    return P;
+}
+
+// Size the per-class quartet lists by the Schwarz-only count (an upper bound
+// for every density), once per geometry and cutoff.
+static double g_sized_cutoff = -1.0;
+static int size_quartet_lists(Context& c)
+{
+    CK(c.d_screen_cls.alloc(kNumClasses));
+    CK(c.d_counts.alloc(kNumClasses));
+    CK(c.d_class_count.alloc(kNumClasses));
+    CK(c.d_class_offset.alloc(kNumClasses));
+    CK(c.d_overflow.alloc(1));
+    CK(cudaMemcpy(c.d_screen_cls.p, c.screen_cls.data(), kNumClasses * sizeof(ScreenClass), cudaMemcpyHostToDevice));
+    CK(cudaMemsetAsync(c.d_counts.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
+    FockParams P = fock_params(c);
+    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, nullptr};
+    launch_screen(S, P, kNumClasses, 1, c.nsm, c.stream);
+    CK(cudaGetLastError());
+    std::vector<unsigned long long> cnt(kNumClasses);
+    CK(cudaMemcpyAsync(cnt.data(), c.d_counts.p, kNumClasses * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    long long off = 0;
+    std::vector<long long> offs(kNumClasses);
+    for (int k = 0; k < kNumClasses; k++) {
+        c.screen_cls[k].out_offset = off;
+        c.screen_cls[k].capacity = (long long)cnt[k];
+        offs[k] = off;
+        off += (long long)cnt[k];
+    }
+    CK(c.d_quartets.alloc((size_t)std::max<long long>(off, 1)));
+    CK(cudaMemcpy(c.d_screen_cls.p, c.screen_cls.data(), kNumClasses * sizeof(ScreenClass), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.d_class_offset.p, offs.data(), kNumClasses * sizeof(long long), cudaMemcpyHostToDevice));
+    g_sized_cutoff = c.integralCutoff;
+    return 0;
+}
+
+// The Fock build proper, on device data already in place (d_dense,
+// d_cut_matrix): screening, class kernels, O_out = O_in + G.
+static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
+{
+    if (require(c.have_pairs, "gpu_upload_cutoff_matrix_ must precede the Fock build")) return 1;
+    if (require(c.have_cutoff, "gpu_upload_cutoff_ must precede the Fock build")) return 1;
+    if (g_sized_cutoff != c.integralCutoff || c.d_quartets.p == nullptr)
+        if (size_quartet_lists(c)) return 2;
+    int n = c.nbasis;
+    CK(c.d_fock.alloc((size_t)n * n));
+    CK(cudaMemsetAsync(c.d_fock.p, 0, (size_t)n * n * sizeof(double), c.stream));
+    CK(cudaMemsetAsync(c.d_counts.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
+    CK(cudaMemsetAsync(c.d_overflow.p, 0, sizeof(int), c.stream));
+    CK(c.d_dense.alloc((size_t)n * n));
+    launch_scale_density(c.d_dense_raw.p, c.d_cons.p, c.d_dense.p, n, c.stream);
+    FockParams P = fock_params(c);
+    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p};
+    for (int k = 0; k < 4; k++)
+        if (!c.ev[k]) CK(cudaEventCreate(&c.ev[k]));
+    CK(cudaEventRecord(c.ev[0], c.stream));
+    launch_screen(S, P, kNumClasses, 0, c.nsm, c.stream);
+    launch_finish_counts(S, c.d_class_count.p, c.d_overflow.p, kNumClasses, c.stream);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c.ev[1], c.stream));
+    std::vector<int> cnt(kNumClasses);
+    int ovf = 0;
+    CK(cudaMemcpyAsync(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&ovf, c.d_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (ovf) return set_error(3, "quartet list overflow (internal sizing error)"), 3;
+    long long total = 0;
+    CK(cudaEventRecord(c.ev[2], c.stream));
+    for (int k = 0; k < kNumClasses; k++) {
+        if (cnt[k] == 0) continue;
+        total += cnt[k];
+        int block = 128;
+        long long warps = (cnt[k] + 31) / 32;
+        long long grid = std::min<long long>((warps * 32 + block - 1) / block, (long long)c.nsm * 16);
+        launch_class(k, P, (int)std::max<long long>(grid, 1), block, c.stream);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c.ev[3], c.stream));
+    launch_fock_finish(c.d_fock.p, c.d_cons.p, d_o_in, d_o_out, n, c.stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c.stream));
+    float ms0 = 0, ms1 = 0;
+    CK(cudaEventElapsedTime(&ms0, c.ev[0], c.ev[1]));
+    CK(cudaEventElapsedTime(&ms1, c.ev[2], c.ev[3]));
+    c.last_ms_screen = ms0;
+    c.last_ms_eri = ms1;
+    c.last_quartets = total;
+    return 0;
+}
+
+static Context& ctx()
+{
+    if (!g) g = new Context();
+    return *g;
+}
+
+}  // namespace qb
+
+using namespace qb;
+
+extern "C" {
+
+int qb_status(void) { return g_status; }
+const char* qb_last_error(void) { return g_err.c_str(); }
+void qb_clear_error(void)
+{
+    g_status = 0;
+    g_err.clear();
+}
+
+void gpu_startup_(void)
+{
+    delete g;
+    g = new Context();
+}
+
+void gpu_set_device_(int* gpu_dev_id) { ctx().dev_id = *gpu_dev_id; }
+
+void gpu_init_(void)
+{
+    Context& c = ctx();
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        set_error(10, "no CUDA device available (%s)", cudaGetErrorString(e));
+        return;
+    }
+    int dev = c.dev_id < 0 ? 0 : c.dev_id;
+    if (dev >= count) {
+        set_error(11, "GPU id %d is illegal, select from 0 to %d", dev, count - 1);
+        return;
+    }
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, dev);
+    if (prop.major < 10) {
+        set_error(12, "device %d is sm_%d%d; this build targets sm_100a (B200)", dev, prop.major, prop.minor);
+        return;
+    }
+    if (cudaSetDevice(dev) != cudaSuccess) {
+        set_error(13, "cudaSetDevice(%d) failed", dev);
+        return;
+    }
+    c.dev_id = dev;
+    c.nsm = prop.multiProcessorCount;
+    if (!c.own_stream) cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking);
+    if (!c.stream) c.stream = c.own_stream;
+    std::vector<double> tab;
+    boys_table(tab);
+    if (c.d_boys.alloc(tab.size()) != cudaSuccess ||
+        cudaMemcpy(c.d_boys.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        set_error(2, "cannot upload the Boys table");
+        return;
+    }
+    c.inited = true;
+}
+
+int qb_set_stream(void* stream)
+{
+    Context& c = ctx();
+    c.stream = stream ? (cudaStream_t)stream : c.own_stream;
+    return 0;
+}
+
+void gpu_shutdown_(void)
+{
+    if (!g) return;
+    Context& c = *g;
+    DevBuf<double>* dbl[] = {&c.d_cut_prim, &c.d_pair_Y, &c.d_boys, &c.d_dense, &c.d_dense_raw, &c.d_cons, &c.d_fock, &c.d_cut_matrix, &c.d_o_in, &c.d_o_out};
+    for (auto* b : dbl) b->release();
+    c.d_prim.release();
+    c.d_pair_bf.release();
+    c.d_pair_sh.release();
+    c.d_pair_AB.release();
+    c.d_screen_cls.release();
+    c.d_counts.release();
+    c.d_class_count.release();
+    c.d_overflow.release();
+    c.d_class_offset.release();
+    c.d_quartets.release();
+    for (auto& e : c.ev)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    if (c.own_stream) cudaStreamDestroy(c.own_stream);
+    delete g;
+    g = nullptr;
+    g_sized_cutoff = -1.0;
+}
+
+void gpu_get_device_info_(int* gpu_dev_count, int* gpu_dev_id, int* gpu_dev_mem, int* gpu_num_proc, double* gpu_core_freq,
+                          char* gpu_dev_name, int* name_len, int* majorv, int* minorv)
+{
+    Context& c = ctx();
+    *gpu_dev_id = c.dev_id;
+    if (cudaGetDeviceCount(gpu_dev_count) != cudaSuccess || *gpu_dev_count == 0) {
+        *gpu_dev_count = 0;
+        set_error(10, "no CUDA device found");
+        return;
+    }
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, c.dev_id < 0 ? 0 : c.dev_id);
+    *gpu_dev_mem = (int)(prop.totalGlobalMem / (1024 * 1024));
+    *gpu_num_proc = prop.multiProcessorCount;
+    int clk = 0;
+    cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, c.dev_id < 0 ? 0 : c.dev_id);
+    *gpu_core_freq = clk * 1e-6;
+    strcpy(gpu_dev_name, prop.name);
+    *name_len = (int)strlen(gpu_dev_name);
+    *majorv = prop.major;
+    *minorv = prop.minor;
+}
+
+void gpu_setup_(int* natom, int* nbasis, int* nElec, int* imult, int* molchg, int* iAtomType)
+{
+    Context& c = ctx();
+    c.natom = *natom;
+    c.nbasis = *nbasis;
+    c.nelec = *nElec;
+    c.imult = *imult;
+    c.molchg = *molchg;
+    c.iAtomType = *iAtomType;
+}
+
+void gpu_upload_method_(int* quick_method)
+{
+    if (*quick_method < 0 || *quick_method > 2) {
+        set_error(1, "unknown method %d", *quick_method);
+        return;
+    }
+    ctx().method = *quick_method;
+}
+
+void gpu_upload_xyz_(double* atom_xyz)
+{
+    Context& c = ctx();
+    c.xyz.assign(atom_xyz, atom_xyz + 3 * c.natom);
+}
+
+void gpu_upload_atom_and_chg_(int* atom, double* atom_chg)
+{
+    Context& c = ctx();
+    c.iattype.assign(atom, atom + c.natom);
+    c.chg.assign(atom_chg, atom_chg + c.natom);
+}
+
+void gpu_upload_basis_(int* nshell, int* nprim, int* jshell, int* jbasis, int* maxcontract, int* ncontract, int* itype,
+                       double* aexp, double* dcoeff, int* first_basis_function, int* last_basis_function,
+                       int* first_shell_basis_function, int* last_shell_basis_function, int* ncenter, int* kstart,
+                       int* katom, int* ktype, int* kprim, int* kshell, int* Ksumtype, int* Qnumber, int* Qstart,
+                       int* Qfinal, int* Qsbasis, int* Qfbasis, double* gccoeff, double* cons, double* gcexpo, int* KLMN)
+{
+    Context& c = ctx();
+    c.nshell = *nshell;
+    c.nprim = *nprim;
+    c.jshell = *jshell;
+    c.jbasis = *jbasis;
+    c.maxcontract = *maxcontract;
+    int ns = c.nshell, nb = c.nbasis;
+    c.kstart.assign(kstart, kstart + ns);
+    c.katom.assign(katom, katom + ns);
+    c.kprim.assign(kprim, kprim + ns);
+    c.Ksumtype.assign(Ksumtype, Ksumtype + ns + 1);
+    c.Qnumber.assign(Qnumber, Qnumber + ns);
+    c.Qstart.assign(Qstart, Qstart + ns);
+    c.Qfinal.assign(Qfinal, Qfinal + ns);
+    c.Qsbasis.assign(Qsbasis, Qsbasis + 4 * ns);
+    c.Qfbasis.assign(Qfbasis, Qfbasis + 4 * ns);
+    c.KLMN.assign(KLMN, KLMN + 3 * nb);
+    c.gccoeff.assign(gccoeff, gccoeff + (size_t)MAXPRIM * nb);
+    c.gcexpo.assign(gcexpo, gcexpo + (size_t)MAXPRIM * nb);
+    c.cons.assign(cons, cons + nb);
+    (void)ncontract; (void)itype; (void)aexp; (void)dcoeff; (void)first_basis_function; (void)last_basis_function;
+    (void)first_shell_basis_function; (void)last_shell_basis_function; (void)ncenter; (void)ktype; (void)kshell;
+    for (int s = 0; s < ns; s++) {
+        if (c.kprim[s] < 1 || c.kprim[s] > MAXPRIM) {
+            set_error(1, "shell %d has %d primitives (1..%d supported)", s + 1, c.kprim[s], MAXPRIM);
+            return;
+        }
+        if (c.Qstart[s] < 0 || c.Qfinal[s] > 3 || c.Qfinal[s] < c.Qstart[s]) {
+            set_error(1, "shell %d has angular momentum %d..%d (s..f supported)", s + 1, c.Qstart[s], c.Qfinal[s]);
+            return;
+        }
+    }
+    // The generated kernels emit Cartesian components in QUICK's KLMN order
+    // (src/basis.f90:546-643); refuse any other order.
+    static const int order[4][10][3] = {
+        {{0, 0, 0}},
+        {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}},
+        {{2, 0, 0}, {1, 1, 0}, {0, 2, 0}, {1, 0, 1}, {0, 1, 1}, {0, 0, 2}},
+        {{3, 0, 0}, {2, 1, 0}, {1, 2, 0}, {0, 3, 0}, {2, 0, 1}, {1, 1, 1}, {0, 2, 1}, {1, 0, 2}, {0, 1, 2}, {0, 0, 3}}};
+    for (int s = 0; s < ns; s++)
+        for (int L = c.Qstart[s]; L <= c.Qfinal[s]; L++) {
+            int f0 = bf_first(c, s, L);
+            for (int k = 0; k < (L + 1) * (L + 2) / 2; k++)
+                for (int x = 0; x < 3; x++)
+                    if (c.KLMN[3 * (f0 + k) + x] != order[L][k][x]) {
+                        set_error(1, "basis function %d: Cartesian order differs from QUICK's", f0 + k + 1);
+                        return;
+                    }
+        }
+    sort_qshells(c);
+    if (c.d_cons.alloc(nb) != cudaSuccess ||
+        cudaMemcpy(c.d_cons.p, c.cons.data(), nb * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        set_error(2, "cannot upload cons");
+        return;
+    }
+    c.have_basis = true;
+    c.have_pairs = false;
+}
+
+void gpu_upload_cutoff_matrix_(double* YCutoff, double* cutPrim)
+{
+    Context& c = ctx();
+    if (require(c.have_basis, "gpu_upload_basis_ must precede gpu_upload_cutoff_matrix_")) return;
+    if (require(c.inited, "gpu_init_ must precede gpu_upload_cutoff_matrix_")) return;
+    c.YCutoff.assign(YCutoff, YCutoff + (size_t)c.nshell * c.nshell);
+    c.cutPrim.assign(cutPrim, cutPrim + (size_t)c.jbasis * c.jbasis);
+    build_pairlist(c.Qshell, c.sorted_Q.data(), c.sorted_Qnumber.data(), c.kprim.data(), c.nshell, c.YCutoff.data(), c.ref_xy,
+                   c.fStart, c.ffStart);
+    if (build_tables(c)) return;
+    g_sized_cutoff = -1.0;
+    c.have_pairs = true;
+}
+
+void gpu_upload_calculated_(double* o, double* co, double* vec, double* dense)
+{
+    (void)co;
+    (void)vec;
+    Context& c = ctx();
+    size_t nn = (size_t)c.nbasis * c.nbasis;
+    c.o_host.assign(o, o + nn);
+    c.dense_host.assign(dense, dense + nn);
+    c.have_calc = true;
+}
+
+void gpu_upload_cutoff_(double* cutMatrix, double* integralCutoff, double* primLimit, double* DMCutoff)
+{
+    (void)DMCutoff;   // never read: Fortran callers pass three arguments
+    Context& c = ctx();
+    c.integralCutoff = *integralCutoff;
+    c.primLimit = *primLimit;
+    c.DMCutoff = 1e-9;
+    c.cutMatrix.assign(cutMatrix, cutMatrix + (size_t)c.nshell * c.nshell);
+    if (c.d_cut_matrix.alloc(c.cutMatrix.size()) != cudaSuccess ||
+        cudaMemcpyAsync(c.d_cut_matrix.p, c.cutMatrix.data(), c.cutMatrix.size() * sizeof(double), cudaMemcpyHostToDevice,
+                        c.stream) != cudaSuccess) {
+        set_error(2, "cannot upload cutMatrix");
+        return;
+    }
+    c.have_cutoff = true;
+}
+
+void gpu_get2e_(double* o)
+{
+    Context& c = ctx();
+    if (require(c.have_calc, "gpu_upload_calculated_ must precede gpu_get2e_")) return;
+    size_t nn = (size_t)c.nbasis * c.nbasis;
+    if (c.d_dense_raw.alloc(nn) != cudaSuccess || c.d_o_in.alloc(nn) != cudaSuccess || c.d_o_out.alloc(nn) != cudaSuccess) {
+        set_error(2, "cannot allocate %zu-element matrices", nn);
+        return;
+    }
+    if (cudaMemcpyAsync(c.d_dense_raw.p, c.dense_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
+        cudaMemcpyAsync(c.d_o_in.p, c.o_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess) {
+        set_error(2, "upload of density / operator failed");
+        return;
+    }
+    if (fock_build(c, c.d_o_in.p, c.d_o_out.p)) return;
+    if (cudaMemcpyAsync(o, c.d_o_out.p, nn * sizeof(double), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+        cudaStreamSynchronize(c.stream) != cudaSuccess) {
+        set_error(2, "download of the operator failed");
+        return;
+    }
+}
+
+int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out)
+{
+    Context& c = ctx();
+    size_t nn = (size_t)c.nbasis * c.nbasis;
+    CK(c.d_dense_raw.alloc(nn));
+    CK(cudaMemcpyAsync(c.d_dense_raw.p, d_dense, nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    return fock_build(c, d_o_in, d_o_out);
+}
+
+int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen)
+{
+    Context& c = ctx();
+    *quartets = c.last_quartets;
+    *ms_eri = c.last_ms_eri;
+    *ms_screen = c.last_ms_screen;
+    return 0;
+}
+
+int qb_get_pairlist(int* xy, int cap, int* sorted_Q, int* sorted_Qnumber, int qcap, int* fStart, int* ffStart)
+{
+    Context& c = ctx();
+    int n = (int)c.ref_xy.size() / 2;
+    if (n > cap || c.Qshell > qcap) return -1;
+    std::copy(c.ref_xy.begin(), c.ref_xy.end(), xy);
+    std::copy(c.sorted_Q.begin(), c.sorted_Q.end(), sorted_Q);
+    std::copy(c.sorted_Qnumber.begin(), c.sorted_Qnumber.end(), sorted_Qnumber);
+    *fStart = c.fStart;
+    *ffStart = c.ffStart;
+    return n;
+}
+
+int qb_build_pairlist_host(int Qshell, const int* sorted_Q, const int* sorted_Qnumber, const int* kprim, int nshell,
+                           const double* YCutoff, int* xy_out, int cap, int* fStart, int* ffStart)
+{
+    std::vector<int> xy;
+    int n = build_pairlist(Qshell, sorted_Q, sorted_Qnumber, kprim, nshell, YCutoff, xy, *fStart, *ffStart);
+    if (n > cap) return -1;
+    std::copy(xy.begin(), xy.end(), xy_out);
+    return n;
+}
+
+void gpu_cleanup_(void)
+{
+    if (!g) return;
+    Context& c = *g;
+    c.have_basis = c.have_pairs = c.have_calc = c.have_cutoff = false;
+}
+
+void gpu_upload_grad_(double* grad, double* gradCutoff)
+{
+    (void)grad;
+    (void)gradCutoff;
+    set_error(20, "gpu_upload_grad_: gradient not available in this build yet");
+}
+void gpu_grad_(double* grad)
+{
+    (void)grad;
+    set_error(20, "gpu_grad_: gradient not available in this build yet");
+}
+void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double* belec, double* o)
+{
+    (void)isg; (void)sigrad2; (void)Eelxc; (void)aelec; (void)belec; (void)o;
+    set_error(21, "gpu_getxc_: XC quadrature not available in this build yet");
+}
+int gpu_schwarz_(double* YCutoff, double* cutPrim)
+{
+    (void)YCutoff;
+    (void)cutPrim;
+    return set_error(22, "gpu_schwarz_: not available in this build yet"), 22;
+}
+void gpu_aoint_(double* leastIntegralCutoff, double* maxIntegralCutoff, int* intNum, char* intFileName)
+{
+    (void)leastIntegralCutoff; (void)maxIntegralCutoff; (void)intNum; (void)intFileName;
+    set_error(23, "gpu_aoint_: the conventional stored-integral path is not part of this build");
+}
+void gpu_addint_(double* o, int* intindex, char* intFileName)
+{
+    (void)o; (void)intindex; (void)intFileName;
+    set_error(23, "gpu_addint_: the conventional stored-integral path is not part of this build");
+}
+
+}  // extern "C"

@@ -1,0 +1,343 @@
+"""Generate the per-class electron-repulsion kernels of the Fock build.
+
+For every angular-momentum class (LA LB | LC LD) with LA >= LB, LC >= LD and
+bra total >= ket total, this script writes straight-line CUDA for one shell
+quartet per thread:
+
+  * the Head-Gordon-Pople vertical recurrence (Obara-Saika form) producing
+    [e0|f0]^(0) for LA <= |e| <= LA+LB, LC <= |f| <= LC+LD from F_m(T),
+    emitted from a dependency walk so only intermediates that feed a target
+    are computed;
+  * contraction of those targets over the primitive quartets;
+  * the horizontal recurrence (a,b+1_i| = (a+1_i,b| + AB_i (a,b| on both
+    sides, with common sub-expressions shared;
+  * the Coulomb/exchange digestion of the (ab|cd) block into the Fock
+    matrix, bra-side Coulomb terms reduced across the warp first.
+
+This is the same algorithm QUICK's generated int.h / gpu_get2e_subs_hrr.h
+implement (gpu_get2e_subs.h:586-850), emitted by our own generator with
+register-resident intermediates instead of QUICK's local-memory `store`.
+
+Cartesian components of each shell are produced in QUICK's basis-function
+order (src/basis.f90:546-643), so component k of a sub-shell is basis
+function first+k.
+
+    python gen_eri.py OUTDIR [--lmax 2]
+"""
+import itertools
+import os
+import sys
+
+# QUICK's Cartesian order per shell (KLMN as readbasis assigns it)
+QUICK_ORDER = {
+    0: [(0, 0, 0)],
+    1: [(1, 0, 0), (0, 1, 0), (0, 0, 1)],
+    2: [(2, 0, 0), (1, 1, 0), (0, 2, 0), (1, 0, 1), (0, 1, 1), (0, 0, 2)],
+    3: [(3, 0, 0), (2, 1, 0), (1, 2, 0), (0, 3, 0), (2, 0, 1), (1, 1, 1), (0, 2, 1),
+        (1, 0, 2), (0, 1, 2), (0, 0, 3)],
+}
+AX = "xyz"
+
+
+def carts(n):
+    return [(x, y, n - x - y) for x in range(n, -1, -1) for y in range(n - x, -1, -1)]
+
+
+def nm(t):
+    return "%d%d%d" % t
+
+
+def sub(t, i, k=1):
+    l = list(t)
+    l[i] -= k
+    return tuple(l)
+
+
+def add(t, i, k=1):
+    l = list(t)
+    l[i] += k
+    return tuple(l)
+
+
+def classes(lmax):
+    """Canonical classes: LA>=LB, LC>=LD, (LA+LB,LA,LB) >= (LC+LD,LC,LD)."""
+    pairs = [(a, b) for a in range(lmax + 1) for b in range(a + 1)]
+    key = lambda p: (p[0] + p[1], p[0], p[1])
+    out = []
+    for p in pairs:
+        for q in pairs:
+            if key(p) >= key(q):
+                out.append(p + q)
+    return out
+
+
+def pair_types(lmax):
+    return sorted([(a, b) for a in range(lmax + 1) for b in range(a + 1)],
+                  key=lambda p: (p[0] + p[1], p[0], p[1]))
+
+
+class VRR:
+    """Dependency-driven emission of [e0|f0]^(m)."""
+
+    def __init__(self, prec="double"):
+        self.memo = {}
+        self.lines = []
+        self.prec = prec
+        self.nflops = 0
+
+    def get(self, e, f, m):
+        if min(e) < 0 or min(f) < 0:
+            return None
+        key = (e, f, m)
+        if key in self.memo:
+            return self.memo[key]
+        if sum(e) == 0 and sum(f) == 0:
+            name = "F%d" % m
+            self.memo[key] = name
+            return name
+        terms = []
+        if sum(f) > 0:
+            i = [k for k in range(3) if f[k] > 0][0]
+            f1 = sub(f, i)
+            a = self.get(e, f1, m)
+            b = self.get(e, f1, m + 1)
+            terms.append("QC%s*%s" % (AX[i], a))
+            terms.append("WQ%s*%s" % (AX[i], b))
+            if f1[i] > 0:
+                f2 = sub(f, i, 2)
+                c = self.get(e, f2, m)
+                d = self.get(e, f2, m + 1)
+                terms.append("%d.0*o2q*(%s - rq*%s)" % (f1[i], c, d) if f1[i] > 1 else "o2q*(%s - rq*%s)" % (c, d))
+                self.nflops += 4
+            if e[i] > 0:
+                g = self.get(sub(e, i), f1, m + 1)
+                terms.append("%s*%s" % ("%d.0*o2pq" % e[i] if e[i] > 1 else "o2pq", g))
+                self.nflops += 2
+            self.nflops += 4
+        else:
+            i = [k for k in range(3) if e[k] > 0][0]
+            e1 = sub(e, i)
+            a = self.get(e1, f, m)
+            b = self.get(e1, f, m + 1)
+            terms.append("PA%s*%s" % (AX[i], a))
+            terms.append("WP%s*%s" % (AX[i], b))
+            if e1[i] > 0:
+                e2 = sub(e, i, 2)
+                c = self.get(e2, f, m)
+                d = self.get(e2, f, m + 1)
+                terms.append("%d.0*o2p*(%s - rp*%s)" % (e1[i], c, d) if e1[i] > 1 else "o2p*(%s - rp*%s)" % (c, d))
+                self.nflops += 4
+            self.nflops += 4
+        name = "v%s_%s_%d" % (nm(e), nm(f), m)
+        self.lines.append("const %s %s = %s;" % (self.prec, name, " + ".join(terms)))
+        self.memo[key] = name
+        return name
+
+
+class HRR:
+    """(ab|cd) from contracted (e0|f0) accumulators c_<e>_<f>."""
+
+    def __init__(self):
+        self.memo = {}
+        self.lines = []
+        self.nflops = 0
+
+    def get(self, a, b, c, d):
+        key = (a, b, c, d)
+        if key in self.memo:
+            return self.memo[key]
+        if sum(d) > 0:
+            i = [k for k in range(3) if d[k] > 0][0]
+            x = self.get(a, b, add(c, i), sub(d, i))
+            y = self.get(a, b, c, sub(d, i))
+            expr = "%s + CD%s*%s" % (x, AX[i], y)
+        elif sum(b) > 0:
+            i = [k for k in range(3) if b[k] > 0][0]
+            x = self.get(add(a, i), sub(b, i), c, d)
+            y = self.get(a, sub(b, i), c, d)
+            expr = "%s + AB%s*%s" % (x, AX[i], y)
+        else:
+            name = "c_%s_%s" % (nm(a), nm(c))
+            self.memo[key] = name
+            return name
+        self.nflops += 2
+        name = "h%s_%s_%s_%s" % (nm(a), nm(b), nm(c), nm(d))
+        self.lines.append("const double %s = %s;" % (name, expr))
+        self.memo[key] = name
+        return name
+
+
+def gen_class(la, lb, lc, ld):
+    L = la + lb + lc + ld
+    tag = "%d%d%d%d" % (la, lb, lc, ld)
+    ebra = [e for n in range(la, la + lb + 1) for e in carts(n)]
+    fket = [f for n in range(lc, lc + ld + 1) for f in carts(n)]
+    vrr = VRR()
+    targets = []
+    for e in ebra:
+        for f in fket:
+            targets.append((e, f, vrr.get(e, f, 0)))
+    hrr = HRR()
+    A, B, Cc, D = QUICK_ORDER[la], QUICK_ORDER[lb], QUICK_ORDER[lc], QUICK_ORDER[ld]
+    vals = {}
+    for ia, a in enumerate(A):
+        for ib, b in enumerate(B):
+            for ic, c in enumerate(Cc):
+                for id_, d in enumerate(D):
+                    vals[(ia, ib, ic, id_)] = hrr.get(a, b, c, d)
+    na, nb, nc, nd = len(A), len(B), len(Cc), len(D)
+    o = []
+    w = o.append
+    w("// generated by gen_eri.py: class (%s %s | %s %s)" % tuple("spdf"[x] for x in (la, lb, lc, ld)))
+    w('#include "eri_common.cuh"')
+    w("namespace qb {")
+    w("template <> __device__ __forceinline__ void quartet_class<%d, %d, %d, %d>(const QuartetCtx& q, const FockParams& P)" % (la, lb, lc, ld))
+    w("{")
+    w("    constexpr int L = %d;" % L)
+    for e, f, _ in targets:
+        w("    double c_%s_%s = 0.0;" % (nm(e), nm(f)))
+    w("    for (int ib = 0; ib < q.nbra; ib++) {")
+    w("        const PrimPair pb = load_prim(P, q.bra_off + ib);")
+    w("        const double cpb = P.cut_prim[q.bra_off + ib];")
+    w("        for (int ik = 0; ik < q.nket; ik++) {")
+    w("            const double cpk = P.cut_prim[q.ket_off + ik];")
+    w("            if (!prim_survives(q, cpb, cpk, P.prim_limit)) continue;")
+    w("            const PrimPair pk = load_prim(P, q.ket_off + ik);")
+    w("            PrimQuartet s;")
+    w("            double Fm[L + 1];")
+    w("            prim_quartet<L>(pb, pk, P, s, Fm);")
+    w("            const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
+    w("            const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
+    w("            const double WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;")
+    w("            const double o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;")
+    w("            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;")
+    w("            (void)WQx; (void)WQy; (void)WQz; (void)o2p; (void)o2q; (void)o2pq; (void)rp; (void)rq;")
+    for m in range(L + 1):
+        w("            const double F%d = Fm[%d];" % (m, m))
+    for ln in vrr.lines:
+        w("            " + ln)
+    for e, f, v in targets:
+        w("            c_%s_%s += %s;" % (nm(e), nm(f), v))
+    w("        }")
+    w("    }")
+    w("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
+    w("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
+    for ln in hrr.lines:
+        w("    " + ln)
+    # ---- digestion
+    w("    // Coulomb / exchange digestion (weights and symmetry in digest_*)")
+    w("    const double* __restrict__ Dm = P.dense;")
+    w("    const int n = P.nbasis;")
+    w("    const int a0 = q.bfA, b0 = q.bfB, c0 = q.bfC, d0 = q.bfD;")
+
+    def dl(x, y):
+        return "__ldg(Dm + (size_t)(%s) * n + (%s))" % (x, y)
+    # density loads
+    for ic in range(nc):
+        for id_ in range(nd):
+            w("    const double Dcd_%d_%d = %s;" % (ic, id_, dl("c0+%d" % ic, "d0+%d" % id_)))
+    for ia in range(na):
+        for ib in range(nb):
+            w("    const double Dab_%d_%d = %s;" % (ia, ib, dl("a0+%d" % ia, "b0+%d" % ib)))
+    w("    if (P.hybrid != 0.0) {")
+    # exchange needs D_bd, D_bc, D_ad, D_ac
+    Kspec = [("ac", "bd", na, nc, nb, nd), ("ad", "bc", na, nd, nb, nc), ("bc", "ad", nb, nc, na, nd), ("bd", "ac", nb, nd, na, nc)]
+    idxmap = {"a": "ia", "b": "ib", "c": "ic", "d": "id_"}
+    bases = {"a": "a0", "b": "b0", "c": "c0", "d": "d0"}
+    sizes = {"a": na, "b": nb, "c": nc, "d": nd}
+    # load the four exchange density blocks
+    for blk in ("bd", "bc", "ad", "ac"):
+        x, y = blk
+        for i in range(sizes[x]):
+            for j in range(sizes[y]):
+                w("        const double D%s_%d_%d = %s;" % (blk, i, j, dl("%s+%d" % (bases[x], i), "%s+%d" % (bases[y], j))))
+    for out_blk, d_blk, n1, n2, m1, m2 in Kspec:
+        x, y = out_blk
+        u, v = d_blk
+        for i in range(n1):
+            for j in range(n2):
+                terms = []
+                for k in range(m1):
+                    for l in range(m2):
+                        idx = {x: i, y: j, u: k, v: l}
+                        key = (idx["a"], idx["b"], idx["c"], idx["d"])
+                        terms.append("D%s_%d_%d*%s" % (d_blk, k, l, vals[key]))
+                w("        const double K%s_%d_%d = %s;" % (out_blk, i, j, " + ".join(terms)))
+    for out_blk, _, n1, n2, _, _ in Kspec:
+        x, y = out_blk
+        for i in range(n1):
+            for j in range(n2):
+                w("        digest_exchange(P, q, %s+%d, %s+%d, K%s_%d_%d);" % (bases[x], i, bases[y], j, out_blk, i, j))
+    w("    }")
+    # Coulomb
+    for ia in range(na):
+        for ib in range(nb):
+            terms = ["Dcd_%d_%d*%s" % (ic, id_, vals[(ia, ib, ic, id_)]) for ic in range(nc) for id_ in range(nd)]
+            w("    const double Jab_%d_%d = %s;" % (ia, ib, " + ".join(terms)))
+    for ic in range(nc):
+        for id_ in range(nd):
+            terms = ["Dab_%d_%d*%s" % (ia, ib, vals[(ia, ib, ic, id_)]) for ia in range(na) for ib in range(nb)]
+            w("    const double Jcd_%d_%d = %s;" % (ic, id_, " + ".join(terms)))
+    w("    const bool bra_uniform = warp_bra_uniform(q);")
+    for ia in range(na):
+        for ib in range(nb):
+            w("    digest_coulomb_bra(P, q, a0+%d, b0+%d, Jab_%d_%d, bra_uniform);" % (ia, ib, ia, ib))
+    for ic in range(nc):
+        for id_ in range(nd):
+            w("    digest_coulomb(P, q, c0+%d, d0+%d, Jcd_%d_%d);" % (ic, id_, ic, id_))
+    w("}")
+    w("void launch_%s(const FockParams& P, int cls, int grid, int block, cudaStream_t st)" % tag)
+    w("{")
+    w("    auto kern = fock_class_kernel<%d, %d, %d, %d>;" % (la, lb, lc, ld))
+    w("    QB_LAUNCH(kern, grid, block, 0, st, P, cls);")
+    w("}")
+    w("}  // namespace qb")
+    stats = dict(vrr_flops=vrr.nflops, vrr_nodes=len(vrr.lines), hrr_flops=hrr.nflops, targets=len(targets),
+                 ncomp=na * nb * nc * nd)
+    return "\n".join(o) + "\n", stats
+
+
+def main(outdir, lmax=2):
+    os.makedirs(outdir, exist_ok=True)
+    cls = classes(lmax)
+    lines = ["// generated by gen_eri.py", "#pragma once", "namespace qb {",
+             "static const int kNumClasses = %d;" % len(cls),
+             "static const int kClassL[%d][4] = {%s};" % (len(cls), ", ".join("{%d,%d,%d,%d}" % c for c in cls)),
+             "static const int kNumPairTypes = %d;" % len(pair_types(lmax)),
+             "static const int kPairTypeL[%d][2] = {%s};" % (len(pair_types(lmax)), ", ".join("{%d,%d}" % p for p in pair_types(lmax))),
+             "}"]
+    with open(os.path.join(outdir, "eri_classes.h"), "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    stats = {}
+    for c in cls:
+        src, st = gen_class(*c)
+        stats[c] = st
+        path = os.path.join(outdir, "eri_%d%d%d%d.cu" % c)
+        old = open(path).read() if os.path.exists(path) else None
+        if old != src:
+            with open(path, "w") as fh:
+                fh.write(src)
+    # launch table
+    lt = ['#include "eri_common.cuh"', '#include "eri_classes.h"', "namespace qb {"]
+    for c in cls:
+        lt.append("void launch_%d%d%d%d(const FockParams& P, int cls, int grid, int block, cudaStream_t st);" % c)
+    lt += ["void launch_class(int cls, const FockParams& P, int grid, int block, cudaStream_t st)", "{",
+           "    switch (cls) {"]
+    for k, c in enumerate(cls):
+        lt.append("    case %d: launch_%d%d%d%d(P, %d, grid, block, st); break;" % ((k,) + c + (k,)))
+    lt += ["    default: break;", "    }", "}", "}  // namespace qb"]
+    with open(os.path.join(outdir, "eri_launch.cu"), "w") as fh:
+        fh.write("\n".join(lt) + "\n")
+    return stats
+
+
+if __name__ == "__main__":
+    lmax = 2
+    args = [a for a in sys.argv[1:]]
+    if "--lmax" in args:
+        k = args.index("--lmax")
+        lmax = int(args[k + 1])
+        del args[k:k + 2]
+    st = main(args[0] if args else "gen", lmax)
+    for c, s in st.items():
+        print(c, s)

@@ -1,0 +1,119 @@
+// Quartet screening: builds, per angular-momentum class, the list of shell
+// quartets that pass QUICK's Schwarz and density tests
+// (gpu_get2e_subs.h:311-328), grouped by bra pair.  Replaces QUICK's dense
+// walk over all sqrQshell^2 pair-pairs with a sorted, early-exit scan.
+#include "eri_common.cuh"
+#include "qb_internal.h"
+
+namespace qb {
+
+// One warp per (class, bra pair).  Kets of the class's ket type are sorted
+// by Schwarz bound, descending, so the scan stops at the first ket whose
+// bound product fails.  count_only: Schwarz test only, just count (used once
+// per geometry to size the lists).
+__global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const FockParams P, int count_only)
+{
+    const int cls = blockIdx.y;
+    const ScreenClass c = S.cls[cls];
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const double cut = P.integral_cutoff;
+    for (int a = c.bra_begin + warp; a < c.bra_end; a += nwarps) {
+        const double Ya = P.pair_Y[a];
+        const int4 sa = P.pair_sh[a];
+        const int kb = c.same_type ? a : c.ket_begin;
+        for (int k0 = kb; k0 < c.ket_end; k0 += 32) {
+            if (!(P.pair_Y[k0] * Ya > cut)) break;      // sorted: the rest fail too
+            const int b = k0 + lane;
+            bool pass = false;
+            if (b < c.ket_end) {
+                const double yy = P.pair_Y[b] * Ya;
+                if (yy > cut) {
+                    if (count_only) {
+                        pass = true;
+                    } else {
+                        const int4 sb = P.pair_sh[b];
+                        const double dn = dn_max(P, sa.x, sa.y, sb.x, sb.y);
+                        pass = yy * dn > cut;
+                    }
+                }
+            }
+            const unsigned m = __ballot_sync(FULL, pass);
+            if (m == 0) continue;
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(S.counts + cls, (unsigned long long)__popc(m));
+            base = __shfl_sync(FULL, base, 0);
+            if (!count_only && pass) {
+                const unsigned long long pos = base + __popc(m & ((1u << lane) - 1u));
+                if (pos < (unsigned long long)c.capacity)
+                    S.out[c.out_offset + pos] = make_int2(a, b);
+            }
+        }
+    }
+}
+
+// Clamp counters to capacities and publish them as int for the class kernels.
+__global__ void finish_counts_kernel(const ScreenParams S, int* class_count, int* overflow, int ncls)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ncls) {
+        unsigned long long n = S.counts[c];
+        if (n > (unsigned long long)S.cls[c].capacity) {
+            atomicExch(overflow, 1);
+            n = S.cls[c].capacity;
+        }
+        class_count[c] = (int)n;
+    }
+}
+
+// QUICK scales every Cartesian component by cons() inside its horizontal
+// recurrence (gpu_get2e_subs_hrr.h:42).  Here the scaling is folded into the
+// density going in, D'(k,l) = cons(k) cons(l) D(k,l), and into the Fock
+// matrix coming out, which costs nothing inside the class kernels.
+__global__ void scale_density_kernel(const double* __restrict__ D, const double* __restrict__ cons,
+                                     double* __restrict__ Ds, int n)
+{
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < (size_t)n * n) {
+        const int i = (int)(idx % n), j = (int)(idx / n);
+        Ds[idx] = D[idx] * cons[i] * cons[j];
+    }
+}
+
+// O_out(i,j) = O_in(i,j) + cons(i) cons(j) G(max(i,j), min(i,j)), column-major, symmetric.
+__global__ void fock_finish_kernel(const double* __restrict__ G, const double* __restrict__ cons,
+                                   const double* __restrict__ Oin, double* __restrict__ Oout, int n)
+{
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < (size_t)n * n) {
+        const int i = (int)(idx % n), j = (int)(idx / n);
+        const int hi = i > j ? i : j, lo = i > j ? j : i;
+        Oout[idx] = Oin[idx] + cons[i] * cons[j] * G[(size_t)hi * n + lo];
+    }
+}
+
+void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int count_only, int nsm, cudaStream_t st)
+{
+    dim3 grid(nsm * 4, ncls);
+    QB_LAUNCH(screen_kernel, grid, 256, 0, st, S, P, count_only);
+}
+
+void launch_finish_counts(const ScreenParams& S, int* class_count, int* overflow, int ncls, cudaStream_t st)
+{
+    QB_LAUNCH(finish_counts_kernel, (ncls + 63) / 64, 64, 0, st, S, class_count, overflow, ncls);
+}
+
+void launch_scale_density(const double* D, const double* cons, double* Ds, int n, cudaStream_t st)
+{
+    const size_t N = (size_t)n * n;
+    QB_LAUNCH(scale_density_kernel, (unsigned)((N + 255) / 256), 256, 0, st, D, cons, Ds, n);
+}
+
+void launch_fock_finish(const double* G, const double* cons, const double* Oin, double* Oout, int n, cudaStream_t st)
+{
+    const size_t N = (size_t)n * n;
+    QB_LAUNCH(fock_finish_kernel, (unsigned)((N + 255) / 256), 256, 0, st, G, cons, Oin, Oout, n);
+}
+
+}  // namespace qb

@@ -1,0 +1,58 @@
+"""GPU Fock build against the CPU oracle (which is itself pinned to QUICK's
+own kernels, tests/test_oracle_ref.py).  Tolerance: 1e-8 on Fock elements."""
+import numpy as np
+import pytest
+
+from tests.helpers import CASES, case, random_density
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-8
+
+
+@pytest.fixture(scope="module")
+def session():
+    from quick_b200 import capi
+    s = capi.Session(0)
+    yield s
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("method", [0, 1])
+def test_fock_matches_oracle(session, oracle_lib, name, method):
+    oracle = oracle_lib
+    m, b = case(name)
+    Y, cp = oracle.schwarz(b, m.xyz_bohr)
+    session.upload_molecule(m, b, Y, cp)
+    D = random_density(b.nbasis, seed=7)
+    cm = oracle.cutmatrix(b, D)
+    H = random_density(b.nbasis, seed=8, scale=0.3)
+    hyb = {0: 1.0, 1: 0.2, 2: 0.0}[method]
+    ref, cnt = oracle.fock(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20, hybrid=hyb, O=H)
+    got = session.get2e(H, D, cm, 1e-10, 1e-20, method=method)
+    err = np.abs(got - ref).max()
+    assert err < TOL, (name, err)
+    assert np.array_equal(got, got.T)
+
+
+def test_pairlist_matches_host(session, oracle_lib):
+    from quick_b200 import capi
+    m, b = case("water3_631gss")
+    Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
+    session.upload_molecule(m, b, Y, cp)
+    dev = session.pairlist()
+    host = capi.build_pairlist_host(b, Y)
+    assert np.array_equal(dev["pairs"], host["pairs"])
+    assert (dev["fStart"], dev["ffStart"]) == (host["fStart"], host["ffStart"])
+
+
+def test_repeated_builds_reuse_buffers(session, oracle_lib):
+    m, b = case("water2_631gs")
+    Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
+    session.upload_molecule(m, b, Y, cp)
+    for seed in range(3):
+        D = random_density(b.nbasis, seed=seed)
+        cm = oracle_lib.cutmatrix(b, D)
+        ref, _ = oracle_lib.fock(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
+        got = session.get2e(np.zeros_like(D), D, cm, 1e-10, 1e-20)
+        assert np.abs(got - ref).max() < TOL
