@@ -1,0 +1,351 @@
+"""Fock-build throughput of QUICK's direct-SCF two-electron path on B200.
+
+One step = one two-electron Fock build G(D) of the workload molecule
+(QUICK's gpu_get2e_: screening, all angular classes, O + G), inputs resident
+in HBM.  Metric: shell quartets per second, a shell quartet being one
+(IJ|KL) block of unique integrals over angular sub-shells that passes QUICK's
+Schwarz and density screens.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+The default workload is (H2O)32 in 6-31G** (800 Cartesian basis functions),
+seeded geometry, CUTOFF=1e-10 semantics (integral cutoff 1e-10, primitive
+limit 1e-20).  For N > 1 every rank builds the Fock matrix of its own replica
+(weak scaling, no collective on the data path); the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="(H2O)32 6-31G** RHF Fock build", grid=(4, 4, 2), basis="6-31G**", seed=0,
+                integral_cutoff=1e-10, prim_limit=1e-20)
+SAMPLE = dict(name="(H2O)16 6-31G** RHF Fock build", grid=(4, 2, 2), basis="6-31G**", seed=0)
+
+
+def model_density(mol, basis, seed=0):
+    """A symmetric density with the magnitude structure of a real one:
+    |D_ij| ~ 0.5 exp(-R_ij / 1.5 bohr) between the centres of functions i and
+    j, random signs, unit diagonal.  Seeded; used where no SCF density exists."""
+    rng = np.random.default_rng(seed)
+    xyz = mol.xyz_bohr.T
+    c = xyz[basis.ncenter - 1]
+    R = np.linalg.norm(c[:, None, :] - c[None, :, :], axis=-1)
+    u = rng.uniform(-1.0, 1.0, R.shape)
+    u = 0.5 * (u + u.T)
+    D = 0.5 * np.exp(-R / 1.5) * u
+    np.fill_diagonal(D, 1.0)
+    return np.asfortranarray(D)
+
+
+def shell_cut_matrix(basis, D):
+    """QUICK's density screen cutMatrix(II,JJ) = max |D| over the shell-pair
+    block (src/schwarz.f90:550-599), vectorised."""
+    first = basis.Ksumtype[:-1] - 1
+    last = basis.Ksumtype[1:] - 1
+    A = np.abs(D)
+    rowmax = np.stack([A[f:l].max(axis=0) for f, l in zip(first, last)])   # (nshell, nbasis)
+    cm = np.stack([rowmax[:, f:l].max(axis=1) for f, l in zip(first, last)], axis=1)
+    return np.asfortranarray(np.maximum(cm, cm.T))
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        self.p.wait()
+        rows = []
+        with open(self.f.name) as fh:
+            for ln in fh:
+                t = [x.strip() for x in ln.split(",")]
+                if len(t) >= 9:
+                    rows.append(t)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        num = lambda s: s.replace(".", "", 1).isdigit()
+        sm = [float(r[1]) for r in rows if num(r[1])]
+        mx = [float(r[2]) for r in rows if num(r[2])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def unique_quartets(b, Y, cm, cutoff):
+    """Unique shell quartets of the metric's unit (see module docstring),
+    counted on the host from QUICK's pair list and QUICK's two screens."""
+    from quick_b200 import capi
+    pl = capi.build_pairlist_host(b, Y)
+    sq, sqn = pl["sorted_Q"], pl["sorted_Qnumber"]
+    keep = []
+    for x, y in pl["pairs"]:
+        if sq[x] == sq[y] and x != y and sqn[x] > sqn[y]:
+            continue
+        keep.append((sq[x], sq[y]))
+    keep = np.array(keep)
+    Yp = Y[keep[:, 0], keep[:, 1]]
+    n = len(keep)
+    tot = 0
+    for a in range(n):
+        yy = Yp[a:] * Yp[a]
+        i, j = keep[a]
+        k, l = keep[a:, 0], keep[a:, 1]
+        dn = np.maximum.reduce([np.full(n - a, 4 * cm[i, j]), 4 * cm[k, l], cm[i, l], cm[i, k], cm[j, k], cm[j, l]])
+        tot += int(np.count_nonzero((yy > cutoff) & (yy * dn > cutoff)))
+    return tot
+
+
+def cpu_reference(threads, steps=1, warmup=0):
+    """QUICK's own two-electron kernel (src/cuda/gpu_get2e_subs.h, driven by
+    QUICK's src/cuda/gpu.cu bridge) compiled for the host cores, on a bounded
+    sample of the workload.  Returns (quartets/s, quartets per step, s/step)."""
+    import oracle
+    from quick_b200.basis import build_basis
+    from quick_b200.molecule import water_cluster
+    m = water_cluster(SAMPLE["grid"], seed=SAMPLE["seed"])
+    b = build_basis(m.symbols, SAMPLE["basis"])
+    Y, cp = oracle.schwarz(b, m.xyz_bohr)
+    D = model_density(m, b)
+    cm = shell_cut_matrix(b, D)
+    nq = unique_quartets(b, Y, cm, WORKLOAD["integral_cutoff"])
+    oracle.ref_upload_molecule(m, b, Y, cp, threads=threads)
+    Z = np.zeros_like(D)
+    for _ in range(warmup):
+        oracle.ref_get2e(Z, D, cm, WORKLOAD["integral_cutoff"], WORKLOAD["prim_limit"])
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        oracle.ref_get2e(Z, D, cm, WORKLOAD["integral_cutoff"], WORKLOAD["prim_limit"])
+        ts.append(time.perf_counter() - t0)
+    return nq / np.mean(ts), nq, float(np.mean(ts))
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from quick_b200 import capi, flops
+    from quick_b200.basis import build_basis
+    from quick_b200.molecule import water_cluster
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    m = water_cluster(WORKLOAD["grid"], seed=WORKLOAD["seed"])
+    b = build_basis(m.symbols, WORKLOAD["basis"])
+    n = b.nbasis
+    sess = capi.Session(local)
+    lib = capi.lib()
+    lib.qb_set_stream(capi.C.c_void_p(stream.cuda_stream))
+    sess.upload_molecule(m, b)          # Schwarz bounds from the GPU kernel
+    D = model_density(m, b, seed=WORKLOAD["seed"])
+    cm = shell_cut_matrix(b, D)
+    cutoff, plim = WORKLOAD["integral_cutoff"], WORKLOAD["prim_limit"]
+    O0 = np.zeros((n, n), order="F")
+    sess.get2e(O0, D, cm, cutoff, plim, method=0)    # uploads cutoffs, sizes the quartet lists
+    dD = torch.from_numpy(np.ascontiguousarray(D)).to(dev)
+    dO = torch.zeros((n, n), dtype=torch.float64, device=dev)
+    dOut = torch.empty_like(dO)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+    def step():
+        rc = lib.qb_fock_device(capi.C.c_void_p(dD.data_ptr()), capi.C.c_void_p(dO.data_ptr()),
+                                capi.C.c_void_p(dOut.data_ptr()))
+        if rc:
+            capi.check()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    quartets = sess.fock_stats()["quartets"]
+    ncls = capi.C.c_int(0)
+    cl = np.zeros(4 * 128, dtype=np.int32)
+    cq = np.zeros(128, dtype=np.int64)
+    lib.qb_class_info(capi.C.byref(ncls), capi._ptr(cl), capi._ptr(cq), 128)
+    npq = np.zeros(128, dtype=np.int64)
+    lib.qb_count_prim_quartets(capi._ptr(npq), 128)
+    capi.check()
+    k = ncls.value
+    alg_flops = flops.fock_flops(cl[:4 * k].reshape(k, 4), cq[:k], npq[:k], exchange=True)
+    peak64 = capi.C.c_double(0)
+    lib.qb_fma_peak(1, capi.C.byref(peak64))
+
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = Clocks(local) if rank == 0 else None
+    l0 = lib.qb_launch_count()
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    eri_ms, scr_ms = [], []
+    for i in range(args.steps):
+        flush.zero_()
+        e0[i].record(stream)
+        step()
+        e1[i].record(stream)
+        s = sess.fock_stats()
+        eri_ms.append(s["ms_eri"])
+        scr_ms.append(s["ms_screen"])
+    torch.cuda.synchronize()
+    barrier(ws)
+    launches = lib.qb_launch_count() - l0
+    step_ms = [a.elapsed_time(b_) for a, b_ in zip(e0, e1)]
+    ms = max_over_ranks(float(np.mean(step_ms)), ws)
+    clk = clocks.stop() if clocks else None
+
+    # end to end through QUICK's C ABI with pinned host buffers: upload D, O and
+    # cutMatrix, Fock build, download O, every step
+    pinD = torch.from_numpy(np.asfortranarray(D).ravel(order="F").copy()).pin_memory()
+    pinO = torch.zeros(n * n, dtype=torch.float64).pin_memory()
+    pinCM = torch.from_numpy(np.asfortranarray(cm).ravel(order="F").copy()).pin_memory()
+    ptr = lambda t: capi.C.c_void_p(t.data_ptr())
+    one = capi.C.byref
+    co = torch.zeros(1, dtype=torch.float64)
+    ec0, ec1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    ec0.record(stream)
+    for i in range(args.steps):
+        pinO.zero_()
+        lib.gpu_upload_method_(one(capi.C.c_int(0)))
+        lib.gpu_upload_calculated_(ptr(pinO), ptr(co), ptr(co), ptr(pinD))
+        lib.gpu_upload_cutoff_(ptr(pinCM), one(capi.C.c_double(cutoff)), one(capi.C.c_double(plim)), None)
+        lib.gpu_get2e_(ptr(pinO))
+    ec1.record(stream)
+    torch.cuda.synchronize()
+    capi.check()
+    e2e_ms = max_over_ranks(ec0.elapsed_time(ec1) / args.steps, ws)
+
+    mean_eri = float(np.mean(eri_ms))
+    achieved = alg_flops / (mean_eri * 1e-3) / 1e12
+    peak = peak64.value / 1e3
+    out = {
+        "metric": "Fock-build shell quartets/s (FP64)",
+        "value": quartets * ws / (ms * 1e-3),
+        "unit": "quartets/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: seeded (H2O)32 geometry, model density",
+        "config": {"workload": WORKLOAD["name"], "nbasis": n, "quartets_per_step": quartets,
+                   "integral_cutoff": cutoff, "prim_limit": plim, "method": "HF (full exchange)",
+                   "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas"},
+        "e2e": {"value": quartets * ws / (e2e_ms * 1e-3), "unit": "quartets/s",
+                "h2d_bytes_per_step": int(2 * n * n * 8 + b.nshell ** 2 * 8),
+                "d2h_bytes_per_step": int(n * n * 8), "ms_per_step": e2e_ms},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "kernel": "fock_class_kernel<LA,LB,LC,LD> (all classes of one build)",
+                     "peak_source": "measured: FP64 FMA-chain probe run in this process (qb_fma_peak)",
+                     "flops_per_step": alg_flops, "kernel_ms": mean_eri,
+                     "screen_ms": float(np.mean(scr_ms))},
+        "gpu_launches": int(launches),
+    }
+    if clk:
+        out["clocks"] = clk
+    if args.classes:
+        out["classes"] = {"%d%d%d%d" % tuple(cl[4 * i:4 * i + 4]): [int(cq[i]), int(npq[i])] for i in range(k)}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--classes", action="store_true", help="add per-class quartet counts")
+    args = ap.parse_args()
+    ws, rank, local = dist_setup()
+    threads = os.cpu_count() or 1
+    if args.impl == "reference":
+        if rank == 0:
+            qps, nq, sec = cpu_reference(threads, steps=args.steps, warmup=args.warmup)
+            sample = ("%s, %d quartets per step; QUICK's gpu_get2e_subs.h kernel and gpu.cu bridge "
+                      "compiled for the host cores" % (SAMPLE["name"], nq))
+            out = {"impl": "reference", "metric": "Fock-build shell quartets/s (FP64)", "value": qps,
+                   "unit": "quartets/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                   "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                   "dtype": "f64", "data": "synthetic: seeded water cluster, model density",
+                   "config": {"workload": WORKLOAD["name"], "sample": SAMPLE["name"]},
+                   "cpu_baseline": {"value": qps, "unit": "quartets/s", "cores": threads, "kind": "reference",
+                                    "sample": sample},
+                   "e2e": {"value": qps, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(out))
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    out = run_ours(args, ws, rank, local)
+    if rank == 0 and not args.no_cpu_baseline:
+        qps, nq, sec = cpu_reference(threads)
+        out["cpu_baseline"] = {"value": qps, "unit": "quartets/s", "cores": threads, "kind": "reference",
+                               "sample": "one Fock build of %s (%d quartets, %.2f s); QUICK's gpu_get2e_subs.h "
+                                         "kernel and gpu.cu bridge compiled for the host cores" % (
+                                             SAMPLE["name"], nq, sec)}
+    if rank == 0:
+        print(json.dumps(out))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -104,9 +104,24 @@ int gpu_schwarz_(double* YCutoff, double* cutPrim);
    pointers, may alias).  Uses the cutoffs and density screen from the last gpu_upload_cutoff_. */
 int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out);
 
-/* Statistics of the last Fock build: shell quartets (QUICK's iclass-call count),
-   device time of the class kernels in ms, device time of the screening in ms. */
+/* Statistics of the last Fock build: unique shell quartets evaluated (one per unordered pair of
+   kept shell pairs that passes QUICK's Schwarz and density tests), device time of the class
+   kernels in ms, device time of the screening in ms. */
 int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen);
+
+/* Measured FMA throughput of this GPU in GFLOP/s (FP64 if fp64 != 0, else FP32): a
+   register-resident FMA chain over 8 blocks per SM, best of 4 timed runs. */
+int qb_fma_peak(int fp64, double* gflops);
+
+/* Per angular-momentum class of the last Fock build: the number of primitive quartets that
+   passed the primitive screen (cap >= number of classes). */
+int qb_count_prim_quartets(long long* per_class, int cap);
+
+/* Number of kernels this library has launched since it was loaded. */
+long long qb_launch_count(void);
+
+/* Classes of this build: their (LA, LB, LC, LD) and the shell quartets of the last build. */
+int qb_class_info(int* nclasses, int* class_L, long long* class_quartets, int cap);
 
 #ifdef __cplusplus
 }

@@ -21,6 +21,7 @@
 #include "../../include/quick_b200.h"
 #include "gen/eri_classes.h"
 #include "qb_internal.h"
+#include "schwarz.cuh"
 
 namespace qb {
 
@@ -96,6 +97,7 @@ struct Context {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
+unsigned long long g_launches = 0;   // kernels launched by this library
 static Context* g = nullptr;
 static int g_status = 0;
 static std::string g_err;
@@ -817,9 +819,143 @@ void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double*
 }
 int gpu_schwarz_(double* YCutoff, double* cutPrim)
 {
-    (void)YCutoff;
-    (void)cutPrim;
-    return set_error(22, "gpu_schwarz_: not available in this build yet"), 22;
+    Context& c = ctx();
+    if (require(c.inited, "gpu_init_ must precede gpu_schwarz_")) return 1;
+    if (require(c.have_basis && !c.xyz.empty(), "basis and coordinates must be uploaded before gpu_schwarz_")) return 1;
+    struct Rec {
+        int type, s1, s2, shA, LA, shB, LB;
+        bool swapped;
+    };
+    std::vector<Rec> recs;
+    for (int s1 = 0; s1 < c.nshell; s1++)
+        for (int s2 = s1; s2 < c.nshell; s2++)
+            for (int L1 = c.Qstart[s1]; L1 <= c.Qfinal[s1]; L1++)
+                for (int L2 = c.Qstart[s2]; L2 <= c.Qfinal[s2]; L2++) {
+                    Rec r{0, s1, s2, s1, L1, s2, L2, false};
+                    if (L1 < L2) { r.shA = s2; r.LA = L2; r.shB = s1; r.LB = L1; r.swapped = true; }
+                    r.type = pair_type_index(r.LA, r.LB);
+                    if (r.type < 0) return set_error(1, "angular momentum (%d,%d) beyond this build", r.LA, r.LB), 1;
+                    recs.push_back(r);
+                }
+    std::stable_sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) { return a.type < b.type; });
+    int nrec = (int)recs.size();
+    std::vector<int4> pbf(nrec);
+    std::vector<double4> pAB(nrec), prim;
+    std::vector<int> tbeg(kNumPairTypes, 0), tend(kNumPairTypes, 0);
+    for (int i = 0; i < nrec; i++) {
+        const Rec& e = recs[i];
+        const double *A = center(c, e.shA), *B = center(c, e.shB);
+        double AB2 = 0;
+        for (int k = 0; k < 3; k++) AB2 += (A[k] - B[k]) * (A[k] - B[k]);
+        int off = (int)prim.size() / 2;
+        for (int pa = 0; pa < c.kprim[e.shA]; pa++)
+            for (int pb = 0; pb < c.kprim[e.shB]; pb++) {
+                double a = cexpo(c, e.shA, pa), bb = cexpo(c, e.shB, pb), p = a + bb;
+                double K = X0 * (exp(-a * bb / p * AB2) / p) * ccoef(c, e.shA, e.LA, pa) * ccoef(c, e.shB, e.LB, pb);
+                double P[3], PA[3];
+                for (int k = 0; k < 3; k++) {
+                    P[k] = (A[k] * a + B[k] * bb) / p;
+                    PA[k] = P[k] - A[k];
+                }
+                prim.push_back(make_double4(p, K, P[0], P[1]));
+                prim.push_back(make_double4(P[2], PA[0], PA[1], PA[2]));
+            }
+        pbf[i] = make_int4(bf_first(c, e.shA, e.LA), bf_first(c, e.shB, e.LB), off, (int)prim.size() / 2 - off);
+        pAB[i] = make_double4(A[0] - B[0], A[1] - B[1], A[2] - B[2], 1.0);
+        if (i == 0 || recs[i - 1].type != e.type) tbeg[e.type] = i;
+        tend[e.type] = i + 1;
+    }
+    int nprimpair = (int)prim.size() / 2;
+    DevBuf<double4> d_prim, d_ab;
+    DevBuf<int4> d_bf;
+    DevBuf<double> d_oc, d_op;
+    CK(d_prim.alloc(prim.size()));
+    CK(d_ab.alloc(nrec));
+    CK(d_bf.alloc(nrec));
+    CK(d_oc.alloc(nrec));
+    CK(d_op.alloc(nprimpair));
+    CK(cudaMemcpy(d_prim.p, prim.data(), prim.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_ab.p, pAB.data(), nrec * sizeof(double4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_bf.p, pbf.data(), nrec * sizeof(int4), cudaMemcpyHostToDevice));
+    SchwarzParams S{d_prim.p, d_bf.p, d_ab.p, c.d_cons.p, c.d_boys.p, d_oc.p, d_op.p};
+    for (int t = 0; t < kNumPairTypes; t++) {
+        if (tend[t] <= tbeg[t]) continue;
+        int n = tend[t] - tbeg[t];
+        launch_schwarz(t, S, tbeg[t], tend[t], 0, std::min((n + 127) / 128, c.nsm * 8), 128, c.stream);
+        int np = pbf[tend[t] - 1].z + pbf[tend[t] - 1].w - pbf[tbeg[t]].z;
+        launch_schwarz(t, S, tbeg[t], tend[t], 1, std::min((np + 127) / 128, c.nsm * 8), 128, c.stream);
+    }
+    CK(cudaGetLastError());
+    std::vector<double> oc(nrec), op(nprimpair);
+    CK(cudaMemcpyAsync(oc.data(), d_oc.p, nrec * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(op.data(), d_op.p, nprimpair * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    d_prim.release(); d_ab.release(); d_bf.release(); d_oc.release(); d_op.release();
+    int ns = c.nshell;
+    std::vector<double> ymax((size_t)ns * ns, 0.0), pmax((size_t)c.jbasis * c.jbasis, 0.0);
+    for (int i = 0; i < nrec; i++) {
+        const Rec& e = recs[i];
+        double& y = ymax[(size_t)e.s1 + (size_t)e.s2 * ns];
+        y = std::max(y, oc[i]);
+        int k = 0;
+        for (int pa = 0; pa < c.kprim[e.shA]; pa++)
+            for (int pb = 0; pb < c.kprim[e.shB]; pb++, k++) {
+                int p1 = e.swapped ? pb : pa, p2 = e.swapped ? pa : pb;
+                double& v = pmax[(size_t)(c.kstart[e.s1] - 1 + p1) + (size_t)(c.kstart[e.s2] - 1 + p2) * c.jbasis];
+                v = std::max(v, op[pbf[i].z + k]);
+            }
+    }
+    // cutPrim carries QUICK's extra factor X0 = 2 pi^2.5 (schwarz.f90:417)
+    const double X0F = 2.0 * pow(3.1415926535897932384626433832795, 2.5);
+    for (int s1 = 0; s1 < ns; s1++)
+        for (int s2 = s1; s2 < ns; s2++) {
+            double v = sqrt(ymax[(size_t)s1 + (size_t)s2 * ns]);
+            YCutoff[(size_t)s1 + (size_t)s2 * ns] = v;
+            YCutoff[(size_t)s2 + (size_t)s1 * ns] = v;
+        }
+    for (size_t k = 0; k < pmax.size(); k++) cutPrim[k] = sqrt(pmax[k] * X0F);
+    return 0;
+}
+
+long long qb_launch_count(void) { return (long long)g_launches; }
+
+int qb_fma_peak(int fp64, double* gflops)
+{
+    Context& c = ctx();
+    if (require(c.inited, "gpu_init_ must precede qb_fma_peak")) return 1;
+    return fma_probe(fp64, c.nsm, gflops, c.stream);
+}
+
+int qb_count_prim_quartets(long long* per_class, int cap)
+{
+    Context& c = ctx();
+    if (require(c.have_pairs && c.d_quartets.p != nullptr, "a Fock build must precede qb_count_prim_quartets")) return 1;
+    if (cap < kNumClasses) return set_error(1, "per_class needs %d entries", kNumClasses), 1;
+    DevBuf<unsigned long long> d;
+    CK(d.alloc(kNumClasses));
+    CK(cudaMemsetAsync(d.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
+    FockParams P = fock_params(c);
+    launch_count_prims(P, kNumClasses, d.p, c.nsm, c.stream);
+    CK(cudaGetLastError());
+    std::vector<unsigned long long> h(kNumClasses);
+    CK(cudaMemcpyAsync(h.data(), d.p, kNumClasses * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    for (int k = 0; k < kNumClasses; k++) per_class[k] = (long long)h[k];
+    return 0;
+}
+
+int qb_class_info(int* nclasses, int* class_L, long long* class_quartets, int cap)
+{
+    Context& c = ctx();
+    *nclasses = kNumClasses;
+    if (cap < kNumClasses) return 1;
+    std::vector<int> cnt(kNumClasses, 0);
+    if (c.d_class_count.p) CK(cudaMemcpy(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < kNumClasses; k++) {
+        for (int j = 0; j < 4; j++) class_L[4 * k + j] = kClassL[k][j];
+        class_quartets[k] = cnt[k];
+    }
+    return 0;
 }
 void gpu_aoint_(double* leastIntegralCutoff, double* maxIntegralCutoff, int* intNum, char* intFileName)
 {

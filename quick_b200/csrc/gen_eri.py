@@ -297,6 +297,86 @@ def gen_class(la, lb, lc, ld):
     return "\n".join(o) + "\n", stats
 
 
+def gen_schwarz(la, lb):
+    """Diagonal (ab|ab) blocks for QUICK's Schwarz bounds (schwarz.f90:46-548):
+    max over components of |(ab|ab)| cons(a)^2 cons(b)^2, either contracted
+    (mode 0, one thread per shell pair) or for a single primitive pair on both
+    sides (mode 1, one thread per primitive pair)."""
+    L = 2 * (la + lb)
+    tag = "%d%d" % (la, lb)
+    ebra = [e for n in range(la, la + lb + 1) for e in carts(n)]
+    vrr = VRR()
+    targets = []
+    for e in ebra:
+        for f in ebra:
+            targets.append((e, f, vrr.get(e, f, 0)))
+    hrr = HRR()
+    A, B = QUICK_ORDER[la], QUICK_ORDER[lb]
+    diag = []
+    for ia, a in enumerate(A):
+        for ib, b in enumerate(B):
+            diag.append((ia, ib, hrr.get(a, b, a, b)))
+    o = []
+    w = o.append
+    w("// generated by gen_eri.py: Schwarz diagonal (%s %s | %s %s)" % tuple("spdf"[x] for x in (la, lb, la, lb)))
+    w('#include "eri_common.cuh"')
+    w('#include "schwarz.cuh"')
+    w("namespace qb {")
+    w("template <> __device__ __forceinline__ double schwarz_diag<%d, %d>(const SchwarzParams& S, int rec, int p0, int np)" % (la, lb))
+    w("{")
+    w("    constexpr int L = %d;" % L)
+    w("    const int4 info = S.pair_bf[rec];")
+    w("    const double4 ab = S.pair_AB[rec];")
+    w("    FockParams P;")
+    w("    P.boys = S.boys;")
+    for e, f, _ in targets:
+        w("    double c_%s_%s = 0.0;" % (nm(e), nm(f)))
+    w("    for (int ib = p0; ib < p0 + np; ib++) {")
+    w("        const PrimPair pb = load_prim_s(S, info.z + ib);")
+    w("        for (int ik = p0; ik < p0 + np; ik++) {")
+    w("            const PrimPair pk = load_prim_s(S, info.z + ik);")
+    w("            PrimQuartet s;")
+    w("            double Fm[L + 1];")
+    w("            prim_quartet<L>(pb, pk, P, s, Fm);")
+    w("            const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
+    w("            const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
+    w("            const double WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;")
+    w("            const double o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;")
+    w("            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;")
+    w("            (void)WQx; (void)WQy; (void)WQz; (void)o2p; (void)o2q; (void)o2pq; (void)rp; (void)rq;")
+    for m in range(L + 1):
+        w("            const double F%d = Fm[%d];" % (m, m))
+    for ln in vrr.lines:
+        w("            " + ln)
+    for e, f, v in targets:
+        w("            c_%s_%s += %s;" % (nm(e), nm(f), v))
+    w("        }")
+    w("    }")
+    w("    const double ABx = ab.x, ABy = ab.y, ABz = ab.z, CDx = ab.x, CDy = ab.y, CDz = ab.z;")
+    w("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
+    for ln in hrr.lines:
+        w("    " + ln)
+    w("    double m = 0.0;")
+    for ia, ib, v in diag:
+        w("    { const double ca = S.cons[info.x + %d], cb = S.cons[info.y + %d]; m = fmax(m, fabs(%s) * ca * ca * cb * cb); }" % (ia, ib, v))
+    w("    return m;")
+    w("}")
+    w("void launch_schwarz_%s(const SchwarzParams& S, int begin, int end, int mode, int grid, int block, cudaStream_t st)" % tag)
+    w("{")
+    w("    auto kern = schwarz_kernel<%d, %d>;" % (la, lb))
+    w("    QB_LAUNCH(kern, grid, block, 0, st, S, begin, end, mode);")
+    w("}")
+    w("}  // namespace qb")
+    return "\n".join(o) + "\n"
+
+
+def write_if_changed(path, src):
+    old = open(path).read() if os.path.exists(path) else None
+    if old != src:
+        with open(path, "w") as fh:
+            fh.write(src)
+
+
 def main(outdir, lmax=2):
     os.makedirs(outdir, exist_ok=True)
     cls = classes(lmax)
@@ -326,8 +406,21 @@ def main(outdir, lmax=2):
     for k, c in enumerate(cls):
         lt.append("    case %d: launch_%d%d%d%d(P, %d, grid, block, st); break;" % ((k,) + c + (k,)))
     lt += ["    default: break;", "    }", "}", "}  // namespace qb"]
-    with open(os.path.join(outdir, "eri_launch.cu"), "w") as fh:
-        fh.write("\n".join(lt) + "\n")
+    write_if_changed(os.path.join(outdir, "eri_launch.cu"), "\n".join(lt) + "\n")
+    import json
+    write_if_changed(os.path.join(outdir, "class_flops.json"),
+                     json.dumps({"%d%d%d%d" % c: s for c, s in stats.items()}, indent=1))
+    # Schwarz kernels, one per pair type
+    st = ['#include "eri_common.cuh"', '#include "schwarz.cuh"', '#include "eri_classes.h"', "namespace qb {"]
+    for t in pair_types(lmax):
+        write_if_changed(os.path.join(outdir, "sch_%d%d.cu" % t), gen_schwarz(*t))
+        st.append("void launch_schwarz_%d%d(const SchwarzParams& S, int begin, int end, int mode, int grid, int block, cudaStream_t st);" % t)
+    st += ["void launch_schwarz(int type, const SchwarzParams& S, int begin, int end, int mode, int grid, int block, cudaStream_t st)",
+           "{", "    switch (type) {"]
+    for k, t in enumerate(pair_types(lmax)):
+        st.append("    case %d: launch_schwarz_%d%d(S, begin, end, mode, grid, block, st); break;" % ((k,) + t))
+    st += ["    default: break;", "    }", "}", "}  // namespace qb"]
+    write_if_changed(os.path.join(outdir, "sch_launch.cu"), "\n".join(st) + "\n")
     return stats
 
 

@@ -56,3 +56,20 @@ def test_repeated_builds_reuse_buffers(session, oracle_lib):
         ref, _ = oracle_lib.fock(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
         got = session.get2e(np.zeros_like(D), D, cm, 1e-10, 1e-20)
         assert np.abs(got - ref).max() < TOL
+
+
+@pytest.mark.parametrize("name", ["water2_631gs", "propane_631gss"])
+def test_schwarz_kernel_matches_oracle(session, oracle_lib, name):
+    """YCutoff / cutPrim from the GPU kernel against the oracle's restatement
+    of schwarz.f90 (relative 1e-12; cutPrim entries below 1e-150 skipped,
+    their squares are subnormal)."""
+    m, b = case(name)
+    Yo, cpo = oracle_lib.schwarz(b, m.xyz_bohr)
+    session.upload_molecule(m, b)          # GPU Schwarz path
+    Y, cp = session.YCutoff, session.cutPrim
+    assert np.all((Y > 0) == (Yo > 0))
+    mask = Yo > 0
+    assert np.max(np.abs(Y[mask] - Yo[mask]) / Yo[mask]) < 1e-12
+    big = cpo > 1e-150
+    assert np.array_equal(cp > 0, cpo > 0)
+    assert np.max(np.abs(cp[big] - cpo[big]) / cpo[big]) < 1e-12
