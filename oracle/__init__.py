@@ -117,6 +117,40 @@ def fock(basis, xyz_bohr, YCutoff, cutPrim, cutMatrix, dense, integral_cutoff, p
     return O, dict(quartets=int(nq), prim_quartets=int(npq.value), integrals=int(nint.value))
 
 
+def grad2e(basis, xyz_bohr, YCutoff, cutPrim, cutMatrix, dense, integral_cutoff, prim_limit, hybrid=1.0):
+    """Two-electron part of the nuclear gradient, (3, natom) flattened like QUICK's."""
+    inp = OracleInputs(basis, xyz_bohr)
+    g = np.zeros(3 * basis.natom)
+    Y, cp, cm, d = (np.asfortranarray(a, dtype=np.float64) for a in (YCutoff, cutPrim, cutMatrix, dense))
+    lib().oracle_grad(C.byref(inp.s), _ptr(Y), _ptr(cp), _ptr(cm), _ptr(d), C.c_double(integral_cutoff),
+                      C.c_double(prim_limit), C.c_double(hybrid), _ptr(g))
+    return g
+
+
+def energy2e(basis, xyz_bohr, YCutoff, cutPrim, cutMatrix, dense, integral_cutoff, prim_limit, hybrid=1.0):
+    """E2 = Tr[D G(D)] / 2 from the oracle's Fock build."""
+    G, _ = fock(basis, xyz_bohr, YCutoff, cutPrim, cutMatrix, dense, integral_cutoff, prim_limit, hybrid)
+    return 0.5 * float(np.sum(np.asarray(dense) * G))
+
+
+def ref_grad(grad_in, dense, cutMatrix, integral_cutoff, prim_limit, grad_cutoff=1e-7):
+    """QUICK's gradient path (src/gradient.f90:279-286): upload_calculated,
+    upload_cutoff, upload_grad, gpu_grad_.  Returns grad_in + the 2e gradient."""
+    r = ref_lib()
+    n = dense.shape[0]
+    o = np.zeros((n, n), order="F")
+    co = np.zeros((n, n), order="F")
+    d = np.array(dense, order="F", dtype=np.float64)
+    cm = np.array(cutMatrix, order="F", dtype=np.float64)
+    g = np.array(grad_in, dtype=np.float64)
+    with _quiet():
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(co), _ptr(d))
+        r.gpu_upload_cutoff_(_ptr(cm), _d(integral_cutoff), _d(prim_limit), None)
+        r.gpu_upload_grad_(_ptr(g), _d(grad_cutoff))
+        r.gpu_grad_(_ptr(g))
+    return g
+
+
 def shell_quartet(basis, xyz_bohr, ii, jj, kk, ll, I, J, K, L):
     """Contracted (ab|cd) block (0-based shells) without screening."""
     inp = OracleInputs(basis, xyz_bohr)

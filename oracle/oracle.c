@@ -499,3 +499,84 @@ long oracle_fock(const OBasis* b, const double* YCutoff, const double* cutPrim, 
     if (nint_out) *nint_out = nint;
     return nquart;
 }
+
+/* ------------------------------------------------ derivative integrals */
+/* d/dA, d/dB, d/dC of the contracted block (ab|cd) (cons included), laid out
+ * as out[3 * (((i*nJ + j)*nK + k)*nL + l) + x].  See oracle_grad.c. */
+long oracle_shell_quartet_deriv(const OBasis* b, int ii, int jj, int kk, int ll, int I, int J, int K, int L,
+                                double DNMax, const double* cutPrim, double primLimit, double* dA, double* dB,
+                                double* dC)
+{
+    cart_init();
+    int Lab = I + J + 1, Lcd = K + L + 1;
+    VrrWork w;
+    vrr_alloc(&w, Lab, Lcd);
+    int ne = ncart_upto(Lab), nf = ncart_upto(Lcd);
+    size_t nG = (size_t)ne * nf;
+    double* G0 = (double*)calloc(4 * nG, sizeof(double));
+    double *GA = G0 + nG, *GB = G0 + 2 * nG, *GC = G0 + 3 * nG;
+    const double *A = center(b, ii), *B = center(b, jj), *C = center(b, kk), *D = center(b, ll);
+    double AB2 = 0, CD2 = 0;
+    for (int x = 0; x < 3; x++) { AB2 += (A[x] - B[x]) * (A[x] - B[x]); CD2 += (C[x] - D[x]) * (C[x] - D[x]); }
+    long nprimq = 0;
+    for (int pj = 0; pj < b->kprim[jj]; pj++)
+        for (int pi = 0; pi < b->kprim[ii]; pi++) {
+            double ea = cexpo(b, ii, pi), eb = cexpo(b, jj, pj);
+            double Kab = exp(-ea * eb / (ea + eb) * AB2) / (ea + eb) * ccoef(b, ii, I, pi) * ccoef(b, jj, J, pj);
+            double cpij = DNMax * F2(cutPrim, b->kstart[ii] - 1 + pi, b->kstart[jj] - 1 + pj, b->jbasis);
+            for (int pl = 0; pl < b->kprim[ll]; pl++)
+                for (int pk = 0; pk < b->kprim[kk]; pk++) {
+                    if (!(cpij * F2(cutPrim, b->kstart[kk] - 1 + pk, b->kstart[ll] - 1 + pl, b->jbasis) > primLimit)) continue;
+                    double ec = cexpo(b, kk, pk), ed = cexpo(b, ll, pl);
+                    double Kcd = exp(-ec * ed / (ec + ed) * CD2) / (ec + ed) * ccoef(b, kk, K, pk) * ccoef(b, ll, L, pl);
+                    double pref = X0SQ_GPU * Kab * Kcd / sqrt(ea + eb + ec + ed);
+                    vrr_prim(&w, A, C, ea, eb, ec, ed, B, D, pref);
+                    nprimq++;
+                    for (size_t ie = 0; ie < (size_t)ne; ie++)
+                        for (size_t jf = 0; jf < (size_t)nf; jf++) {
+                            double v = VA(&w, ie, jf, 0);
+                            G0[ie * nf + jf] += v;
+                            GA[ie * nf + jf] += 2.0 * ea * v;
+                            GB[ie * nf + jf] += 2.0 * eb * v;
+                            GC[ie * nf + jf] += 2.0 * ec * v;
+                        }
+                }
+        }
+    HrrCtx h0 = {G0, nf, {A[0] - B[0], A[1] - B[1], A[2] - B[2]}, {C[0] - D[0], C[1] - D[1], C[2] - D[2]}};
+    HrrCtx hA = h0, hB = h0, hC = h0;
+    hA.G = GA; hB.G = GB; hC.G = GC;
+    int a0 = bf_first(b, ii, I), a1 = bf_last(b, ii, I);
+    int b0 = bf_first(b, jj, J), b1 = bf_last(b, jj, J);
+    int c0 = bf_first(b, kk, K), c1 = bf_last(b, kk, K);
+    int d0 = bf_first(b, ll, L), d1 = bf_last(b, ll, L);
+    int nJ = b1 - b0 + 1, nK = c1 - c0 + 1, nL = d1 - d0 + 1;
+    for (int ia = a0; ia <= a1; ia++)
+        for (int ib = b0; ib <= b1; ib++)
+            for (int ic = c0; ic <= c1; ic++)
+                for (int id = d0; id <= d1; id++) {
+                    const int* ka = b->KLMN + 3 * ia;
+                    const int* kb = b->KLMN + 3 * ib;
+                    const int* kc = b->KLMN + 3 * ic;
+                    const int* kd = b->KLMN + 3 * id;
+                    double cf = b->cons[ia] * b->cons[ib] * b->cons[ic] * b->cons[id];
+                    size_t o = 3 * ((((size_t)(ia - a0) * nJ + (ib - b0)) * nK + (ic - c0)) * nL + (id - d0));
+                    for (int x = 0; x < 3; x++) {
+                        int ap[3] = {ka[0], ka[1], ka[2]}, am[3] = {ka[0], ka[1], ka[2]};
+                        int bp[3] = {kb[0], kb[1], kb[2]}, bm[3] = {kb[0], kb[1], kb[2]};
+                        int cp[3] = {kc[0], kc[1], kc[2]}, cmm[3] = {kc[0], kc[1], kc[2]};
+                        ap[x]++; am[x]--; bp[x]++; bm[x]--; cp[x]++; cmm[x]--;
+                        double va = hrr_full(&hA, ap, kb, kc[0], kc[1], kc[2], kd[0], kd[1], kd[2]);
+                        if (ka[x] > 0) va -= ka[x] * hrr_full(&h0, am, kb, kc[0], kc[1], kc[2], kd[0], kd[1], kd[2]);
+                        double vb = hrr_full(&hB, ka, bp, kc[0], kc[1], kc[2], kd[0], kd[1], kd[2]);
+                        if (kb[x] > 0) vb -= kb[x] * hrr_full(&h0, ka, bm, kc[0], kc[1], kc[2], kd[0], kd[1], kd[2]);
+                        double vc = hrr_full(&hC, ka, kb, cp[0], cp[1], cp[2], kd[0], kd[1], kd[2]);
+                        if (kc[x] > 0) vc -= kc[x] * hrr_full(&h0, ka, kb, cmm[0], cmm[1], cmm[2], kd[0], kd[1], kd[2]);
+                        dA[o + x] = cf * va;
+                        dB[o + x] = cf * vb;
+                        dC[o + x] = cf * vc;
+                    }
+                }
+    free(G0);
+    free(w.A);
+    return nprimq;
+}

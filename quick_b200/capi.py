@@ -127,6 +127,23 @@ class Session:
         check()
         return o
 
+    def grad(self, grad_in, dense, cutMatrix, integral_cutoff, prim_limit, grad_cutoff=1e-7):
+        """grad_in + dE2/dR: QUICK's upload_calculated / cutoff / grad + gpu_grad_
+        (src/gradient.f90:279-286).  grad_in is QUICK's (3, natom) gradient."""
+        r = lib()
+        n = self.nbasis
+        o = np.zeros((n, n), order="F")
+        co = np.zeros((1,), dtype=np.float64)
+        d = np.asfortranarray(dense, dtype=np.float64)
+        cm = np.asfortranarray(cutMatrix, dtype=np.float64)
+        g = np.array(grad_in, dtype=np.float64).ravel(order="F").copy()
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(co), _ptr(d))
+        r.gpu_upload_cutoff_(_ptr(cm), _d(integral_cutoff), _d(prim_limit), None)
+        r.gpu_upload_grad_(_ptr(g), _d(grad_cutoff))
+        r.gpu_grad_(_ptr(g))
+        check()
+        return g
+
     def fock_stats(self):
         q, a, b = C.c_longlong(0), C.c_double(0), C.c_double(0)
         lib().qb_last_fock_stats(C.byref(q), C.byref(a), C.byref(b))

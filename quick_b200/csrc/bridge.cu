@@ -22,6 +22,7 @@
 #include "gen/eri_classes.h"
 #include "qb_internal.h"
 #include "schwarz.cuh"
+#include "grad_common.cuh"
 
 namespace qb {
 
@@ -75,7 +76,8 @@ struct Context {
     std::vector<int> type_begin, type_end;
     // device tables
     DevBuf<double4> d_prim;
-    DevBuf<double> d_cut_prim, d_pair_Y, d_boys, d_dense, d_dense_raw, d_cons, d_fock, d_cut_matrix, d_o_in, d_o_out;
+    DevBuf<double> d_pair_Y, d_boys, d_dense, d_dense_raw, d_cons, d_fock, d_cut_matrix, d_o_in, d_o_out, d_grad;
+    DevBuf<int> d_shell_atom;
     DevBuf<int4> d_pair_bf, d_pair_sh;
     DevBuf<double4> d_pair_AB;
     DevBuf<ScreenClass> d_screen_cls;
@@ -91,6 +93,8 @@ struct Context {
     double integralCutoff = 1e-7, primLimit = 1e-7, DMCutoff = 1e-9, gradCutoff = 1e-7;
     std::vector<double> cutMatrix;
     bool have_cutoff = false;
+    std::vector<double> grad_host;
+    bool have_grad = false;
     // stats
     long long last_quartets = 0;
     double last_ms_eri = 0, last_ms_screen = 0;
@@ -143,7 +147,7 @@ static void boys_table(std::vector<double>& tab)
     tab.assign((size_t)kBoysPoints * kBoysCols, 0.0);
     for (int k = 0; k < kBoysPoints; k++) {
         long double T = (long double)k / kBoysPerUnit;
-        int mmax = kBoysCols - 1;
+        int mmax = kBoysExpCol - 1;
         long double term = 1.0L / (2 * mmax + 1), sum = term;
         for (int j = 1; j < 2000; j++) {
             term *= 2.0L * T / (2 * mmax + 2 * j + 1);
@@ -152,6 +156,7 @@ static void boys_table(std::vector<double>& tab)
         }
         long double e = expl(-T);
         long double f = e * sum;
+        tab[(size_t)k * kBoysCols + kBoysExpCol] = (double)e;
         tab[(size_t)k * kBoysCols + mmax] = (double)f;
         for (int m = mmax - 1; m >= 0; m--) {
             f = (2.0L * T * f + e) / (2 * m + 1);
@@ -299,13 +304,12 @@ static int build_tables(Context& c)
     std::vector<double> pY(c.npair);
     std::vector<double4> pAB(c.npair);
     std::vector<double4> prim;
-    std::vector<double> cprim;
     for (int i = 0; i < c.npair; i++) {
         const Rec& e = recs[i];
         const double *A = center(c, e.shA), *B = center(c, e.shB);
         double AB2 = 0;
         for (int k = 0; k < 3; k++) AB2 += (A[k] - B[k]) * (A[k] - B[k]);
-        int off = (int)cprim.size();
+        int off = (int)prim.size() / 3;
         // QUICK's own orientation (first Qshell x) indexes cutPrim
         int x = c.ref_xy[2 * e.ref], y = c.ref_xy[2 * e.ref + 1];
         int sx = c.sorted_Q[x], sy = c.sorted_Q[y];
@@ -319,25 +323,28 @@ static int build_tables(Context& c)
                     P[k] = (A[k] * a + B[k] * b) / p;
                     PA[k] = P[k] - A[k];
                 }
-                prim.push_back(make_double4(p, K, P[0], P[1]));
-                prim.push_back(make_double4(P[2], PA[0], PA[1], PA[2]));
                 int px = (e.shA == sx && (sx != sy || e.LA == c.sorted_Qnumber[x])) ? pa : pb;
                 int py = (px == pa) ? pb : pa;
-                cprim.push_back(c.cutPrim[(size_t)(c.kstart[sx] - 1 + px) + (size_t)(c.kstart[sy] - 1 + py) * c.jbasis]);
+                double cp = c.cutPrim[(size_t)(c.kstart[sx] - 1 + px) + (size_t)(c.kstart[sy] - 1 + py) * c.jbasis];
+                prim.push_back(make_double4(p, K, P[0], P[1]));
+                prim.push_back(make_double4(P[2], PA[0], PA[1], PA[2]));
+                prim.push_back(make_double4(0.5 / p, a, cp, 0.0));
             }
-        pbf[i] = make_int4(bf_first(c, e.shA, e.LA), bf_first(c, e.shB, e.LB), off, (int)cprim.size() - off);
+        pbf[i] = make_int4(bf_first(c, e.shA, e.LA), bf_first(c, e.shB, e.LB), off, (int)prim.size() / 3 - off);
         psh[i] = make_int4(e.shA, e.shB, e.key, e.ref);
         pY[i] = e.Y;
         pAB[i] = make_double4(A[0] - B[0], A[1] - B[1], A[2] - B[2], e.w);
     }
     CK(c.d_prim.alloc(prim.size()));
-    CK(c.d_cut_prim.alloc(cprim.size()));
     CK(c.d_pair_bf.alloc(c.npair));
     CK(c.d_pair_sh.alloc(c.npair));
     CK(c.d_pair_Y.alloc(c.npair));
     CK(c.d_pair_AB.alloc(c.npair));
     CK(cudaMemcpy(c.d_prim.p, prim.data(), prim.size() * sizeof(double4), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c.d_cut_prim.p, cprim.data(), cprim.size() * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<int> satom(c.nshell);
+    for (int s = 0; s < c.nshell; s++) satom[s] = c.katom[s] - 1;
+    CK(c.d_shell_atom.alloc(c.nshell));
+    CK(cudaMemcpy(c.d_shell_atom.p, satom.data(), c.nshell * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.d_pair_bf.p, pbf.data(), pbf.size() * sizeof(int4), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.d_pair_sh.p, psh.data(), psh.size() * sizeof(int4), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.d_pair_Y.p, pY.data(), pY.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -363,7 +370,6 @@ static FockParams fock_params(Context& c)
 {
     FockParams P;
     P.prim = c.d_prim.p;
-    P.cut_prim = c.d_cut_prim.p;
     P.pair_bf = c.d_pair_bf.p;
     P.pair_sh = c.d_pair_sh.p;
     P.pair_Y = c.d_pair_Y.p;
@@ -414,6 +420,54 @@ static int size_quartet_lists(Context& c)
     CK(cudaMemcpy(c.d_screen_cls.p, c.screen_cls.data(), kNumClasses * sizeof(ScreenClass), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.d_class_offset.p, offs.data(), kNumClasses * sizeof(long long), cudaMemcpyHostToDevice));
     g_sized_cutoff = c.integralCutoff;
+    return 0;
+}
+
+// Screening into the per-class quartet lists for the current density; the
+// class counts come back to the host to size the class launches.
+static int screen_quartets(Context& c, std::vector<int>& cnt)
+{
+    if (require(c.have_pairs, "gpu_upload_cutoff_matrix_ must precede the two-electron kernels")) return 1;
+    if (require(c.have_cutoff, "gpu_upload_cutoff_ must precede the two-electron kernels")) return 1;
+    if (g_sized_cutoff != c.integralCutoff || c.d_quartets.p == nullptr)
+        if (size_quartet_lists(c)) return 2;
+    int n = c.nbasis;
+    CK(cudaMemsetAsync(c.d_counts.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
+    CK(cudaMemsetAsync(c.d_overflow.p, 0, sizeof(int), c.stream));
+    CK(c.d_dense.alloc((size_t)n * n));
+    launch_scale_density(c.d_dense_raw.p, c.d_cons.p, c.d_dense.p, n, c.stream);
+    FockParams P = fock_params(c);
+    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p};
+    launch_screen(S, P, kNumClasses, 0, c.nsm, c.stream);
+    launch_finish_counts(S, c.d_class_count.p, c.d_overflow.p, kNumClasses, c.stream);
+    CK(cudaGetLastError());
+    cnt.assign(kNumClasses, 0);
+    int ovf = 0;
+    CK(cudaMemcpyAsync(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&ovf, c.d_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (ovf) return set_error(3, "quartet list overflow (internal sizing error)"), 3;
+    return 0;
+}
+
+// Two-electron gradient into d_grad (3 natom), same quartet lists.
+static int grad_build(Context& c)
+{
+    std::vector<int> cnt;
+    if (int rc = screen_quartets(c, cnt)) return rc;
+    CK(c.d_grad.alloc(3 * (size_t)c.natom));
+    CK(cudaMemsetAsync(c.d_grad.p, 0, 3 * (size_t)c.natom * sizeof(double), c.stream));
+    FockParams P = fock_params(c);
+    GradExtra G{c.d_shell_atom.p, c.d_pair_sh.p, c.d_grad.p};
+    for (int k = 0; k < kNumClasses; k++) {
+        if (cnt[k] == 0) continue;
+        int block = 128;
+        long long warps = (cnt[k] + 31) / 32;
+        long long grid = std::min<long long>((warps * 32 + block - 1) / block, (long long)c.nsm * 16);
+        launch_grad_class(k, P, G, (int)std::max<long long>(grid, 1), block, c.stream);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c.stream));
     return 0;
 }
 
@@ -548,7 +602,8 @@ void gpu_shutdown_(void)
 {
     if (!g) return;
     Context& c = *g;
-    DevBuf<double>* dbl[] = {&c.d_cut_prim, &c.d_pair_Y, &c.d_boys, &c.d_dense, &c.d_dense_raw, &c.d_cons, &c.d_fock, &c.d_cut_matrix, &c.d_o_in, &c.d_o_out};
+    DevBuf<double>* dbl[] = {&c.d_pair_Y, &c.d_boys, &c.d_dense, &c.d_dense_raw, &c.d_cons, &c.d_fock, &c.d_cut_matrix, &c.d_o_in, &c.d_o_out, &c.d_grad};
+    c.d_shell_atom.release();
     for (auto* b : dbl) b->release();
     c.d_prim.release();
     c.d_pair_bf.release();
@@ -803,14 +858,32 @@ void gpu_cleanup_(void)
 
 void gpu_upload_grad_(double* grad, double* gradCutoff)
 {
-    (void)grad;
-    (void)gradCutoff;
-    set_error(20, "gpu_upload_grad_: gradient not available in this build yet");
+    Context& c = ctx();
+    c.grad_host.assign(grad, grad + 3 * (size_t)c.natom);
+    c.gradCutoff = *gradCutoff;
+    c.have_grad = true;
 }
+
+// grad <- grad + dE2/dR, E2 = sum (pq|rs) [D_pq D_rs / 2 - h D_pr D_qs / 4]
+// (QUICK: gpu.cu:1481-1551 with getGrad_kernel, gpu_get2e_subs_grad.h).
 void gpu_grad_(double* grad)
 {
-    (void)grad;
-    set_error(20, "gpu_grad_: gradient not available in this build yet");
+    Context& c = ctx();
+    if (require(c.have_grad, "gpu_upload_grad_ must precede gpu_grad_")) return;
+    if (require(c.have_calc, "gpu_upload_calculated_ must precede gpu_grad_")) return;
+    size_t nn = (size_t)c.nbasis * c.nbasis;
+    if (c.d_dense_raw.alloc(nn) != cudaSuccess ||
+        cudaMemcpyAsync(c.d_dense_raw.p, c.dense_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess) {
+        set_error(2, "upload of the density failed");
+        return;
+    }
+    if (grad_build(c)) return;
+    std::vector<double> g2(3 * (size_t)c.natom);
+    if (cudaMemcpy(g2.data(), c.d_grad.p, g2.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_error(2, "download of the gradient failed");
+        return;
+    }
+    for (size_t k = 0; k < g2.size(); k++) grad[k] = c.grad_host[k] + g2[k];
 }
 void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double* belec, double* o)
 {
@@ -847,7 +920,7 @@ int gpu_schwarz_(double* YCutoff, double* cutPrim)
         const double *A = center(c, e.shA), *B = center(c, e.shB);
         double AB2 = 0;
         for (int k = 0; k < 3; k++) AB2 += (A[k] - B[k]) * (A[k] - B[k]);
-        int off = (int)prim.size() / 2;
+        int off = (int)prim.size() / 3;
         for (int pa = 0; pa < c.kprim[e.shA]; pa++)
             for (int pb = 0; pb < c.kprim[e.shB]; pb++) {
                 double a = cexpo(c, e.shA, pa), bb = cexpo(c, e.shB, pb), p = a + bb;
@@ -859,13 +932,14 @@ int gpu_schwarz_(double* YCutoff, double* cutPrim)
                 }
                 prim.push_back(make_double4(p, K, P[0], P[1]));
                 prim.push_back(make_double4(P[2], PA[0], PA[1], PA[2]));
+                prim.push_back(make_double4(0.5 / p, a, 0.0, 0.0));
             }
-        pbf[i] = make_int4(bf_first(c, e.shA, e.LA), bf_first(c, e.shB, e.LB), off, (int)prim.size() / 2 - off);
+        pbf[i] = make_int4(bf_first(c, e.shA, e.LA), bf_first(c, e.shB, e.LB), off, (int)prim.size() / 3 - off);
         pAB[i] = make_double4(A[0] - B[0], A[1] - B[1], A[2] - B[2], 1.0);
         if (i == 0 || recs[i - 1].type != e.type) tbeg[e.type] = i;
         tend[e.type] = i + 1;
     }
-    int nprimpair = (int)prim.size() / 2;
+    int nprimpair = (int)prim.size() / 3;
     DevBuf<double4> d_prim, d_ab;
     DevBuf<int4> d_bf;
     DevBuf<double> d_oc, d_op;

@@ -197,12 +197,12 @@ def gen_class(la, lb, lc, ld):
     for e, f, _ in targets:
         w("    double c_%s_%s = 0.0;" % (nm(e), nm(f)))
     w("    for (int ib = 0; ib < q.nbra; ib++) {")
-    w("        const PrimPair pb = load_prim(P, q.bra_off + ib);")
-    w("        const double cpb = P.cut_prim[q.bra_off + ib];")
+    w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
+    w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
     w("        for (int ik = 0; ik < q.nket; ik++) {")
-    w("            const double cpk = P.cut_prim[q.ket_off + ik];")
-    w("            if (!prim_survives(q, cpb, cpk, P.prim_limit)) continue;")
-    w("            const PrimPair pk = load_prim(P, q.ket_off + ik);")
+    w("            const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
+    w("            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
+    w("            const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
     w("            PrimQuartet s;")
     w("            double Fm[L + 1];")
     w("            prim_quartet<L>(pb, pk, P, s, Fm);")
@@ -297,6 +297,161 @@ def gen_class(la, lb, lc, ld):
     return "\n".join(o) + "\n", stats
 
 
+def gen_grad_class(la, lb, lc, ld):
+    """Nuclear gradient of the two-electron energy for one class: derivative
+    integrals from exponent-weighted contractions,
+      d/dA (ab|cd) = (a+1 b|cd)_{2 alpha} - a_i (a-1 b|cd),
+      d/dB (ab|cd) = (a b+1|cd)_{2 beta}  - b_i (a b-1|cd),
+      d/dC (ab|cd) = (ab|c+1 d)_{2 gamma} - c_i (ab|c-1 d),   d/dD = -(A+B+C)
+    (QUICK: gpu_get2e_subs_grad.h:143-512, storeAA/BB/CC), contracted with
+    Gamma = w [4 D_ab D_cd - h (D_ac D_bd + D_ad D_bc)], the sum of the
+    energy's density factors over the eight index permutations."""
+    L = la + lb + lc + ld + 1
+    tag = "%d%d%d%d" % (la, lb, lc, ld)
+    rng = lambda lo, hi: [e for n in range(max(lo, 0), hi + 1) for e in carts(n)]
+    S0e, S0f = rng(la - 1, la + lb), rng(lc - 1, lc + ld)
+    SAe, SAf = rng(la + 1, la + lb + 1), rng(lc, lc + ld)
+    SBe, SBf = rng(la, la + lb + 1), rng(lc, lc + ld)
+    SCe, SCf = rng(la, la + lb), rng(lc + 1, lc + ld + 1)
+    vrr = VRR()
+    acc = {}
+    for nmz, es, fs in (("s0", S0e, S0f), ("sa", SAe, SAf), ("sb", SBe, SBf), ("sc", SCe, SCf)):
+        acc[nmz] = [(e, f, vrr.get(e, f, 0)) for e in es for f in fs]
+    hrrs = {k: HRRX(k) for k in acc}
+    A, B, Cc, D = QUICK_ORDER[la], QUICK_ORDER[lb], QUICK_ORDER[lc], QUICK_ORDER[ld]
+    na, nb, nc, nd = len(A), len(B), len(Cc), len(D)
+    deriv = {}
+    for ia, a in enumerate(A):
+        for ib, b in enumerate(B):
+            for ic, c in enumerate(Cc):
+                for id_, d in enumerate(D):
+                    for i in range(3):
+                        ta = [hrrs["sa"].get(add(a, i), b, c, d)]
+                        if a[i] > 0:
+                            ta.append("-%d.0*%s" % (a[i], hrrs["s0"].get(sub(a, i), b, c, d)))
+                        tb = [hrrs["sb"].get(a, add(b, i), c, d)]
+                        if b[i] > 0:
+                            tb.append("-%d.0*%s" % (b[i], hrrs["s0"].get(a, sub(b, i), c, d)))
+                        tc = [hrrs["sc"].get(a, b, add(c, i), d)]
+                        if c[i] > 0:
+                            tc.append("-%d.0*%s" % (c[i], hrrs["s0"].get(a, b, sub(c, i), d)))
+                        deriv[(ia, ib, ic, id_, i)] = (" + ".join(ta), " + ".join(tb), " + ".join(tc))
+    o = []
+    w = o.append
+    w("// generated by gen_eri.py: gradient class (%s %s | %s %s)" % tuple("spdf"[x] for x in (la, lb, lc, ld)))
+    w('#include "eri_common.cuh"')
+    w('#include "grad_common.cuh"')
+    w("namespace qb {")
+    w("template <> __device__ __forceinline__ void grad_class<%d, %d, %d, %d>(const QuartetCtx& q, const FockParams& P, const GradExtra& G)" % (la, lb, lc, ld))
+    w("{")
+    w("    constexpr int L = %d;" % L)
+    for k, lst in acc.items():
+        for e, f, _ in lst:
+            w("    double %s_%s_%s = 0.0;" % (k, nm(e), nm(f)))
+    w("    for (int ib = 0; ib < q.nbra; ib++) {")
+    w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
+    w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
+    w("        const double a2 = 2.0 * xb.y;")
+    w("        const double b2 = 2.0 * pb.p - a2;")
+    w("        for (int ik = 0; ik < q.nket; ik++) {")
+    w("            const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
+    w("            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
+    w("            const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
+    w("            const double c2 = 2.0 * xk.y;")
+    w("            PrimQuartet s;")
+    w("            double Fm[L + 1];")
+    w("            prim_quartet<L>(pb, pk, P, s, Fm);")
+    w("            const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
+    w("            const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
+    w("            const double WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;")
+    w("            const double o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;")
+    w("            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;")
+    w("            (void)WQx; (void)WQy; (void)WQz; (void)o2p; (void)o2q; (void)o2pq; (void)rp; (void)rq;")
+    for m in range(L + 1):
+        w("            const double F%d = Fm[%d];" % (m, m))
+    for ln in vrr.lines:
+        w("            " + ln)
+    wt = {"s0": "", "sa": "a2*", "sb": "b2*", "sc": "c2*"}
+    for k, lst in acc.items():
+        for e, f, v in lst:
+            w("            %s_%s_%s += %s%s;" % (k, nm(e), nm(f), wt[k], v))
+    w("        }")
+    w("    }")
+    w("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
+    w("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
+    for h in hrrs.values():
+        for ln in h.lines:
+            w("    " + ln)
+    w("    const double* __restrict__ Dm = P.dense;")
+    w("    const int n = P.nbasis;")
+    w("    const int a0 = q.bfA, b0 = q.bfB, c0 = q.bfC, d0 = q.bfD;")
+    w("    const double hx = P.hybrid;")
+
+    def dl(x, y):
+        return "__ldg(Dm + (size_t)(%s) * n + (%s))" % (x, y)
+    bases = {"a": "a0", "b": "b0", "c": "c0", "d": "d0"}
+    sizes = {"a": na, "b": nb, "c": nc, "d": nd}
+    for blk in ("ab", "cd", "ac", "bd", "ad", "bc"):
+        x, y = blk
+        for i in range(sizes[x]):
+            for j in range(sizes[y]):
+                w("    const double D%s_%d_%d = %s;" % (blk, i, j, dl("%s+%d" % (bases[x], i), "%s+%d" % (bases[y], j))))
+    w("    double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};")
+    for ia in range(na):
+        for ib in range(nb):
+            for ic in range(nc):
+                for id_ in range(nd):
+                    w("    {")
+                    w("        const double g = 4.0*Dab_%d_%d*Dcd_%d_%d - hx*(Dac_%d_%d*Dbd_%d_%d + Dad_%d_%d*Dbc_%d_%d);" % (
+                        ia, ib, ic, id_, ia, ic, ib, id_, ia, id_, ib, ic))
+                    for i in range(3):
+                        da, db, dc = deriv[(ia, ib, ic, id_, i)]
+                        w("        gA[%d] += g*(%s); gB[%d] += g*(%s); gC[%d] += g*(%s);" % (i, da, i, db, i, dc))
+                    w("    }")
+    w("    grad_digest(q, G, gA, gB, gC);")
+    w("}")
+    w("void launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int grid, int block, cudaStream_t st)" % tag)
+    w("{")
+    w("    auto kern = grad_class_kernel<%d, %d, %d, %d>;" % (la, lb, lc, ld))
+    w("    QB_LAUNCH(kern, grid, block, 0, st, P, G, cls);")
+    w("}")
+    w("}  // namespace qb")
+    return "\n".join(o) + "\n", dict(vrr_flops=vrr.nflops, hrr_flops=sum(h.nflops for h in hrrs.values()),
+                                      lines=len(o))
+
+
+class HRRX(HRR):
+    """HRR over one named accumulator set (prefix_<e>_<f> leaves)."""
+
+    def __init__(self, prefix):
+        HRR.__init__(self)
+        self.prefix = prefix
+
+    def get(self, a, b, c, d):
+        key = (a, b, c, d)
+        if key in self.memo:
+            return self.memo[key]
+        if sum(d) > 0:
+            i = [k for k in range(3) if d[k] > 0][0]
+            x = self.get(a, b, add(c, i), sub(d, i))
+            y = self.get(a, b, c, sub(d, i))
+            expr = "%s + CD%s*%s" % (x, AX[i], y)
+        elif sum(b) > 0:
+            i = [k for k in range(3) if b[k] > 0][0]
+            x = self.get(add(a, i), sub(b, i), c, d)
+            y = self.get(a, sub(b, i), c, d)
+            expr = "%s + AB%s*%s" % (x, AX[i], y)
+        else:
+            name = "%s_%s_%s" % (self.prefix, nm(a), nm(c))
+            self.memo[key] = name
+            return name
+        self.nflops += 2
+        name = "%s_h%s_%s_%s_%s" % (self.prefix, nm(a), nm(b), nm(c), nm(d))
+        self.lines.append("const double %s = %s;" % (name, expr))
+        self.memo[key] = name
+        return name
+
+
 def gen_schwarz(la, lb):
     """Diagonal (ab|ab) blocks for QUICK's Schwarz bounds (schwarz.f90:46-548):
     max over components of |(ab|ab)| cons(a)^2 cons(b)^2, either contracted
@@ -332,9 +487,9 @@ def gen_schwarz(la, lb):
     for e, f, _ in targets:
         w("    double c_%s_%s = 0.0;" % (nm(e), nm(f)))
     w("    for (int ib = p0; ib < p0 + np; ib++) {")
-    w("        const PrimPair pb = load_prim_s(S, info.z + ib);")
+    w("        const PrimPair pb = load_prim_tab(S.prim, info.z + ib, load_prim_aux(S.prim, info.z + ib));")
     w("        for (int ik = p0; ik < p0 + np; ik++) {")
-    w("            const PrimPair pk = load_prim_s(S, info.z + ik);")
+    w("            const PrimPair pk = load_prim_tab(S.prim, info.z + ik, load_prim_aux(S.prim, info.z + ik));")
     w("            PrimQuartet s;")
     w("            double Fm[L + 1];")
     w("            prim_quartet<L>(pb, pk, P, s, Fm);")
@@ -410,6 +565,21 @@ def main(outdir, lmax=2):
     import json
     write_if_changed(os.path.join(outdir, "class_flops.json"),
                      json.dumps({"%d%d%d%d" % c: s for c, s in stats.items()}, indent=1))
+    # gradient kernels, one per class
+    gl = ['#include "eri_common.cuh"', '#include "grad_common.cuh"', '#include "eri_classes.h"', "namespace qb {"]
+    gstats = {}
+    for c in cls:
+        src, st_ = gen_grad_class(*c)
+        gstats["%d%d%d%d" % c] = st_
+        write_if_changed(os.path.join(outdir, "grad_%d%d%d%d.cu" % c), src)
+        gl.append("void launch_grad_%d%d%d%d(const FockParams& P, const GradExtra& G, int cls, int grid, int block, cudaStream_t st);" % c)
+    gl += ["void launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st)",
+           "{", "    switch (cls) {"]
+    for k, c in enumerate(cls):
+        gl.append("    case %d: launch_grad_%d%d%d%d(P, G, %d, grid, block, st); break;" % ((k,) + c + (k,)))
+    gl += ["    default: break;", "    }", "}", "}  // namespace qb"]
+    write_if_changed(os.path.join(outdir, "grad_launch.cu"), "\n".join(gl) + "\n")
+    write_if_changed(os.path.join(outdir, "grad_flops.json"), json.dumps(gstats, indent=1))
     # Schwarz kernels, one per pair type
     st = ['#include "eri_common.cuh"', '#include "schwarz.cuh"', '#include "eri_classes.h"', "namespace qb {"]
     for t in pair_types(lmax):

@@ -34,9 +34,9 @@ __global__ void __launch_bounds__(256) count_prims_kernel(const FockParams P, in
         QuartetCtx q;
         load_quartet(P, list[i], true, q);
         for (int ib = 0; ib < q.nbra; ib++) {
-            const double cpb = P.cut_prim[q.bra_off + ib];
+            const double cpb = load_prim_aux(P.prim, q.bra_off + ib).z;
             for (int ik = 0; ik < q.nket; ik++)
-                if (prim_survives(q, cpb, P.cut_prim[q.ket_off + ik], P.prim_limit)) mine++;
+                if (prim_survives(q, cpb, load_prim_aux(P.prim, q.ket_off + ik).z, P.prim_limit)) mine++;
         }
     }
     for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(FULL, mine, o);

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "eri_common.cuh"
+#include "grad_common.cuh"
 
 namespace qb {
 
@@ -24,6 +25,7 @@ void launch_finish_counts(const ScreenParams& S, int* class_count, int* overflow
 void launch_scale_density(const double* D, const double* cons, double* Ds, int n, cudaStream_t st);
 void launch_fock_finish(const double* G, const double* cons, const double* Oin, double* Oout, int n, cudaStream_t st);
 void launch_class(int cls, const FockParams& P, int grid, int block, cudaStream_t st);
+void launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st);
 int fma_probe(int fp64, int nsm, double* gflops, cudaStream_t st);
 void launch_count_prims(const FockParams& P, int ncls, unsigned long long* out, int nsm, cudaStream_t st);
 

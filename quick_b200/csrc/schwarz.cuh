@@ -16,15 +16,6 @@ struct SchwarzParams {
     double* out_prim;          // per primitive pair: the same for that pair alone
 };
 
-__device__ __forceinline__ PrimPair load_prim_s(const SchwarzParams& S, int i)
-{
-    const double4 u = S.prim[2 * i];
-    const double4 v = S.prim[2 * i + 1];
-    PrimPair r;
-    r.p = u.x; r.K = u.y; r.Px = u.z; r.Py = u.w;
-    r.Pz = v.x; r.PAx = v.y; r.PAy = v.z; r.PAz = v.w;
-    return r;
-}
 
 template <int LA, int LB>
 __device__ double schwarz_diag(const SchwarzParams& S, int rec, int p0, int np);

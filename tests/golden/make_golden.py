@@ -39,6 +39,13 @@ def main():
         out = {}
         for method in (0, 1):
             out["fock_m%d" % method] = oracle.ref_get2e(H, D, cm, 1e-10, 1e-20, method=method)
+        # QUICK's two-electron gradient (its gradient path runs with the HF method)
+        oracle.ref_lib().gpu_upload_method_(oracle._i(0))
+        Dg = random_density(b.nbasis, seed=5, scale=0.05)
+        cmg = oracle.cutmatrix(b, Dg)
+        out["grad_dense"] = Dg
+        out["grad_cutMatrix"] = cmg
+        out["grad2e"] = oracle.ref_grad(np.zeros(3 * m.natom), Dg, cmg, 1e-10, 1e-20)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), YCutoff=Y, cutPrim=cp, dense=D, cutMatrix=cm,
                             O_in=H, pairs=pl["pairs"], fStart=pl["fStart"], ffStart=pl["ffStart"],
                             sorted_Q=pl["sorted_Q"], sorted_Qnumber=pl["sorted_Qnumber"], **out)

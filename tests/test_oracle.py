@@ -64,3 +64,47 @@ def test_oracle_matches_quick_live(oracle_lib):
     ref = oracle_lib.ref_get2e(np.zeros_like(D), D, cm, 1e-9, 1e-12)
     got, _ = oracle_lib.fock(b, m.xyz_bohr, Y, cp, cm, D, 1e-9, 1e-12)
     assert np.abs(got - ref).max() < 1e-8
+
+
+def test_oracle_grad_matches_finite_differences(oracle_lib):
+    """Analytic two-electron gradient vs central differences (h = 1e-4 bohr)
+    of E2 = Tr[D G(D)]/2 with the density held fixed."""
+    m, b = case("water2_631gs")
+    D = random_density(b.nbasis, seed=3, scale=0.05)
+    cut, plim = 1e-14, 1e-30
+    X = m.xyz_bohr.copy()
+    Y, cp = oracle_lib.schwarz(b, X)
+    cm = oracle_lib.cutmatrix(b, D)
+    g = oracle_lib.grad2e(b, X, Y, cp, cm, D, cut, plim)
+    h = 1e-4
+    for k in (0, 4, 8, 13):
+        xs = []
+        for sgn in (1, -1):
+            v = X.ravel(order="F").copy()
+            v[k] += sgn * h
+            Xd = np.asfortranarray(v.reshape(3, -1, order="F"))
+            Yd, cpd = oracle_lib.schwarz(b, Xd)
+            xs.append(oracle_lib.energy2e(b, Xd, Yd, cpd, cm, D, cut, plim))
+        assert abs((xs[0] - xs[1]) / (2 * h) - g[k]) < 1e-7
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="QUICK host build not present")
+@pytest.mark.parametrize("name", ["water2_631gs", "propane_631gss"])
+def test_oracle_grad_matches_quick_live(oracle_lib, name):
+    m, b = case(name)
+    D = random_density(b.nbasis, seed=3, scale=0.05)
+    Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
+    cm = oracle_lib.cutmatrix(b, D)
+    g = oracle_lib.grad2e(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
+    oracle_lib.ref_upload_molecule(m, b, Y, cp, threads=8)
+    gr = oracle_lib.ref_grad(np.zeros_like(g), D, cm, 1e-10, 1e-20)
+    assert np.abs(g - gr).max() < 1e-8
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_oracle_grad_matches_quick_golden(oracle_lib, name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    m, b = case(name)
+    g = oracle_lib.grad2e(b, m.xyz_bohr, z["YCutoff"], z["cutPrim"], z["grad_cutMatrix"], z["grad_dense"],
+                          1e-10, 1e-20)
+    assert np.abs(g - z["grad2e"]).max() < 1e-8
