@@ -297,7 +297,7 @@ def gen_class(la, lb, lc, ld):
     return "\n".join(o) + "\n", stats
 
 
-def gen_grad_class(la, lb, lc, ld):
+def gen_grad_class(la, lb, lc, ld, part=0):
     """Nuclear gradient of the two-electron energy for one class: derivative
     integrals from exponent-weighted contractions,
       d/dA (ab|cd) = (a+1 b|cd)_{2 alpha} - a_i (a-1 b|cd),
@@ -307,8 +307,9 @@ def gen_grad_class(la, lb, lc, ld):
     Gamma = w [4 D_ab D_cd - h (D_ac D_bd + D_ad D_bc)], the sum of the
     energy's density factors over the eight index permutations."""
     L = la + lb + lc + ld + 1
-    tag = "%d%d%d%d" % (la, lb, lc, ld)
+    tag = "%d%d%d%d" % (la, lb, lc, ld) + ("" if part == 0 else "_" + "abc"[part - 1])
     rng = lambda lo, hi: [e for n in range(max(lo, 0), hi + 1) for e in carts(n)]
+    want = {"s0": True, "sa": part in (0, 1), "sb": part in (0, 2), "sc": part in (0, 3)}
     S0e, S0f = rng(la - 1, la + lb), rng(lc - 1, lc + ld)
     SAe, SAf = rng(la + 1, la + lb + 1), rng(lc, lc + ld)
     SBe, SBf = rng(la, la + lb + 1), rng(lc, lc + ld)
@@ -316,7 +317,8 @@ def gen_grad_class(la, lb, lc, ld):
     vrr = VRR()
     acc = {}
     for nmz, es, fs in (("s0", S0e, S0f), ("sa", SAe, SAf), ("sb", SBe, SBf), ("sc", SCe, SCf)):
-        acc[nmz] = [(e, f, vrr.get(e, f, 0)) for e in es for f in fs]
+        if want[nmz]:
+            acc[nmz] = [(e, f, None) for e in es for f in fs]
     hrrs = {k: HRRX(k) for k in acc}
     A, B, Cc, D = QUICK_ORDER[la], QUICK_ORDER[lb], QUICK_ORDER[lc], QUICK_ORDER[ld]
     na, nb, nc, nd = len(A), len(B), len(Cc), len(D)
@@ -326,23 +328,34 @@ def gen_grad_class(la, lb, lc, ld):
             for ic, c in enumerate(Cc):
                 for id_, d in enumerate(D):
                     for i in range(3):
-                        ta = [hrrs["sa"].get(add(a, i), b, c, d)]
-                        if a[i] > 0:
-                            ta.append("-%d.0*%s" % (a[i], hrrs["s0"].get(sub(a, i), b, c, d)))
-                        tb = [hrrs["sb"].get(a, add(b, i), c, d)]
-                        if b[i] > 0:
-                            tb.append("-%d.0*%s" % (b[i], hrrs["s0"].get(a, sub(b, i), c, d)))
-                        tc = [hrrs["sc"].get(a, b, add(c, i), d)]
-                        if c[i] > 0:
-                            tc.append("-%d.0*%s" % (c[i], hrrs["s0"].get(a, b, sub(c, i), d)))
+                        ta = tb = tc = ["0.0"]
+                        if want["sa"]:
+                            ta = [hrrs["sa"].get(add(a, i), b, c, d)]
+                            if a[i] > 0:
+                                ta.append("-%d.0*%s" % (a[i], hrrs["s0"].get(sub(a, i), b, c, d)))
+                        if want["sb"]:
+                            tb = [hrrs["sb"].get(a, add(b, i), c, d)]
+                            if b[i] > 0:
+                                tb.append("-%d.0*%s" % (b[i], hrrs["s0"].get(a, sub(b, i), c, d)))
+                        if want["sc"]:
+                            tc = [hrrs["sc"].get(a, b, add(c, i), d)]
+                            if c[i] > 0:
+                                tc.append("-%d.0*%s" % (c[i], hrrs["s0"].get(a, b, sub(c, i), d)))
                         deriv[(ia, ib, ic, id_, i)] = (" + ".join(ta), " + ".join(tb), " + ".join(tc))
+    # only the accumulators the horizontal recurrence reads, and only their
+    # vertical-recurrence targets
+    used = set()
+    for h in hrrs.values():
+        used |= set(h.leaves)
+    for k in list(acc):
+        acc[k] = [(e, f, vrr.get(e, f, 0)) for e, f, _ in acc[k] if "%s_%s_%s" % (k, nm(e), nm(f)) in used]
     o = []
     w = o.append
     w("// generated by gen_eri.py: gradient class (%s %s | %s %s)" % tuple("spdf"[x] for x in (la, lb, lc, ld)))
     w('#include "eri_common.cuh"')
     w('#include "grad_common.cuh"')
     w("namespace qb {")
-    w("template <> __device__ __forceinline__ void grad_class<%d, %d, %d, %d>(const QuartetCtx& q, const FockParams& P, const GradExtra& G)" % (la, lb, lc, ld))
+    w("template <> __device__ __forceinline__ void grad_class<%d, %d, %d, %d, %d>(const QuartetCtx& q, const FockParams& P, const GradExtra& G)" % (la, lb, lc, ld, part))
     w("{")
     w("    constexpr int L = %d;" % L)
     for k, lst in acc.items():
@@ -408,11 +421,11 @@ def gen_grad_class(la, lb, lc, ld):
                         da, db, dc = deriv[(ia, ib, ic, id_, i)]
                         w("        gA[%d] += g*(%s); gB[%d] += g*(%s); gC[%d] += g*(%s);" % (i, da, i, db, i, dc))
                     w("    }")
-    w("    grad_digest(q, G, gA, gB, gC);")
+    w("    grad_digest<%d>(q, G, gA, gB, gC);" % part)
     w("}")
     w("void launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int grid, int block, cudaStream_t st)" % tag)
     w("{")
-    w("    auto kern = grad_class_kernel<%d, %d, %d, %d>;" % (la, lb, lc, ld))
+    w("    auto kern = grad_class_kernel<%d, %d, %d, %d, %d>;" % (la, lb, lc, ld, part))
     w("    QB_LAUNCH(kern, grid, block, 0, st, P, G, cls);")
     w("}")
     w("}  // namespace qb")
@@ -426,6 +439,7 @@ class HRRX(HRR):
     def __init__(self, prefix):
         HRR.__init__(self)
         self.prefix = prefix
+        self.leaves = set()
 
     def get(self, a, b, c, d):
         key = (a, b, c, d)
@@ -443,6 +457,7 @@ class HRRX(HRR):
             expr = "%s + AB%s*%s" % (x, AX[i], y)
         else:
             name = "%s_%s_%s" % (self.prefix, nm(a), nm(c))
+            self.leaves.add(name)
             self.memo[key] = name
             return name
         self.nflops += 2
@@ -568,15 +583,24 @@ def main(outdir, lmax=2):
     # gradient kernels, one per class
     gl = ['#include "eri_common.cuh"', '#include "grad_common.cuh"', '#include "eri_classes.h"', "namespace qb {"]
     gstats = {}
+    parts = {}
     for c in cls:
-        src, st_ = gen_grad_class(*c)
-        gstats["%d%d%d%d" % c] = st_
-        write_if_changed(os.path.join(outdir, "grad_%d%d%d%d.cu" % c), src)
-        gl.append("void launch_grad_%d%d%d%d(const FockParams& P, const GradExtra& G, int cls, int grid, int block, cudaStream_t st);" % c)
+        # classes with total angular momentum >= 7 get one kernel per
+        # derivative centre (A, B, C): a third of the code each, which keeps
+        # the compile time of the largest classes in minutes
+        parts[c] = [0] if sum(c) < 7 else [1, 2, 3]
+        for pt in parts[c]:
+            src, st_ = gen_grad_class(*c, part=pt)
+            tg = "%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1])
+            gstats[tg] = st_
+            write_if_changed(os.path.join(outdir, "grad_%s.cu" % tg), src)
+            gl.append("void launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int grid, int block, cudaStream_t st);" % tg)
     gl += ["void launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st)",
            "{", "    switch (cls) {"]
     for k, c in enumerate(cls):
-        gl.append("    case %d: launch_grad_%d%d%d%d(P, G, %d, grid, block, st); break;" % ((k,) + c + (k,)))
+        calls = " ".join("launch_grad_%s(P, G, %d, grid, block, st);" % ("%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1]), k)
+                         for pt in parts[c])
+        gl.append("    case %d: %s break;" % (k, calls))
     gl += ["    default: break;", "    }", "}", "}  // namespace qb"]
     write_if_changed(os.path.join(outdir, "grad_launch.cu"), "\n".join(gl) + "\n")
     write_if_changed(os.path.join(outdir, "grad_flops.json"), json.dumps(gstats, indent=1))
