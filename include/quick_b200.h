@@ -104,6 +104,18 @@ int gpu_schwarz_(double* YCutoff, double* cutPrim);
    pointers, may alias).  Uses the cutoffs and density screen from the last gpu_upload_cutoff_. */
 int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out);
 
+/* No counterpart in QUICK.  The same Fock build as qb_fock_device for callers that cannot
+   allocate GPU memory while they run (a host program whose pool allocator owns the device
+   memory, or code that must not allocate after its set-up): it calls no cudaMalloc/cudaFree
+   and takes its working memory from one fixed 64 MiB array compiled into the library, present
+   on every GPU that loads it until the process exits.  Molecules whose density, Fock
+   accumulator and screened quartet lists do not fit are rejected with an error (use
+   qb_fock_device).  The first call on a device looks up the array's device address and
+   should come before any stream capture.  Calls share the array: calls that overlap on the GPU
+   race and must not be made.  Tables uploaded earlier (gpu_upload_basis_,
+   gpu_upload_cutoff_matrix_, gpu_upload_cutoff_) are used as they are. */
+int qb_fock_device_static(const double* d_dense, const double* d_o_in, double* d_o_out);
+
 /* Statistics of the last Fock build: unique shell quartets evaluated (one per unordered pair of
    kept shell pairs that passes QUICK's Schwarz and density tests), device time of the class
    kernels in ms, device time of the screening in ms. */

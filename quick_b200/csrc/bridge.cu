@@ -1043,3 +1043,37 @@ void gpu_addint_(double* o, int* intindex, char* intFileName)
 }
 
 }  // extern "C"
+
+namespace qb {
+
+// Read-only view of the current session's device tables, for entry points
+// that bring their own working memory (noalloc.cu).  Working-memory fields of
+// the returned FockParams (quartets, counts, dense, fock) are left null.
+int session_view(SessionView* v)
+{
+    if (!g) return set_error(1, "no session: gpu_startup_ and the uploads must come first"), 1;
+    Context& c = *g;
+    if (require(c.inited, "gpu_init_ must come first")) return 1;
+    if (require(c.have_pairs, "gpu_upload_cutoff_matrix_ must come first")) return 1;
+    if (require(c.have_cutoff, "gpu_upload_cutoff_ must come first")) return 1;
+    FockParams P = fock_params(c);
+    P.quartets = nullptr;
+    P.class_offset = nullptr;
+    P.class_count = nullptr;
+    P.dense = nullptr;
+    P.fock = nullptr;
+    v->P = P;
+    v->cls = c.screen_cls;
+    v->cons = c.d_cons.p;
+    v->nsm = c.nsm;
+    v->stream = c.stream;
+    return 0;
+}
+
+int report_error(int code, const char* msg)
+{
+    set_error(code, "%s", msg);
+    return code;
+}
+
+}  // namespace qb

@@ -1,6 +1,7 @@
 // Internal declarations shared by the host bridge and the kernels.
 #pragma once
 #include <cuda_runtime.h>
+#include <vector>
 #include "eri_common.cuh"
 #include "grad_common.cuh"
 
@@ -19,6 +20,16 @@ struct ScreenParams {
     unsigned long long* counts;
     int2* out;
 };
+
+struct SessionView {
+    FockParams P;                       // session tables; working-memory pointers null
+    std::vector<ScreenClass> cls;       // class ranges of the pair table
+    const double* cons;
+    int nsm;
+    cudaStream_t stream;
+};
+int session_view(SessionView* v);
+int report_error(int code, const char* msg);
 
 void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int count_only, int nsm, cudaStream_t st);
 void launch_finish_counts(const ScreenParams& S, int* class_count, int* overflow, int ncls, cudaStream_t st);

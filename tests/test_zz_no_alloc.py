@@ -1,0 +1,77 @@
+"""The fixed-scratch Fock build, qb_fock_device_static.
+
+Some callers cannot allocate GPU memory while they run (their own pool
+allocator owns the device, or nothing may be allocated after set-up); this
+entry point serves them from a fixed array inside the library.  Checked
+against the ordinary device-resident entry point, qb_fock_device, on two
+calls in a row, at the Fock tolerance of the other tests (1e-8).  Kept in a
+file of its own that pytest collects last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from tests.helpers import case, random_density
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-8
+
+
+def _dev(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def test_static_scratch_matches_device_entry_point(oracle_lib):
+    import torch
+    from quick_b200 import capi
+    s = capi.Session(0)
+    lib = capi.lib()
+    try:
+        m, b = case("water3_631gss")
+        Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
+        s.upload_molecule(m, b, Y, cp)
+        n = b.nbasis
+        D0 = random_density(n, seed=11)
+        cm = oracle_lib.cutmatrix(b, D0)
+        s.get2e(np.zeros((n, n)), D0, cm, 1e-10, 1e-20)     # uploads cutoffs
+        lib.qb_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        for seed in (11, 12):                                # two calls in a row
+            D = torch.from_numpy(np.ascontiguousarray(random_density(n, seed=seed))).cuda()
+            Oin = torch.from_numpy(np.ascontiguousarray(random_density(n, seed=seed + 50, scale=0.3))).cuda()
+            ref = torch.empty_like(Oin)
+            got = torch.full_like(Oin, np.nan)
+            assert lib.qb_fock_device(_dev(D), _dev(Oin), _dev(ref)) == 0, capi.check()
+            assert lib.qb_fock_device_static(_dev(D), _dev(Oin), _dev(got)) == 0, capi.check()
+            torch.cuda.synchronize()
+            err = (got - ref).abs().max().item()
+            assert err < TOL, err
+    finally:
+        lib.qb_set_stream(None)
+        s.close()
+
+
+def test_static_scratch_rejects_too_large(oracle_lib):
+    """(H2O)16 in 6-31G** screens to ~3e7 quartets, more than the fixed array holds."""
+    import torch
+    from quick_b200 import capi
+    from quick_b200.basis import build_basis
+    from quick_b200.molecule import water_cluster
+    s = capi.Session(0)
+    lib = capi.lib()
+    try:
+        m = water_cluster((4, 2, 2), seed=0)
+        b = build_basis(m.symbols, "6-31G**")
+        s.upload_molecule(m, b)
+        n = b.nbasis
+        D = random_density(n, seed=3)
+        cm = oracle_lib.cutmatrix(b, D)
+        s.get2e(np.zeros((n, n)), D, cm, 1e-10, 1e-20)
+        dD = torch.from_numpy(np.ascontiguousarray(D)).cuda()
+        out = torch.empty_like(dD)
+        rc = lib.qb_fock_device_static(_dev(dD), _dev(out), _dev(out))
+        assert rc != 0
+        with pytest.raises(capi.QuickB200Error, match="fixed array"):
+            capi.check()
+    finally:
+        s.close()
