@@ -67,7 +67,10 @@ void gpu_get2e_(double* o);
 void gpu_upload_grad_(double* grad, double* gradCutoff);
 /* src/cuda/gpu.cu:1481-1551: grad <- grad + two-electron gradient */
 void gpu_grad_(double* grad);
-/* src/cuda/gpu.cu:1866-1975 */
+/* src/cuda/gpu.cu:1866-1975: XC quadrature on QUICK's SG1 grid for the method of the last
+   gpu_upload_method_ (1 = B3LYP, 2 = BLYP).  Eelxc, aelec and belec are accumulated into; o is
+   overwritten with the symmetrised lower triangle of (O as uploaded by gpu_upload_calculated_ +
+   V_xc).  Only isg = 1 (SG1) is accepted: QUICK's GPU path generates no SG0 points. */
 void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double* belec, double* o);
 /* src/cuda/gpu.cu:1446-1479 */
 void gpu_cleanup_(void);
@@ -120,6 +123,26 @@ int qb_fock_device_static(const double* d_dense, const double* d_o_in, double* d
    kept shell pairs that passes QUICK's Schwarz and density tests), device time of the class
    kernels in ms, device time of the screening in ms. */
 int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen);
+
+/* XC quadrature on device pointers (no counterpart in QUICK; gpu_getxc_ without the host
+   round trip): adds V_xc to the lower triangle of d_vxc (column-major nbasis^2, V(j, i) for
+   j >= i; not zeroed here) for the density d_dense, and returns the grid sums of the energy
+   density and of the alpha density.  sigrad2 is a host array (nbasis), as for gpu_getxc_. */
+int qb_xc_device(const double* d_dense, const double* sigrad2, double* d_vxc, double* exc, double* nalpha);
+
+/* Statistics of the last XC quadrature: grid points kept (weight above 1e-9), point chunks
+   with at least one significant basis function, device time of the per-call phase in ms, and
+   of the grid build in ms (0 when the grid was reused). */
+int qb_last_xc_stats(long long* npts, long long* nchunks, double* ms, double* ms_grid);
+
+/* The kept grid points (x, y, z, weight per point) of the last XC grid build; copies up to cap
+   points and returns the number of points. */
+long long qb_xc_grid(double* xyzw, long long cap);
+
+/* The closed-shell functional (method 1 = B3LYP, 2 = BLYP) evaluated on the GPU at n pairs
+   (rho = total density, sigma = |grad rho|^2), host arrays: out[3k] = f,
+   out[3k+1] = df/drho, out[3k+2] = 4 df/dsigma (QUICK's b3lyp_e / b3lypf and becke/lyp). */
+int qb_xc_functional(int method, int n, const double* rho, const double* sigma, double* out);
 
 /* Measured FMA throughput of this GPU in GFLOP/s (FP64 if fp64 != 0, else FP32): a
    register-resident FMA chain over 8 blocks per SM, best of 4 timed runs. */

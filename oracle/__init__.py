@@ -200,8 +200,13 @@ def _d(v):
     return C.byref(C.c_double(float(v)))
 
 
+_ref_nshell = 0
+
+
 def ref_upload_molecule(mol, basis, YCutoff, cutPrim, threads=None):
     """QUICK's start-up upload sequence (src/main.f90:84-177)."""
+    global _ref_nshell
+    _ref_nshell = basis.nshell
     r = ref_lib()
     if threads:
         r.qref_set_threads(int(threads))
@@ -263,3 +268,46 @@ def ref_get2e(O, dense, cutMatrix, integral_cutoff, prim_limit, method=0):
         r.gpu_upload_cutoff_(_ptr(cm), _d(integral_cutoff), _d(prim_limit), None)
         r.gpu_get2e_(_ptr(o))
     return o
+
+
+def ref_getxc(O, dense, sigrad2, method=1, isg=1, Eelxc=0.0, aelec=0.0, belec=0.0, threads=None):
+    """One QUICK XC quadrature: upload_method / upload_calculated + gpu_getxc_
+    (src/dft.f90:893-899), run by QUICK's own getxc_kernel compiled for the
+    host.  Needs ref_upload_molecule first.  Returns (O', Eelxc, aelec, belec)."""
+    r = ref_lib()
+    r.qref_set_threads(int(threads or os.cpu_count() or 1))
+    n = O.shape[0]
+    o = np.array(O, order="F", dtype=np.float64)
+    co = np.zeros((n, n), order="F")
+    vec = np.zeros((n, n), order="F")
+    d = np.array(dense, order="F", dtype=np.float64)
+    sg = np.ascontiguousarray(sigrad2, dtype=np.float64)
+    e, a, b = C.c_double(Eelxc), C.c_double(aelec), C.c_double(belec)
+    # gpu_upload_cutoff_ is where QUICK's bridge sets its DMCutoff (1e-9,
+    # src/cuda/gpu.cu:370); the cut matrix itself is not read by the XC path.
+    cm = np.zeros((max(_ref_nshell, 1),) * 2, order="F")
+    with _quiet():
+        r.gpu_upload_method_(_i(method))
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(vec), _ptr(d))
+        r.gpu_upload_cutoff_(_ptr(cm), _d(1e-10), _d(1e-20), None)
+        r.qref_set_virtual_threads(1024)
+        try:
+            r.gpu_getxc_(_i(isg), _ptr(sg), C.byref(e), C.byref(a), C.byref(b), _ptr(o))
+        finally:
+            r.qref_set_virtual_threads(0)
+    return o, e.value, a.value, b.value
+
+
+def ref_functional(method, rho, sigma):
+    """QUICK's functional routines at closed-shell points (total density rho,
+    sigma = |grad rho|^2): returns (f, dfdr, dot) arrays."""
+    r = ref_lib()
+    f, fr, fs = C.c_double(), C.c_double(), C.c_double()
+    rho = np.asarray(rho, dtype=np.float64).ravel()
+    sigma = np.asarray(sigma, dtype=np.float64).ravel()
+    out = np.zeros((rho.size, 3))
+    for k in range(rho.size):
+        r.qref_functional(C.c_int(method), C.c_double(rho[k]), C.c_double(sigma[k]), C.byref(f), C.byref(fr),
+                          C.byref(fs))
+        out[k] = f.value, fr.value, fs.value
+    return out[:, 0], out[:, 1], out[:, 2]

@@ -15,7 +15,13 @@
 thread_local qref_dim qref_blockIdx, qref_threadIdx, qref_blockDim, qref_gridDim;
 
 static int qref_nthreads = 1;
+static int qref_nvirtual = 0;   // 0: one virtual thread per host thread
 extern "C" void qref_set_threads(int n) { qref_nthreads = n > 0 ? n : 1; }
+/* Number of GPU threads the launch pretends to have (gridDim.x of one-thread
+   blocks), run round-robin by the host threads.  getxc_kernel takes at most
+   one point of each radial shell per thread, so it needs at least as many
+   threads as the largest Lebedev sphere (194), as every real launch has. */
+extern "C" void qref_set_virtual_threads(int n) { qref_nvirtual = n > 0 ? n : 0; }
 
 typedef void (*qref_kernel_fn)();
 static const struct { const char* name; qref_kernel_fn fn; } qref_kernels[] = {
@@ -53,14 +59,17 @@ void qref_launch(const char* expr)
         abort();
     }
     int n = qref_nthreads;
+    int nv = qref_nvirtual > 0 ? qref_nvirtual : n;
     std::vector<std::thread> pool;
     for (int t = 0; t < n; t++) {
-        pool.emplace_back([fn, t, n]() {
-            qref_blockIdx = {(unsigned)t, 0, 0};
-            qref_threadIdx = {0, 0, 0};
-            qref_blockDim = {1, 1, 1};
-            qref_gridDim = {(unsigned)n, 1, 1};
-            fn();
+        pool.emplace_back([fn, t, n, nv]() {
+            for (int v = t; v < nv; v += n) {
+                qref_blockIdx = {(unsigned)v, 0, 0};
+                qref_threadIdx = {0, 0, 0};
+                qref_blockDim = {1, 1, 1};
+                qref_gridDim = {(unsigned)nv, 1, 1};
+                fn();
+            }
         });
     }
     for (auto& th : pool) th.join();

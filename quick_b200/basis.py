@@ -309,6 +309,11 @@ def build_basis(atoms, basis_name):
             last_bf[iatm - 2] = is_ - 1
     last_bf[iatm - 1] = nbasis
 
+    # getMol (src/getMol.f90:85) folds the normalisation into dcoeff before
+    # main.f90:168 uploads it; the XC quadrature evaluates basis functions
+    # from these coefficients.
+    normalize_dcoeff(ncontract, itype, aexp, dcoeff)
+
     return Basis(natom=natom, nshell=nshell, nprim=nprim, jshell=jshell, jbasis=jbasis,
                  nbasis=nbasis, maxcontract=maxcontract, ncontract=ncontract, itype=itype,
                  aexp=aexp, dcoeff=dcoeff, first_basis_function=first_bf,
@@ -318,3 +323,56 @@ def build_basis(atoms, basis_name):
                  Qnumber=Qnumber, Qstart=Qstart, Qfinal=Qfinal, Qsbasis=Qsbasis,
                  Qfbasis=Qfbasis, gccoeff=gccoeff, cons=cons, gcexpo=gcexpo, KLMN=KLMN,
                  gcexpomin=gcexpomin)
+
+
+def normalize_dcoeff(ncontract, itype, aexp, dcoeff):
+    """In-place restatement of normalize_basis
+    (src/modules/quick_basis_module_.f90:331-373): primitive norms, then the
+    contracted renormalisation, applied to dcoeff column by column."""
+    nbasis = dcoeff.shape[1]
+    for jb in range(nbasis):
+        i, j, k = (int(v) for v in itype[:, jb])
+        for c in range(int(ncontract[jb])):
+            dcoeff[c, jb] = dcoeff[c, jb] * xnorm(aexp[c, jb], i, j, k)
+    for ib in range(nbasis):
+        i, j, k = (int(v) for v in itype[:, ib])
+        n = int(ncontract[ib])
+        xponent = -1.5 + float(-i - j - k)
+        v = 0.0
+        for c1 in range(n):
+            for c2 in range(n):
+                v = v + dcoeff[c1, ib] * dcoeff[c2, ib] * (aexp[c1, ib] + aexp[c2, ib]) ** xponent
+        gamma = 1.0
+        for m in (i, j, k):
+            for L in range(1, m + 1):
+                gamma = gamma * ((m - L) + 0.5)
+        v = (v * gamma * PITO3HALF) ** (-0.5)
+        for c in range(n):
+            dcoeff[c, ib] = v * dcoeff[c, ib]
+
+
+def sigrad2(basis, basis_cutoff=1.0e-10):
+    """Squared radius of significance per basis function, restating get_sigrad
+    (src/dft.f90:536-612): the radius where r^L exp(-a_min r^2) first falls
+    below basis_cutoff / sqrt((2 a_min)^(L+3/2) / (2 pi Gamma(L+3/2))),
+    located by the same decimal step search (1, 0.1, ... 1e-4)."""
+    out = np.zeros(basis.nbasis)
+    for ib in range(basis.nbasis):
+        amin = 10.0e10
+        for c in range(int(basis.ncontract[ib])):
+            amin = min(amin, basis.aexp[c, ib])
+        L = int(basis.itype[:, ib].sum())
+        gamma = 1.0
+        for i in range(1, L + 2):
+            gamma = gamma * ((L + 1 - i) + 0.5)
+        gamma2pi = gamma * 11.13665599366341569
+        target = basis_cutoff * (((2.0 * amin) ** (L + 1.5)) / gamma2pi) ** (-0.5)
+        step, radial = 1.0, 0.0
+        while step > 1.0e-4:
+            radial = radial + step
+            current = math.exp(-amin * radial * radial) * radial ** L
+            if current < target:
+                radial = radial - step
+                step = step / 10.0
+        out[ib] = radial * radial
+    return out

@@ -8,6 +8,7 @@ the CUDA runtime linked statically.  Rebuilds only what changed.
 """
 import argparse
 import os
+import re
 import subprocess
 import sys
 from concurrent.futures import ThreadPoolExecutor
@@ -37,6 +38,26 @@ def _extra_flags(src):
     return []
 
 
+_INC = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(src, seen=None):
+    """The file and every header it includes with quotes, recursively."""
+    seen = set() if seen is None else seen
+    if src in seen:
+        return seen
+    seen.add(src)
+    with open(src) as fh:
+        text = fh.read()
+    for inc in _INC.findall(text):
+        for base in (os.path.dirname(src), CSRC, GEN, os.path.join(HERE, "..", "include")):
+            cand = os.path.normpath(os.path.join(base, inc))
+            if os.path.exists(cand):
+                _deps(cand, seen)
+                break
+    return seen
+
+
 def _newer(target, deps):
     if not os.path.exists(target):
         return True
@@ -48,11 +69,11 @@ def build(lmax=2, jobs=None, verbose=False):
     jobs = jobs or max(2, os.cpu_count() or 2)
     subprocess.run([sys.executable, os.path.join(CSRC, "gen_eri.py"), GEN, "--lmax", str(lmax)],
                    check=True, stdout=subprocess.DEVNULL)
+    subprocess.run([sys.executable, os.path.join(CSRC, "gen_xc.py"), GEN], check=True, stdout=subprocess.DEVNULL)
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
-    headers += [os.path.join(GEN, "eri_classes.h"), os.path.join(HERE, "..", "include", "quick_b200.h")]
     srcs = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]
+    srcs += [os.path.join(CSRC, "xc", f) for f in sorted(os.listdir(os.path.join(CSRC, "xc"))) if f.endswith(".cu")]
     srcs += [os.path.join(GEN, f) for f in sorted(os.listdir(GEN)) if f.endswith(".cu")]
     # drop generated classes beyond lmax (left over from an earlier build)
     keep = []
@@ -69,7 +90,7 @@ def build(lmax=2, jobs=None, verbose=False):
     for s in srcs:
         o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
         objs.append(o)
-        if _newer(o, [s] + headers):
+        if _newer(o, sorted(_deps(s))):
             todo.append((s, o))
 
     def cc(so):
@@ -87,7 +108,7 @@ def build(lmax=2, jobs=None, verbose=False):
     with ThreadPoolExecutor(jobs) as ex:
         list(ex.map(cc, todo))
     if todo or not os.path.exists(LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lpthread"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lcublas", "-lpthread"]
         subprocess.run(cmd, check=True)
     return LIB
 

@@ -144,6 +144,37 @@ class Session:
         check()
         return g
 
+    def getxc(self, O, dense, sigrad2, method=1, isg=1, Eelxc=0.0, aelec=0.0, belec=0.0):
+        """QUICK's DFT step (src/dft.f90:893-899): upload_method / calculated +
+        gpu_getxc_.  Returns (O + V_xc symmetrised, Eelxc, aelec, belec), the
+        three scalars accumulated onto the given inputs."""
+        r = lib()
+        o = np.array(O, order="F", dtype=np.float64)
+        co = np.zeros((1,), dtype=np.float64)
+        d = np.asfortranarray(dense, dtype=np.float64)
+        sg = np.ascontiguousarray(sigrad2, dtype=np.float64)
+        e, a, b = C.c_double(Eelxc), C.c_double(aelec), C.c_double(belec)
+        r.gpu_upload_method_(_i(method))
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(co), _ptr(d))
+        r.gpu_getxc_(_i(isg), _ptr(sg), C.byref(e), C.byref(a), C.byref(b), _ptr(o))
+        check()
+        return o, e.value, a.value, b.value
+
+    def xc_stats(self):
+        n, c, a, b = C.c_longlong(0), C.c_longlong(0), C.c_double(0), C.c_double(0)
+        lib().qb_last_xc_stats(C.byref(n), C.byref(c), C.byref(a), C.byref(b))
+        return dict(npts=n.value, nchunks=c.value, ms=a.value, ms_grid=b.value)
+
+    def xc_grid(self):
+        """(npts, 4) array of the kept grid points: x, y, z, weight."""
+        r = lib()
+        r.qb_xc_grid.restype = C.c_longlong
+        n = r.qb_xc_grid(None, C.c_longlong(0))
+        out = np.zeros((max(n, 1), 4))
+        r.qb_xc_grid(_ptr(out), C.c_longlong(n))
+        check()
+        return out[:n]
+
     def fock_stats(self):
         q, a, b = C.c_longlong(0), C.c_double(0), C.c_double(0)
         lib().qb_last_fock_stats(C.byref(q), C.byref(a), C.byref(b))
@@ -163,6 +194,19 @@ class Session:
 
     def close(self):
         lib().gpu_shutdown_()
+
+
+def xc_functional(method, rho, sigma):
+    """The closed-shell functional on the GPU at arrays rho (total density)
+    and sigma = |grad rho|^2: returns (f, df/drho, 4 df/dsigma)."""
+    r = lib()
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    sigma = np.ascontiguousarray(sigma, dtype=np.float64)
+    out = np.zeros(3 * rho.size)
+    r.qb_xc_functional(C.c_int(method), C.c_int(rho.size), _ptr(rho), _ptr(sigma), _ptr(out))
+    check()
+    out = out.reshape(-1, 3)
+    return out[:, 0].copy(), out[:, 1].copy(), out[:, 2].copy()
 
 
 def build_pairlist_host(basis, YCutoff):

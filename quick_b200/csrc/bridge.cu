@@ -23,6 +23,7 @@
 #include "qb_internal.h"
 #include "schwarz.cuh"
 #include "grad_common.cuh"
+#include "xc/xc_api.h"
 
 namespace qb {
 
@@ -63,6 +64,9 @@ struct Context {
     int nshell = 0, nprim = 0, jshell = 0, jbasis = 0, maxcontract = 0;
     std::vector<int> kstart, katom, kprim, Ksumtype, Qnumber, Qstart, Qfinal, Qsbasis, Qfbasis, KLMN;
     std::vector<double> gccoeff, gcexpo, cons;
+    std::vector<int> ncontract, itype, ncenter;     // per basis function (XC quadrature)
+    std::vector<double> aexp, dcoeff;
+    long long geom_version = 0;                     // bumped by every coordinate or basis upload
     bool have_basis = false;
     int Qshell = 0, maxL = 0;
     std::vector<int> sorted_Q, sorted_Qnumber;
@@ -97,11 +101,13 @@ struct Context {
     bool have_grad = false;
     // stats
     long long last_quartets = 0;
+    XcResult last_xc;
     double last_ms_eri = 0, last_ms_screen = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 unsigned long long g_launches = 0;   // kernels launched by this library
+static long long g_geom_counter = 0; // process-wide, so a cached XC grid never outlives its molecule
 static Context* g = nullptr;
 static int g_status = 0;
 static std::string g_err;
@@ -617,6 +623,7 @@ void gpu_shutdown_(void)
     c.d_quartets.release();
     for (auto& e : c.ev)
         if (e) cudaEventDestroy(e), e = nullptr;
+    xc_release();
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
     delete g;
     g = nullptr;
@@ -670,6 +677,7 @@ void gpu_upload_xyz_(double* atom_xyz)
 {
     Context& c = ctx();
     c.xyz.assign(atom_xyz, atom_xyz + 3 * c.natom);
+    c.geom_version = ++g_geom_counter;
 }
 
 void gpu_upload_atom_and_chg_(int* atom, double* atom_chg)
@@ -705,8 +713,14 @@ void gpu_upload_basis_(int* nshell, int* nprim, int* jshell, int* jbasis, int* m
     c.gccoeff.assign(gccoeff, gccoeff + (size_t)MAXPRIM * nb);
     c.gcexpo.assign(gcexpo, gcexpo + (size_t)MAXPRIM * nb);
     c.cons.assign(cons, cons + nb);
-    (void)ncontract; (void)itype; (void)aexp; (void)dcoeff; (void)first_basis_function; (void)last_basis_function;
-    (void)first_shell_basis_function; (void)last_shell_basis_function; (void)ncenter; (void)ktype; (void)kshell;
+    c.ncontract.assign(ncontract, ncontract + nb);
+    c.itype.assign(itype, itype + 3 * nb);
+    c.ncenter.assign(ncenter, ncenter + nb);
+    c.aexp.assign(aexp, aexp + (size_t)c.maxcontract * nb);
+    c.dcoeff.assign(dcoeff, dcoeff + (size_t)c.maxcontract * nb);
+    c.geom_version = ++g_geom_counter;
+    (void)first_basis_function; (void)last_basis_function;
+    (void)first_shell_basis_function; (void)last_shell_basis_function; (void)ktype; (void)kshell;
     for (int s = 0; s < ns; s++) {
         if (c.kprim[s] < 1 || c.kprim[s] > MAXPRIM) {
             set_error(1, "shell %d has %d primitives (1..%d supported)", s + 1, c.kprim[s], MAXPRIM);
@@ -817,6 +831,67 @@ int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out)
     return fock_build(c, d_o_in, d_o_out);
 }
 
+int qb_xc_device(const double* d_dense, const double* sigrad2, double* d_vxc, double* exc, double* nalpha)
+{
+    Context& c = ctx();
+    if (require(c.have_basis && !c.xyz.empty(), "basis and coordinates must be uploaded before qb_xc_device")) return 1;
+    XcInputs in;
+    in.natom = c.natom;
+    in.nbasis = c.nbasis;
+    in.maxcontract = c.maxcontract;
+    in.method = c.method;
+    in.xyz = c.xyz.data();
+    in.iattype = c.iattype.data();
+    in.ncenter = c.ncenter.data();
+    in.itype = c.itype.data();
+    in.ncontract = c.ncontract.data();
+    in.aexp = c.aexp.data();
+    in.dcoeff = c.dcoeff.data();
+    in.sigrad2 = sigrad2;
+    in.geom_version = c.geom_version;
+    in.stream = c.stream;
+    XcResult r;
+    if (int rc = xc_quadrature(in, d_dense, d_vxc, &r)) return rc;
+    c.last_xc = r;
+    *exc = r.exc;
+    *nalpha = r.nalpha;
+    return 0;
+}
+
+int qb_last_xc_stats(long long* npts, long long* nchunks, double* ms, double* ms_grid)
+{
+    Context& c = ctx();
+    *npts = c.last_xc.npts;
+    *nchunks = c.last_xc.nchunks;
+    *ms = c.last_xc.ms;
+    *ms_grid = c.last_xc.ms_grid;
+    return 0;
+}
+
+long long qb_xc_grid(double* xyzw, long long cap) { return xc_grid_points(xyzw, cap); }
+
+int qb_xc_functional(int method, int n, const double* rho, const double* sigma, double* out)
+{
+    Context& c = ctx();
+    if (require(c.inited, "gpu_init_ must precede qb_xc_functional")) return 1;
+    if (n <= 0) return 0;
+    DevBuf<double> r, s, o;
+    CK(r.alloc(n));
+    CK(s.alloc(n));
+    CK(o.alloc(3 * (size_t)n));
+    CK(cudaMemcpyAsync(r.p, rho, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(s.p, sigma, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    int rc = xc_functional_device(method, n, r.p, s.p, o.p, c.stream);
+    if (!rc) {
+        CK(cudaMemcpyAsync(out, o.p, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+    }
+    r.release();
+    s.release();
+    o.release();
+    return rc;
+}
+
 int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen)
 {
     Context& c = ctx();
@@ -885,10 +960,64 @@ void gpu_grad_(double* grad)
     }
     for (size_t k = 0; k < g2.size(); k++) grad[k] = c.grad_host[k] + g2[k];
 }
+// Eelxc, aelec, belec <- input + grid sums; o <- symmetrised lower triangle
+// of (O as uploaded + V_xc)  (QUICK: gpu.cu:1866-1975 with getxc_kernel).
 void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double* belec, double* o)
 {
-    (void)isg; (void)sigrad2; (void)Eelxc; (void)aelec; (void)belec; (void)o;
-    set_error(21, "gpu_getxc_: XC quadrature not available in this build yet");
+    Context& c = ctx();
+    if (require(c.have_calc, "gpu_upload_calculated_ must precede gpu_getxc_")) return;
+    if (require(c.have_basis && !c.xyz.empty(), "basis and coordinates must be uploaded before gpu_getxc_")) return;
+    if (*isg != 1) {
+        // QUICK's GPU path builds no grid points for SG0 (gridFormSG0 is
+        // commented out, gpu_getxc.cu:117-121) and silently returns zeros.
+        set_error(1, "gpu_getxc_: only the SG1 grid (isg = 1) is implemented, got isg = %d", *isg);
+        return;
+    }
+    const size_t nn = (size_t)c.nbasis * c.nbasis;
+    if (c.d_dense_raw.alloc(nn) != cudaSuccess || c.d_o_out.alloc(nn) != cudaSuccess) {
+        set_error(2, "cannot allocate %zu-element matrices", nn);
+        return;
+    }
+    if (cudaMemcpyAsync(c.d_dense_raw.p, c.dense_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
+        cudaMemsetAsync(c.d_o_out.p, 0, nn * sizeof(double), c.stream) != cudaSuccess) {
+        set_error(2, "upload of the density failed");
+        return;
+    }
+    XcInputs in;
+    in.natom = c.natom;
+    in.nbasis = c.nbasis;
+    in.maxcontract = c.maxcontract;
+    in.method = c.method;
+    in.xyz = c.xyz.data();
+    in.iattype = c.iattype.data();
+    in.ncenter = c.ncenter.data();
+    in.itype = c.itype.data();
+    in.ncontract = c.ncontract.data();
+    in.aexp = c.aexp.data();
+    in.dcoeff = c.dcoeff.data();
+    in.sigrad2 = sigrad2;
+    in.geom_version = c.geom_version;
+    in.stream = c.stream;
+    XcResult r;
+    if (xc_quadrature(in, c.d_dense_raw.p, c.d_o_out.p, &r)) return;
+    c.last_xc = r;
+    std::vector<double> v(nn);
+    if (cudaMemcpyAsync(v.data(), c.d_o_out.p, nn * sizeof(double), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+        cudaStreamSynchronize(c.stream) != cudaSuccess) {
+        set_error(2, "download of V_xc failed");
+        return;
+    }
+    const int n = c.nbasis;
+    for (int i = 0; i < n; i++)
+        for (int j = i; j < n; j++) {
+            const size_t lo = (size_t)j + (size_t)i * n;   // (j, i), j >= i
+            const double val = c.o_host[lo] + v[lo];
+            o[(size_t)i + (size_t)j * n] = val;
+            o[lo] = val;
+        }
+    *Eelxc += r.exc;
+    *aelec += r.nalpha;
+    *belec += r.nalpha;
 }
 int gpu_schwarz_(double* YCutoff, double* cutPrim)
 {

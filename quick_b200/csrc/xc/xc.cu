@@ -1,0 +1,762 @@
+// Exchange-correlation quadrature on QUICK's SG1 grid, B200 layout.
+//
+// QUICK (src/cuda/gpu_getxc.cu:91-265) runs one thread per grid point that
+// rebuilds its Lebedev sphere, evaluates every basis function pair with
+// `pteval` for the density (O(nbasis^2) calls) and again for the operator,
+// and adds each V_ij term with a 64-bit atomic.  Here the same quantities
+// are computed in three phases:
+//
+//  1. Grid (once per geometry): one thread per point of the SG1 grid
+//     (atom x 50 radial shells x 6/38/86/194 Lebedev points, partitioned as
+//     gridFormSG1, gpu_getxc.cu:270-329) computes its position and its
+//     Stratmann-Scuseria-Frisch weight (SSW, :331-454).  Points whose weight
+//     is not above the density cutoff are dropped, the rest are sorted into
+//     spatial chunks, and each chunk gets the ascending list of basis
+//     functions whose radius of significance reaches its bounding box.
+//  2. Per call and chunk (P points, nb functions):
+//       basis kernel  -> Phi, dPhi/dx, dPhi/dy, dPhi/dz   (P x nb each)
+//       DGEMM          T = [Phi; dPhi] * U^T, U the upper triangle of D
+//                      with the diagonal halved (denspt's pair order)
+//       point kernel   rho_alpha, grad rho_alpha, the functional, and the
+//                      operator factors chi = w (f_rho/2 phi + f_sig4 g.grad phi)
+//       DGEMM          M = [Phi'; chi']^T [chi; Phi]
+//       scatter        V(j, i) += M(i, j) for i <= j
+//  3. Deterministic reductions of the per-point energy and electron count.
+//
+// The screening is QUICK's: pteval returns zeros outside sigrad2; denspt
+// skips row i when |D_ii| < cut or |phi_i + dphi_i/dx + dphi_i/dy +
+// dphi_i/dz| < cut (gpu_getxc.cu:551-556); a point contributes only if its
+// weight and its alpha density exceed cut (:163, :170); the operator loop
+// skips row i unless |phi_i + sum dphi_i| > cut (:241).  cut is QUICK's GPU
+// DMCutoff, 1e-9 (src/cuda/gpu.cu:370).
+#include <cublas_v2.h>
+
+#include <cstdarg>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "gen/xc_tables.h"
+#include "qb_internal.h"
+#include "xc/xc_api.h"
+#include "xc/xc_functional.cuh"
+
+namespace qb {
+
+constexpr double kXcCut = 1.0e-9;
+constexpr int kXcChunkPoints = 2048;
+constexpr double kXcCell = 4.0;          // bohr, edge of the sorting cells
+constexpr double kXcChunkSpan = 9.0;     // bohr, max bounding-box diagonal of a merged chunk
+
+struct XcShell {
+    int atom, rad, leb;   // leb: index into kXcLebOrders
+    int begin;            // first point
+};
+
+struct XcGridParams {
+    const XcShell* shells;
+    int nshell;
+    int npts;
+    const double4* leb_pts;   // x, y, z, 4 pi w of the four spheres, concatenated
+    const int* leb_off;
+    const double4* atoms;     // x, y, z, distance to the nearest other atom
+    const double* atom_rad;   // SG-1 radius of each atom
+    int natom;
+    double4* out;             // x, y, z, weight
+};
+
+struct XcBasisParams {
+    const double4* center;    // per basis function: centre x, y, z and sigrad2
+    const int4* itype;        // per basis function: i, j, k, ncontract
+    const double* aexp;       // (maxcontract, nbasis)
+    const double* dcoeff;
+    int maxcontract;
+};
+
+// ---------------------------------------------------------------- grid
+__device__ __forceinline__ double ssf_cell(double mu)
+{
+    // Stratmann-Scuseria-Frisch cell function with a = 0.64
+    if (mu >= 0.64) return 0.0;
+    if (mu < -0.64) return 1.0;
+    double t = mu / 0.64;
+    double t2 = t * t;
+    double g = t * (35.0 + t2 * (-35.0 + t2 * (21.0 - 5.0 * t2))) / 16.0;
+    return 0.5 * (1.0 - g);
+}
+
+__device__ __forceinline__ double dist3(double ax, double ay, double az, double bx, double by, double bz)
+{
+    double dx = ax - bx, dy = ay - by, dz = az - bz;
+    return sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+// SSW weight of a point owned by atom `parent` (gpu_getxc.cu:331-454).
+__device__ double ssw_weight(double gx, double gy, double gz, int parent, const double4* atoms, int natom)
+{
+    if (natom == 1) return 1.0;
+    const double4 P = atoms[parent];
+    const double rpg = dist3(gx, gy, gz, P.x, P.y, P.z);
+    if (rpg < 0.18 * P.w) return 1.0;   // inside 0.5 (1 - a) of the nearest-neighbour distance
+    double wp = 1.0;
+    for (int j = 0; j < natom && wp != 0.0; j++) {
+        if (j == parent) continue;
+        const double4 J = atoms[j];
+        double rjg = dist3(gx, gy, gz, J.x, J.y, J.z);
+        double rij = dist3(P.x, P.y, P.z, J.x, J.y, J.z);
+        wp *= ssf_cell((rpg - rjg) / rij);
+    }
+    if (wp == 0.0) return 0.0;
+    double total = wp;
+    for (int i = 0; i < natom; i++) {
+        if (i == parent) continue;
+        const double4 I = atoms[i];
+        double rig = dist3(gx, gy, gz, I.x, I.y, I.z);
+        double wi = 1.0;
+        for (int j = 0; j < natom && wi != 0.0; j++) {
+            if (j == i) continue;
+            const double4 J = atoms[j];
+            double rjg = dist3(gx, gy, gz, J.x, J.y, J.z);
+            double rij = dist3(I.x, I.y, I.z, J.x, J.y, J.z);
+            wi *= ssf_cell((rig - rjg) / rij);
+        }
+        total += wi;
+    }
+    return wp / total;
+}
+
+__global__ void xc_grid_kernel(XcGridParams p)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.npts) return;
+    int lo = 0, hi = p.nshell - 1;   // last shell with begin <= i
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (p.shells[mid].begin <= i) lo = mid; else hi = mid - 1;
+    }
+    const XcShell s = p.shells[lo];
+    const double4 ang = p.leb_pts[p.leb_off[s.leb] + (i - s.begin)];
+    const double4 A = p.atoms[s.atom];
+    const double R = p.atom_rad[s.atom];
+    const double rr = R * c_xc_rgrid[s.rad];
+    const double gx = A.x + rr * ang.x, gy = A.y + rr * ang.y, gz = A.z + rr * ang.z;
+    const double w = ssw_weight(gx, gy, gz, s.atom, p.atoms, p.natom) * ang.w * (R * R * R * c_xc_rweight[s.rad]);
+    p.out[i] = make_double4(gx, gy, gz, w);
+}
+
+// ---------------------------------------------------------------- per call
+// Cartesian factor x^n with its neighbours x^(n-1) and x^(n+1), as pteval
+// uses them (n = 0: 0, 1, x).
+__device__ __forceinline__ void cart_pows(double x, int n, double& xm, double& xi, double& xp)
+{
+    if (n == 0) {
+        xm = 0.0;
+        xi = 1.0;
+        xp = x;
+        return;
+    }
+    xm = 1.0;
+    for (int k = 1; k < n; k++) xm *= x;
+    xi = xm * x;
+    xp = xi * x;
+}
+
+// Phi and its gradient for P points x nb basis functions of one chunk
+// (pteval, gpu_getxc.cu:456-534).  Column a of B5 (leading dimension 5P)
+// holds rows [P, 2P) phi, [2P, 3P) dphi/dx, [3P, 4P) dphi/dy, [4P, 5P) dphi/dz.
+__global__ void xc_basis_kernel(XcBasisParams B, const double4* __restrict__ pts, int P, const int* __restrict__ funcs,
+                                int nb, double* __restrict__ B5)
+{
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)P * nb) return;
+    const int a = (int)(idx / P), g = (int)(idx - (long long)a * P);
+    const int f = funcs[a];
+    const double4 pt = pts[g];
+    const double4 c = B.center[f];
+    const int4 t = B.itype[f];
+    const double x = pt.x - c.x, y = pt.y - c.y, z = pt.z - c.z;
+    const double r2 = x * x + y * y + z * z;
+    double phi = 0.0, dx = 0.0, dy = 0.0, dz = 0.0;
+    if (r2 <= c.w) {
+        double xm, xi, xp, ym, yi, yp, zm, zi, zp;
+        cart_pows(x, t.x, xm, xi, xp);
+        cart_pows(y, t.y, ym, yi, yp);
+        cart_pows(z, t.z, zm, zi, zp);
+        const double* al = B.aexp + (size_t)f * B.maxcontract;
+        const double* dc = B.dcoeff + (size_t)f * B.maxcontract;
+        double s = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int k = 0; k < t.w; k++) {
+            const double e = dc[k] * exp(-al[k] * r2);
+            const double m2a = -2.0 * al[k];
+            s += e;
+            sx += e * (m2a * xp + t.x * xm);
+            sy += e * (m2a * yp + t.y * ym);
+            sz += e * (m2a * zp + t.z * zm);
+        }
+        phi = s * xi * yi * zi;
+        dx = sx * yi * zi;
+        dy = sy * xi * zi;
+        dz = sz * xi * yi;
+    }
+    double* col = B5 + (size_t)a * 5 * P;
+    col[P + g] = phi;
+    col[2 * P + g] = dx;
+    col[3 * P + g] = dy;
+    col[4 * P + g] = dz;
+}
+
+// U(a, b) = D(f_a, f_b) for b > a, D(f_a, f_a) / 2 for a == b, 0 below:
+// denspt's pair sum (gpu_getxc.cu:551-575) as rho = sum_a phi_a (U Phi)_a.
+__global__ void xc_usub_kernel(const double* __restrict__ dense, int n, const int* __restrict__ funcs, int nb,
+                               double* __restrict__ U)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nb * nb) return;
+    const int a = idx % nb, b = idx / nb;
+    const int fa = funcs[a], fb = funcs[b];
+    double v = 0.0;
+    if (b > a) v = dense[fa + (size_t)fb * n];
+    else if (b == a) v = 0.5 * dense[fa + (size_t)fa * n];
+    U[idx] = v;
+}
+
+struct XcPointParams {
+    const double4* pts;        // chunk's points
+    int P, nb;
+    const int* funcs;
+    const double* dense;
+    int n;
+    double* B5;                // ld 5P
+    const double* T;           // ld 4P: (U [Phi; dPhi]^T)^T
+    double* L;                 // ld 2P
+    double* e_pt;              // chunk's slice of the per-point arrays
+    double* n_pt;
+    int method;
+};
+
+// One thread per point: rho_alpha and its gradient, the functional, and the
+// operator factors (gpu_grid_xc, gpu_getxc.cu:144-265).
+__global__ void xc_point_kernel(XcPointParams q)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= q.P) return;
+    const int P = q.P;
+    const size_t ld5 = 5 * (size_t)P, ld4 = 4 * (size_t)P, ld2 = 2 * (size_t)P;
+    double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int a = 0; a < q.nb; a++) {
+        const int f = q.funcs[a];
+        const double dii = q.dense[f + (size_t)f * q.n];
+        const double* col = q.B5 + a * ld5;
+        const double phi = col[P + g], dx = col[2 * P + g], dy = col[3 * P + g], dz = col[4 * P + g];
+        if (fabs(dii) >= kXcCut && fabs(phi + dx + dy + dz) >= kXcCut) {
+            const double* tc = q.T + a * ld4;
+            const double t0 = tc[g], tx = tc[P + g], ty = tc[2 * P + g], tz = tc[3 * P + g];
+            rho += phi * t0;
+            gx += phi * tx + dx * t0;
+            gy += phi * ty + dy * t0;
+            gz += phi * tz + dz * t0;
+        }
+    }
+    const double w = q.pts[g].w;
+    const bool ok = rho > kXcCut;
+    double frho = 0.0, fs4 = 0.0;
+    if (ok) {
+        const double sigma = 4.0 * (gx * gx + gy * gy + gz * gz);
+        const double f = xc_eval(q.method, 2.0 * rho, sigma, &frho, &fs4);
+        q.e_pt[g] = f * w;
+        q.n_pt[g] = w * rho;
+    } else {
+        q.e_pt[g] = 0.0;
+        q.n_pt[g] = 0.0;
+    }
+    const double hx = fs4 * gx, hy = fs4 * gy, hz = fs4 * gz, hr = 0.5 * frho;
+    for (int a = 0; a < q.nb; a++) {
+        double* col = q.B5 + a * ld5;
+        const double phi = col[P + g], dx = col[2 * P + g], dy = col[3 * P + g], dz = col[4 * P + g];
+        const double chi = ok ? w * (hr * phi + hx * dx + hy * dy + hz * dz) : 0.0;
+        const bool m = ok && fabs(phi + dx + dy + dz) > kXcCut;
+        col[g] = chi;
+        double* lc = q.L + a * ld2;
+        lc[g] = m ? phi : 0.0;
+        lc[P + g] = m ? chi : 0.0;
+    }
+}
+
+// V(f_b, f_a) += M(a, b) for a <= b (lower triangle, column-major).
+__global__ void xc_scatter_kernel(const double* __restrict__ M, int nb, const int* __restrict__ funcs, int n,
+                                  double* __restrict__ V)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nb * nb) return;
+    const int a = idx % nb, b = idx / nb;
+    if (a > b) return;
+    V[funcs[b] + (size_t)funcs[a] * n] += M[idx];
+}
+
+// Fixed-order sum of two arrays by one block (deterministic).
+__global__ void xc_reduce_kernel(const double* __restrict__ x, const double* __restrict__ y, long long n,
+                                 double* __restrict__ out)
+{
+    __shared__ double sx[1024], sy[1024];
+    double ax = 0.0, ay = 0.0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        ax += x[i];
+        ay += y[i];
+    }
+    sx[threadIdx.x] = ax;
+    sy[threadIdx.x] = ay;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sx[threadIdx.x] += sx[threadIdx.x + s];
+            sy[threadIdx.x] += sy[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sx[0];
+        out[1] = sy[0];
+    }
+}
+
+__global__ void xc_functional_kernel(int method, int n, const double* rho, const double* sigma, double* out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double fr, fs;
+    double f = xc_eval(method, rho[i], sigma[i], &fr, &fs);
+    out[3 * i] = f;
+    out[3 * i + 1] = fr;
+    out[3 * i + 2] = fs;
+}
+
+// ---------------------------------------------------------------- host
+template <class T>
+struct XcBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count)
+    {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        n = count;
+        return cudaMalloc((void**)&p, std::max<size_t>(count, 1) * sizeof(T));
+    }
+    cudaError_t upload(const std::vector<T>& v, cudaStream_t st)
+    {
+        cudaError_t e = alloc(v.size());
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct XcChunk {
+    int p0, P;        // points [p0, p0 + P) of the sorted point array
+    int f0, nb;       // functions [f0, f0 + nb) of the concatenated lists
+};
+
+struct XcState {
+    bool valid = false;
+    long long geom_version = -1;
+    std::vector<double> sigrad2;
+    int nbasis = 0;
+    long long npts = 0;
+    std::vector<XcChunk> chunks;
+    int maxP = 0, maxNb = 0;
+    XcBuf<double4> d_pts, d_center;
+    XcBuf<int4> d_itype;
+    XcBuf<double> d_aexp, d_dcoeff;
+    XcBuf<int> d_funcs;
+    // work
+    XcBuf<double> d_B5, d_T, d_L, d_U, d_M, d_e, d_n, d_sum;
+    cublasHandle_t blas = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+static XcState* g_xc = nullptr;
+
+static XcState& xc_state()
+{
+    if (!g_xc) g_xc = new XcState();
+    return *g_xc;
+}
+
+static int xc_fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    return report_error(code, buf);
+}
+
+#define XCK(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return xc_fail(2, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+    } while (0)
+#define XBL(call)                                                                 \
+    do {                                                                          \
+        cublasStatus_t s_ = (call);                                               \
+        if (s_ != CUBLAS_STATUS_SUCCESS) return xc_fail(2, "%s failed: %d", #call, (int)s_); \
+    } while (0)
+
+// Points of one Lebedev-Laikov orbit (octahedral generator codes 1-6).
+static void leb_expand(const LebOrbit& o, std::vector<double4>& out)
+{
+    const double v = o.v;
+    auto add = [&](double x, double y, double z) { out.push_back(make_double4(x, y, z, v)); };
+    const double s2[2] = {1.0, -1.0};
+    switch (o.code) {
+    case 1:   // (+-1, 0, 0) and permutations
+        for (double s : s2) add(s, 0, 0);
+        for (double s : s2) add(0, s, 0);
+        for (double s : s2) add(0, 0, s);
+        break;
+    case 2: {   // (0, +-a, +-a), a = 1/sqrt(2), and permutations
+        const double a = sqrt(0.5);
+        for (double s : s2) for (double t : s2) add(0, s * a, t * a);
+        for (double s : s2) for (double t : s2) add(s * a, 0, t * a);
+        for (double s : s2) for (double t : s2) add(s * a, t * a, 0);
+        break;
+    }
+    case 3: {   // (+-a, +-a, +-a), a = 1/sqrt(3)
+        const double a = sqrt(1.0 / 3.0);
+        for (double s : s2) for (double t : s2) for (double u : s2) add(s * a, t * a, u * a);
+        break;
+    }
+    case 4: {   // (+-a, +-a, +-b), b = sqrt(1 - 2 a^2), and permutations
+        const double a = o.a, b = sqrt(1.0 - 2.0 * a * a);
+        for (double s : s2) for (double t : s2) for (double u : s2) add(s * a, t * a, u * b);
+        for (double s : s2) for (double t : s2) for (double u : s2) add(s * a, t * b, u * a);
+        for (double s : s2) for (double t : s2) for (double u : s2) add(s * b, t * a, u * a);
+        break;
+    }
+    case 5: {   // (+-a, +-b, 0), b = sqrt(1 - a^2), and permutations
+        const double a = o.a, b = sqrt(1.0 - a * a);
+        for (double s : s2) for (double t : s2) add(s * a, t * b, 0);
+        for (double s : s2) for (double t : s2) add(s * b, t * a, 0);
+        for (double s : s2) for (double t : s2) add(s * a, 0, t * b);
+        for (double s : s2) for (double t : s2) add(s * b, 0, t * a);
+        for (double s : s2) for (double t : s2) add(0, s * a, t * b);
+        for (double s : s2) for (double t : s2) add(0, s * b, t * a);
+        break;
+    }
+    case 6: {   // (+-a, +-b, +-c), c = sqrt(1 - a^2 - b^2), all permutations
+        const double a = o.a, b = o.b, c = sqrt(1.0 - a * a - b * b);
+        const double perm[6][3] = {{a, b, c}, {a, c, b}, {b, a, c}, {b, c, a}, {c, a, b}, {c, b, a}};
+        for (auto& p : perm)
+            for (double s : s2) for (double t : s2) for (double u : s2) add(s * p[0], t * p[1], u * p[2]);
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// SG-1 angular order for atom type Z at radial position r / R (gridFormSG1).
+static int sg1_leb_index(int Z, double r)
+{
+    const int row = Z <= 2 ? 0 : (Z <= 10 ? 1 : 2);
+    const double* al = kXcAlpha[row];
+    if (r < al[0]) return 0;
+    if (r < al[1]) return 1;
+    if (r < al[2]) return 2;
+    if (r < al[3]) return 3;
+    return 2;
+}
+
+static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
+{
+    cudaStream_t st = in.stream;
+    const int natom = in.natom, nb = in.nbasis;
+    for (int a = 0; a < natom; a++)
+        if (in.iattype[a] < 1 || in.iattype[a] > kXcMaxZ)
+            return xc_fail(1, "gpu_getxc_: atom %d has atomic number %d; the SG1 grid covers H..Ar", a + 1,
+                           in.iattype[a]);
+    // Lebedev spheres, weights times 4 pi
+    std::vector<double4> leb;
+    std::vector<int> leb_off(4);
+    for (int k = 0; k < 4; k++) {
+        leb_off[k] = (int)leb.size();
+        for (int o = 0; o < kXcLebNOrbits[k]; o++) leb_expand(kXcLebOrbits[k][o], leb);
+        if ((int)leb.size() - leb_off[k] != kXcLebOrders[k])
+            return xc_fail(3, "Lebedev sphere %d has %d points", kXcLebOrders[k], (int)leb.size() - leb_off[k]);
+    }
+    for (auto& p : leb) p.w *= 12.56637061435917295385;
+    // atoms: coordinates and nearest-neighbour distance (capped at 1e3 like SSW)
+    std::vector<double4> atoms(natom);
+    std::vector<double> arad(natom);
+    for (int a = 0; a < natom; a++) {
+        double nn = 1.0e3;
+        for (int b = 0; b < natom; b++) {
+            if (b == a) continue;
+            double dx = in.xyz[3 * a] - in.xyz[3 * b], dy = in.xyz[3 * a + 1] - in.xyz[3 * b + 1],
+                   dz = in.xyz[3 * a + 2] - in.xyz[3 * b + 2];
+            nn = std::min(nn, sqrt(dx * dx + dy * dy + dz * dz));
+        }
+        atoms[a] = make_double4(in.xyz[3 * a], in.xyz[3 * a + 1], in.xyz[3 * a + 2], nn);
+        arad[a] = kXcRadius[in.iattype[a] - 1];
+    }
+    std::vector<XcShell> shells;
+    long long total = 0;
+    for (int a = 0; a < natom; a++)
+        for (int j = 0; j < kXcRadial; j++) {
+            int k = sg1_leb_index(in.iattype[a], kXcRGrid[j]);
+            shells.push_back({a, j, k, (int)total});
+            total += kXcLebOrders[k];
+        }
+    if (total >= (1LL << 31)) return xc_fail(1, "gpu_getxc_: %lld grid points", total);
+    XcBuf<double4> d_leb, d_atoms, d_all;
+    XcBuf<int> d_leb_off;
+    XcBuf<XcShell> d_shells;
+    XcBuf<double> d_arad;
+    XCK(d_leb.upload(leb, st));
+    XCK(d_leb_off.upload(leb_off, st));
+    XCK(d_atoms.upload(atoms, st));
+    XCK(d_arad.upload(arad, st));
+    XCK(d_shells.upload(shells, st));
+    XCK(d_all.alloc(total));
+    XcGridParams gp{d_shells.p, (int)shells.size(), (int)total, d_leb.p, d_leb_off.p, d_atoms.p, d_arad.p, natom, d_all.p};
+    XCK(cudaEventRecord(S.ev[2], st));
+    xc_grid_kernel<<<(unsigned)((total + 127) / 128), 128, 0, st>>>(gp);
+    ++g_launches;
+    XCK(cudaGetLastError());
+    XCK(cudaEventRecord(S.ev[3], st));
+    std::vector<double4> all(total);
+    XCK(cudaMemcpyAsync(all.data(), d_all.p, total * sizeof(double4), cudaMemcpyDeviceToHost, st));
+    XCK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, S.ev[2], S.ev[3]);
+    *ms_grid = ms;
+    d_leb.release(); d_leb_off.release(); d_atoms.release(); d_arad.release(); d_shells.release(); d_all.release();
+
+    // keep points with weight above the cutoff, sort them into cells
+    std::vector<double4> kept;
+    kept.reserve(total);
+    for (auto& p : all)
+        if (p.w > kXcCut) kept.push_back(p);
+    const long long np = (long long)kept.size();
+    std::vector<unsigned long long> key(np);
+    for (long long i = 0; i < np; i++) {
+        auto cell = [](double v) {
+            long long c = (long long)floor(v / kXcCell) + (1LL << 20);
+            return (unsigned long long)std::min<long long>(std::max<long long>(c, 0), (1LL << 21) - 1);
+        };
+        key[i] = (cell(kept[i].x) << 42) | (cell(kept[i].y) << 21) | cell(kept[i].z);
+    }
+    std::vector<long long> order(np);
+    std::iota(order.begin(), order.end(), 0LL);
+    std::stable_sort(order.begin(), order.end(), [&](long long a, long long b) { return key[a] < key[b]; });
+    std::vector<double4> pts(np);
+    for (long long i = 0; i < np; i++) pts[i] = kept[order[i]];
+
+    // chunks: whole cells merged while small and compact, big cells split
+    struct Box { double lo[3], hi[3]; };
+    auto grow = [](Box& b, const double4& p) {
+        b.lo[0] = std::min(b.lo[0], p.x); b.hi[0] = std::max(b.hi[0], p.x);
+        b.lo[1] = std::min(b.lo[1], p.y); b.hi[1] = std::max(b.hi[1], p.y);
+        b.lo[2] = std::min(b.lo[2], p.z); b.hi[2] = std::max(b.hi[2], p.z);
+    };
+    auto empty_box = []() { Box b; for (int d = 0; d < 3; d++) b.lo[d] = 1e300, b.hi[d] = -1e300; return b; };
+    auto diag = [](const Box& b) {
+        double s = 0;
+        for (int d = 0; d < 3; d++) s += (b.hi[d] - b.lo[d]) * (b.hi[d] - b.lo[d]);
+        return sqrt(s);
+    };
+    std::vector<std::pair<long long, long long>> ranges;   // [begin, end) point ranges
+    std::vector<Box> boxes;
+    {
+        long long i = 0;
+        long long cb = -1;
+        Box cbox = empty_box();
+        while (i < np) {
+            long long j = i;
+            Box b = empty_box();
+            while (j < np && key[order[j]] == key[order[i]]) grow(b, pts[j]), j++;
+            // split a big cell
+            for (long long s = i; s < j; s += kXcChunkPoints) {
+                long long e = std::min(j, s + kXcChunkPoints);
+                Box bb = empty_box();
+                for (long long t = s; t < e; t++) grow(bb, pts[t]);
+                Box m = cbox;
+                for (int d = 0; d < 3; d++) m.lo[d] = std::min(m.lo[d], bb.lo[d]), m.hi[d] = std::max(m.hi[d], bb.hi[d]);
+                if (cb >= 0 && (e - cb) <= kXcChunkPoints && diag(m) <= kXcChunkSpan) {
+                    ranges.back().second = e;
+                    boxes.back() = m;
+                    cbox = m;
+                } else {
+                    ranges.push_back({s, e});
+                    boxes.push_back(bb);
+                    cb = s;
+                    cbox = bb;
+                }
+            }
+            i = j;
+        }
+    }
+    // significant functions per chunk
+    std::vector<double> cx(nb), cy(nb), cz(nb);
+    for (int f = 0; f < nb; f++) {
+        int a = in.ncenter[f] - 1;
+        cx[f] = in.xyz[3 * a];
+        cy[f] = in.xyz[3 * a + 1];
+        cz[f] = in.xyz[3 * a + 2];
+    }
+    std::vector<int> funcs;
+    S.chunks.clear();
+    S.maxP = S.maxNb = 0;
+    for (size_t c = 0; c < ranges.size(); c++) {
+        const Box& b = boxes[c];
+        int f0 = (int)funcs.size();
+        for (int f = 0; f < nb; f++) {
+            double d2 = 0.0;
+            const double cc[3] = {cx[f], cy[f], cz[f]};
+            for (int d = 0; d < 3; d++) {
+                double e = std::max(0.0, std::max(b.lo[d] - cc[d], cc[d] - b.hi[d]));
+                d2 += e * e;
+            }
+            if (d2 <= in.sigrad2[f]) funcs.push_back(f);
+        }
+        int nbc = (int)funcs.size() - f0;
+        if (nbc == 0) continue;   // no basis function reaches these points: rho = 0
+        XcChunk ch{(int)ranges[c].first, (int)(ranges[c].second - ranges[c].first), f0, nbc};
+        S.chunks.push_back(ch);
+        S.maxP = std::max(S.maxP, ch.P);
+        S.maxNb = std::max(S.maxNb, nbc);
+    }
+    // basis tables
+    std::vector<double4> center(nb);
+    std::vector<int4> itp(nb);
+    for (int f = 0; f < nb; f++) {
+        center[f] = make_double4(cx[f], cy[f], cz[f], in.sigrad2[f]);
+        itp[f] = make_int4(in.itype[3 * f], in.itype[3 * f + 1], in.itype[3 * f + 2], in.ncontract[f]);
+        if (in.ncontract[f] < 1 || in.ncontract[f] > in.maxcontract)
+            return xc_fail(1, "gpu_getxc_: basis function %d has %d primitives", f + 1, in.ncontract[f]);
+    }
+    std::vector<double> aexp(in.aexp, in.aexp + (size_t)in.maxcontract * nb);
+    std::vector<double> dco(in.dcoeff, in.dcoeff + (size_t)in.maxcontract * nb);
+    XCK(S.d_pts.upload(pts, st));
+    XCK(S.d_center.upload(center, st));
+    XCK(S.d_itype.upload(itp, st));
+    XCK(S.d_aexp.upload(aexp, st));
+    XCK(S.d_dcoeff.upload(dco, st));
+    XCK(S.d_funcs.upload(funcs, st));
+    const size_t P = S.maxP, N = S.maxNb;
+    XCK(S.d_B5.alloc(5 * P * N));
+    XCK(S.d_T.alloc(4 * P * N));
+    XCK(S.d_L.alloc(2 * P * N));
+    XCK(S.d_U.alloc(N * N));
+    XCK(S.d_M.alloc(N * N));
+    XCK(S.d_e.alloc(np));
+    XCK(S.d_n.alloc(np));
+    XCK(S.d_sum.alloc(2));
+    XCK(cudaStreamSynchronize(st));
+    S.npts = np;
+    S.nbasis = nb;
+    S.geom_version = in.geom_version;
+    S.sigrad2.assign(in.sigrad2, in.sigrad2 + nb);
+    S.valid = true;
+    return 0;
+}
+
+int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResult* out)
+{
+    XcState& S = xc_state();
+    cudaStream_t st = in.stream;
+    if (in.method != 1 && in.method != 2)
+        return xc_fail(1, "gpu_getxc_: method %d has no XC functional (1 = B3LYP, 2 = BLYP)", in.method);
+    if (!S.ev[0])
+        for (auto& e : S.ev) XCK(cudaEventCreate(&e));
+    if (!S.blas) XBL(cublasCreate(&S.blas));
+    XBL(cublasSetStream(S.blas, st));
+    out->ms_grid = 0.0;
+    bool same = S.valid && S.geom_version == in.geom_version && S.nbasis == in.nbasis &&
+                std::equal(S.sigrad2.begin(), S.sigrad2.end(), in.sigrad2);
+    if (!same) {
+        S.valid = false;
+        if (int rc = xc_build_grid(S, in, &out->ms_grid)) return rc;
+    }
+    const int n = in.nbasis;
+    XCK(cudaEventRecord(S.ev[0], st));
+    XCK(cudaMemsetAsync(S.d_e.p, 0, std::max<long long>(S.npts, 1) * sizeof(double), st));
+    XCK(cudaMemsetAsync(S.d_n.p, 0, std::max<long long>(S.npts, 1) * sizeof(double), st));
+    XcBasisParams bp{S.d_center.p, S.d_itype.p, S.d_aexp.p, S.d_dcoeff.p, in.maxcontract};
+    const double one = 1.0, zero = 0.0;
+    for (const XcChunk& ch : S.chunks) {
+        const int P = ch.P, nb = ch.nb;
+        const int* funcs = S.d_funcs.p + ch.f0;
+        const double4* pts = S.d_pts.p + ch.p0;
+        long long work = (long long)P * nb;
+        xc_basis_kernel<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(bp, pts, P, funcs, nb, S.d_B5.p);
+        xc_usub_kernel<<<(nb * nb + 255) / 256, 256, 0, st>>>(d_dense, n, funcs, nb, S.d_U.p);
+        g_launches += 2;
+        XBL(cublasDgemm(S.blas, CUBLAS_OP_N, CUBLAS_OP_T, 4 * P, nb, nb, &one, S.d_B5.p + P, 5 * P, S.d_U.p, nb,
+                        &zero, S.d_T.p, 4 * P));
+        XcPointParams q{pts, P, nb, funcs, d_dense, n, S.d_B5.p, S.d_T.p, S.d_L.p, S.d_e.p + ch.p0,
+                        S.d_n.p + ch.p0, in.method};
+        xc_point_kernel<<<(P + 127) / 128, 128, 0, st>>>(q);
+        ++g_launches;
+        XBL(cublasDgemm(S.blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nb, 2 * P, &one, S.d_L.p, 2 * P, S.d_B5.p, 5 * P, &zero,
+                        S.d_M.p, nb));
+        xc_scatter_kernel<<<(nb * nb + 255) / 256, 256, 0, st>>>(S.d_M.p, nb, funcs, n, d_v);
+        ++g_launches;
+    }
+    xc_reduce_kernel<<<1, 1024, 0, st>>>(S.d_e.p, S.d_n.p, S.npts, S.d_sum.p);
+    ++g_launches;
+    XCK(cudaGetLastError());
+    XCK(cudaEventRecord(S.ev[1], st));
+    double sums[2];
+    XCK(cudaMemcpyAsync(sums, S.d_sum.p, sizeof sums, cudaMemcpyDeviceToHost, st));
+    XCK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, S.ev[0], S.ev[1]);
+    out->exc = sums[0];
+    out->nalpha = sums[1];
+    out->npts = S.npts;
+    out->nchunks = (long long)S.chunks.size();
+    out->ms = ms;
+    return 0;
+}
+
+int xc_functional_device(int method, int n, const double* d_rho, const double* d_sigma, double* d_out, cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    xc_functional_kernel<<<(n + 127) / 128, 128, 0, st>>>(method, n, d_rho, d_sigma, d_out);
+    ++g_launches;
+    XCK(cudaGetLastError());
+    XCK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+long long xc_grid_points(double* xyzw, long long cap)
+{
+    XcState& S = xc_state();
+    if (!S.valid) return 0;
+    long long n = std::min(cap, S.npts);
+    if (n > 0 && cudaMemcpy(xyzw, S.d_pts.p, n * sizeof(double4), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return S.npts;
+}
+
+void xc_release()
+{
+    if (!g_xc) return;
+    XcState& S = *g_xc;
+    S.d_pts.release(); S.d_center.release(); S.d_itype.release(); S.d_aexp.release(); S.d_dcoeff.release();
+    S.d_funcs.release(); S.d_B5.release(); S.d_T.release(); S.d_L.release(); S.d_U.release(); S.d_M.release();
+    S.d_e.release(); S.d_n.release(); S.d_sum.release();
+    S.valid = false;
+}
+
+}  // namespace qb

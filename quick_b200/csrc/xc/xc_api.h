@@ -1,0 +1,49 @@
+// Host interface of the XC quadrature (xc.cu) used by the gpu_getxc_ bridge.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace qb {
+
+struct XcInputs {
+    int natom = 0, nbasis = 0, maxcontract = 0;
+    int method = 1;                  // 1: B3LYP, 2: BLYP (QUICK's gpu_upload_method_ codes)
+    const double* xyz = nullptr;     // (3, natom), bohr
+    const int* iattype = nullptr;    // atomic numbers
+    const int* ncenter = nullptr;    // (nbasis), 1-based atom of each basis function
+    const int* itype = nullptr;      // (3, nbasis)
+    const int* ncontract = nullptr;  // (nbasis)
+    const double* aexp = nullptr;    // (maxcontract, nbasis)
+    const double* dcoeff = nullptr;  // (maxcontract, nbasis), normalised
+    const double* sigrad2 = nullptr; // (nbasis)
+    long long geom_version = 0;      // changes whenever coordinates or basis change
+    cudaStream_t stream = nullptr;
+};
+
+struct XcResult {
+    double exc = 0.0;       // sum of w f over the grid
+    double nalpha = 0.0;    // sum of w rho_alpha (QUICK's aelec; belec is the same)
+    long long npts = 0;     // grid points kept (weight above the cutoff)
+    long long nchunks = 0;  // point chunks with at least one significant basis function
+    double ms = 0.0;        // device time of the per-call phase
+    double ms_grid = 0.0;   // device time of the grid build (0 when cached)
+};
+
+// Accumulates V_xc into the lower triangle of d_v (column-major nbasis^2,
+// V(j, i) for j >= i; the caller zeroes it) from the density d_dense
+// (column-major nbasis^2).  Rebuilds the grid when geom_version or sigrad2
+// changed.  Returns 0 or a QUICK-bridge status code after reporting the
+// error.
+int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResult* out);
+
+// Evaluates the functional (xc_functional.cuh) at n (rho, sigma) pairs on the
+// device: out[3k] = f, out[3k+1] = df/drho, out[3k+2] = 4 df/dsigma.
+int xc_functional_device(int method, int n, const double* d_rho, const double* d_sigma, double* d_out,
+                         cudaStream_t st);
+
+// Grid of the last build, for checking: copies up to cap points (x, y, z, w)
+// in the order of the device arrays; returns the number of points.
+long long xc_grid_points(double* xyzw, long long cap);
+
+void xc_release();
+
+}  // namespace qb

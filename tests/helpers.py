@@ -26,3 +26,11 @@ def random_density(n, seed=0, scale=0.1):
     d = d + d.T
     d[np.diag_indices(n)] += 1.0
     return np.asfortranarray(d)
+
+
+def psd_density(n, nocc, seed=0, scale=0.3):
+    """A positive semi-definite closed-shell density 2 C C^T (so rho(r) >= 0
+    everywhere, as for a real density), C random (n x nocc)."""
+    rng = np.random.default_rng(seed)
+    c = rng.standard_normal((n, nocc)) * scale
+    return np.asfortranarray(2.0 * c @ c.T)
