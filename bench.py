@@ -29,6 +29,8 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(name="(H2O)32 6-31G** RHF Fock build", grid=(4, 4, 2), basis="6-31G**", seed=0,
                 integral_cutoff=1e-10, prim_limit=1e-20)
 SAMPLE = dict(name="(H2O)16 6-31G** RHF Fock build", grid=(4, 2, 2), basis="6-31G**", seed=0)
+# mixed-precision split: shell quartets whose Y_ab Y_cd DNMax bound is below this run in FP32
+MIXED_CUT = 1e-3
 
 
 def model_density(mol, basis, seed=0):
@@ -267,6 +269,37 @@ def run_ours(args, ws, rank, local):
     capi.check()
     e2e_ms = max_over_ranks(ec0.elapsed_time(ec1) / args.steps, ws)
 
+    # mixed precision: quartets with Y_ab Y_cd DNMax < MIXED_CUT in FP32, same
+    # density; error against this FP64 build
+    G64 = dOut.double().cpu().numpy().copy()
+    lib.qb_set_mixed_precision(capi.C.c_double(MIXED_CUT))
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    m0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    m1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    mix_eri = []
+    for i in range(args.steps):
+        flush.zero_()
+        m0[i].record(stream)
+        step()
+        m1[i].record(stream)
+        mix_eri.append(sess.fock_stats()["ms_eri"])
+    torch.cuda.synchronize()
+    barrier(ws)
+    mix_ms = max_over_ranks(float(np.mean([a.elapsed_time(c) for a, c in zip(m0, m1)])), ws)
+    split = sess.fock_split()
+    Gmx = dOut.double().cpu().numpy()
+    lib.qb_set_mixed_precision(capi.C.c_double(0.0))
+    Dn = np.ascontiguousarray(D)
+    mixed = {"value": quartets * ws / (mix_ms * 1e-3), "unit": "quartets/s", "ms_per_step": mix_ms,
+             "kernel_ms": float(np.mean(mix_eri)), "cut": MIXED_CUT,
+             "fp32_quartet_fraction": split["fp32"] / max(1, split["fp32"] + split["fp64"]),
+             "speedup_vs_fp64": ms / mix_ms,
+             "abs_dE2_vs_fp64_Eh": float(abs(0.5 * np.sum(Dn * (Gmx - G64)))),
+             "max_abs_dF_vs_fp64": float(np.abs(Gmx - G64).max())}
+
     mean_eri = float(np.mean(eri_ms))
     achieved = alg_flops / (mean_eri * 1e-3) / 1e12
     peak = peak64.value / 1e3
@@ -296,12 +329,125 @@ def run_ours(args, ws, rank, local):
                      "flops_per_step": alg_flops, "kernel_ms": mean_eri,
                      "screen_ms": float(np.mean(scr_ms))},
         "gpu_launches": int(launches),
+        "mixed": mixed,
     }
     if clk:
         out["clocks"] = clk
     if args.classes:
         out["classes"] = {"%d%d%d%d" % tuple(cl[4 * i:4 * i + 4]): [int(cq[i]), int(npq[i])] for i in range(k)}
     return out
+
+
+def measured_hbm_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback (6.65 TB/s)"
+
+
+def run_xc(args, ws, rank, local, sess=None):
+    """B3LYP XC quadrature (gpu_getxc_'s work, qb_xc_device) on the workload
+    molecule's SG1 grid: device time per call with the grid resident, L2
+    flushed before every call; end to end through gpu_getxc_ with host
+    buffers."""
+    import torch
+    from quick_b200 import capi
+    from quick_b200.basis import build_basis, sigrad2
+    from quick_b200.molecule import water_cluster
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    m = water_cluster(WORKLOAD["grid"], seed=WORKLOAD["seed"])
+    b = build_basis(m.symbols, WORKLOAD["basis"])
+    n = b.nbasis
+    own = sess is None
+    if own:
+        sess = capi.Session(local)
+    lib = capi.lib()
+    lib.qb_set_stream(capi.C.c_void_p(stream.cuda_stream))
+    sess.upload_molecule(m, b)
+    sg = np.ascontiguousarray(sigrad2(b))
+    # a positive semi-definite closed-shell density 2 C C^T (rho >= 0 everywhere)
+    rng = np.random.default_rng(WORKLOAD["seed"])
+    C = rng.standard_normal((n, m.n_electrons // 2)) * 0.05
+    D = np.asfortranarray(2.0 * C @ C.T)
+    O0 = np.zeros((n, n), order="F")
+    sess.getxc(O0, D, sg, method=1)                  # builds the grid once
+    grid_ms = sess.xc_stats()["ms_grid"]
+    dD = torch.from_numpy(np.ascontiguousarray(D)).to(dev)
+    dV = torch.zeros((n, n), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    exc, nal = capi.C.c_double(0), capi.C.c_double(0)
+
+    def step():
+        dV.zero_()
+        rc = lib.qb_xc_device(capi.C.c_void_p(dD.data_ptr()), capi._ptr(sg), capi.C.c_void_p(dV.data_ptr()),
+                              capi.C.byref(exc), capi.C.byref(nal))
+        if rc:
+            capi.check()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    l0 = lib.qb_launch_count()
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        e0[i].record(stream)
+        step()
+        e1[i].record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    launches = lib.qb_launch_count() - l0
+    ms = max_over_ranks(float(np.mean([a.elapsed_time(c) for a, c in zip(e0, e1)])), ws)
+    st = sess.xc_stats()
+    # end to end: gpu_upload_method_ + gpu_upload_calculated_ + gpu_getxc_ from pinned host memory
+    pinD = torch.from_numpy(np.asfortranarray(D).ravel(order="F").copy()).pin_memory()
+    pinO = torch.zeros(n * n, dtype=torch.float64).pin_memory()
+    co = torch.zeros(1, dtype=torch.float64)
+    ptr = lambda t: capi.C.c_void_p(t.data_ptr())  # noqa: E731
+    one = capi.C.byref
+    ee = capi.C.c_double(0)
+    ec0, ec1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    ec0.record(stream)
+    for i in range(args.steps):
+        lib.gpu_upload_method_(one(capi.C.c_int(1)))
+        lib.gpu_upload_calculated_(ptr(pinO), ptr(co), ptr(co), ptr(pinD))
+        ee.value = 0.0
+        lib.gpu_getxc_(one(capi.C.c_int(1)), capi._ptr(sg), one(ee), one(capi.C.c_double(0)),
+                       one(capi.C.c_double(0)), ptr(pinO))
+    ec1.record(stream)
+    torch.cuda.synchronize()
+    capi.check()
+    e2e_ms = max_over_ranks(ec0.elapsed_time(ec1) / args.steps, ws)
+    hbm, hbm_src = measured_hbm_gbs()
+    peak64 = capi.C.c_double(0)
+    lib.qb_fma_peak(1, capi.C.byref(peak64))
+    gbs = st["alg_bytes"] / (ms * 1e-3) / 1e9
+    tfl = st["gemm_flops"] / (ms * 1e-3) / 1e12
+    if own:
+        sess.close()
+    return {
+        "metric": "XC quadrature grid points/s (SG1, B3LYP, FP64)",
+        "value": st["npts"] * ws / (ms * 1e-3), "unit": "points/s", "ms_per_call": ms,
+        "config": {"workload": "(H2O)32 6-31G** B3LYP XC quadrature, QUICK SG1 grid", "grid_points": st["npts"],
+                   "chunks": st["nchunks"], "grid_build_ms": grid_ms, "l2": "flushed (256 MB write) before every call"},
+        "e2e": {"value": st["npts"] * ws / (e2e_ms * 1e-3), "unit": "points/s", "ms_per_call": e2e_ms,
+                "h2d_bytes_per_step": int(2 * n * n * 8 + n * 8), "d2h_bytes_per_step": int(n * n * 8)},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                     "traffic": None, "peak_source": hbm_src,
+                     "bytes_per_call": st["alg_bytes"],
+                     "fp64_gemm_tflops": tfl, "fp64_peak_tflops": peak64.value / 1e3,
+                     "fp64_frac": tfl / (peak64.value / 1e3) if peak64.value else None},
+        "gpu_launches": int(launches),
+        "exc": exc.value,
+    }
 
 
 def main():
@@ -312,6 +458,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--classes", action="store_true", help="add per-class quartet counts")
+    ap.add_argument("--part", default="all", choices=["all", "fock", "xc"],
+                    help="fock: the Fock build line only; xc: the XC quadrature line only")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     threads = os.cpu_count() or 1
@@ -333,7 +481,17 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
+    if args.part == "xc":
+        out = run_xc(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps(out))
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     out = run_ours(args, ws, rank, local)
+    if args.part == "all":
+        out["xc"] = run_xc(args, ws, rank, local)
     if rank == 0 and not args.no_cpu_baseline:
         qps, nq, sec = cpu_reference(threads)
         out["cpu_baseline"] = {"value": qps, "unit": "quartets/s", "cores": threads, "kind": "reference",

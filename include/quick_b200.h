@@ -124,6 +124,16 @@ int qb_fock_device_static(const double* d_dense, const double* d_o_in, double* d
    kernels in ms, device time of the screening in ms. */
 int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen);
 
+/* Mixed precision for the following Fock builds (no counterpart in QUICK, which is FP64
+   throughout): shell quartets whose bound Y_ab Y_cd DNMax (QUICK's own screening product,
+   gpu_get2e_subs.h:323-328) is below cut run their Boys function, recurrences and contraction
+   in FP32; the others, and all accumulation into the Fock matrix, stay FP64.  cut = 0 (the
+   default) keeps every quartet in FP64.  Gradients always run in FP64. */
+int qb_set_mixed_precision(double cut);
+
+/* The last Fock build's shell quartets by precision. */
+int qb_last_fock_split(long long* quartets_fp64, long long* quartets_fp32);
+
 /* XC quadrature on device pointers (no counterpart in QUICK; gpu_getxc_ without the host
    round trip): adds V_xc to the lower triangle of d_vxc (column-major nbasis^2, V(j, i) for
    j >= i; not zeroed here) for the density d_dense, and returns the grid sums of the energy
@@ -134,6 +144,12 @@ int qb_xc_device(const double* d_dense, const double* sigrad2, double* d_vxc, do
    with at least one significant basis function, device time of the per-call phase in ms, and
    of the grid build in ms (0 when the grid was reused). */
 int qb_last_xc_stats(long long* npts, long long* nchunks, double* ms, double* ms_grid);
+
+/* Algorithmic work of the last XC quadrature, summed over its point chunks (P points, nb
+   significant functions each): bytes = P nb x 32 (phi and grad phi) + 2 nb^2 x 8 (density and
+   operator tiles), flops = 4 P nb^2 (density and operator contractions), gemm_flops = the
+   8 P nb^2 the three DGEMMs execute. */
+int qb_last_xc_work(double* bytes, double* flops, double* gemm_flops);
 
 /* The kept grid points (x, y, z, weight per point) of the last XC grid build; copies up to cap
    points and returns the number of points. */

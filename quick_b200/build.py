@@ -31,7 +31,7 @@ def _extra_flags(src):
     allocation that spills nearly everything; -O1 keeps 255 registers and
     spills about a quarter as much (measured with -Xptxas -v)."""
     b = os.path.basename(src)
-    for pre in ("eri_", "grad_"):
+    for pre in ("eri_", "eri32_", "grad_"):
         if b.startswith(pre) and b[len(pre):len(pre) + 4].isdigit():
             if sum(int(ch) for ch in b[len(pre):len(pre) + 4]) + (1 if pre == "grad_" else 0) >= 6:
                 return ["-Xptxas", "-O1"]
@@ -79,7 +79,7 @@ def build(lmax=2, jobs=None, verbose=False):
     keep = []
     for s in srcs:
         b = os.path.basename(s)
-        for pre in ("eri_", "grad_"):
+        for pre in ("eri_", "eri32_", "grad_"):
             if b.startswith(pre) and b[len(pre):len(pre) + 4].isdigit() and max(int(ch) for ch in b[len(pre):len(pre) + 4]) > lmax:
                 break
         else:

@@ -163,7 +163,10 @@ class Session:
     def xc_stats(self):
         n, c, a, b = C.c_longlong(0), C.c_longlong(0), C.c_double(0), C.c_double(0)
         lib().qb_last_xc_stats(C.byref(n), C.byref(c), C.byref(a), C.byref(b))
-        return dict(npts=n.value, nchunks=c.value, ms=a.value, ms_grid=b.value)
+        x, y, z = C.c_double(0), C.c_double(0), C.c_double(0)
+        lib().qb_last_xc_work(C.byref(x), C.byref(y), C.byref(z))
+        return dict(npts=n.value, nchunks=c.value, ms=a.value, ms_grid=b.value, alg_bytes=x.value,
+                    alg_flops=y.value, gemm_flops=z.value)
 
     def xc_grid(self):
         """(npts, 4) array of the kept grid points: x, y, z, weight."""
@@ -174,6 +177,16 @@ class Session:
         r.qb_xc_grid(_ptr(out), C.c_longlong(n))
         check()
         return out[:n]
+
+    def set_mixed_precision(self, cut):
+        """Quartets with Y_ab Y_cd DNMax below cut run in FP32 (0: all FP64)."""
+        lib().qb_set_mixed_precision(C.c_double(cut))
+        check()
+
+    def fock_split(self):
+        a, b = C.c_longlong(0), C.c_longlong(0)
+        lib().qb_last_fock_split(C.byref(a), C.byref(b))
+        return dict(fp64=a.value, fp32=b.value)
 
     def fock_stats(self):
         q, a, b = C.c_longlong(0), C.c_double(0), C.c_double(0)

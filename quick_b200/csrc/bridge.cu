@@ -85,11 +85,12 @@ struct Context {
     DevBuf<int4> d_pair_bf, d_pair_sh;
     DevBuf<double4> d_pair_AB;
     DevBuf<ScreenClass> d_screen_cls;
-    DevBuf<unsigned long long> d_counts;
-    DevBuf<int> d_class_count, d_overflow;
-    DevBuf<long long> d_class_offset;
+    DevBuf<unsigned long long> d_counts, d_counts32;
+    DevBuf<int> d_class_count, d_class_count32, d_overflow;
+    DevBuf<long long> d_class_offset, d_class_end;
     DevBuf<int2> d_quartets;
     std::vector<ScreenClass> screen_cls;
+    std::vector<int> class_group;        // lanes per shell quartet of each class kernel
     // per-iteration
     std::vector<double> o_host;          // O as uploaded (one-electron part)
     std::vector<double> dense_host;
@@ -100,7 +101,8 @@ struct Context {
     std::vector<double> grad_host;
     bool have_grad = false;
     // stats
-    long long last_quartets = 0;
+    long long last_quartets = 0, last_quartets32 = 0;
+    double mixed_cut = 0.0;      // Fock builds: quartets with Y Y DNMax below this run in FP32 (0: all FP64)
     XcResult last_xc;
     double last_ms_eri = 0, last_ms_screen = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -369,6 +371,28 @@ static int build_tables(Context& c)
         s.out_offset = 0;
         s.capacity = 0;
     }
+    // lanes per shell quartet: the class's mean primitive quartets before
+    // screening (mean primitive pairs of the bra type x of the ket type) over
+    // QB_FOCK_GDIV (default 2), rounded down to a power of two and clamped to
+    // what the class was compiled for; QB_FOCK_G forces one value
+    std::vector<double> type_prims(kNumPairTypes, 0.0);
+    for (int t = 0; t < kNumPairTypes; t++) {
+        double sum = 0.0;
+        for (int i = c.type_begin[t]; i < c.type_end[t]; i++) sum += pbf[i].w;
+        type_prims[t] = c.type_end[t] > c.type_begin[t] ? sum / (c.type_end[t] - c.type_begin[t]) : 0.0;
+    }
+    const char* gd = getenv("QB_FOCK_GDIV");
+    const char* gf = getenv("QB_FOCK_G");
+    const double div = gd && atof(gd) > 0 ? atof(gd) : 2.0;
+    c.class_group.assign(kNumClasses, 1);
+    for (int k = 0; k < kNumClasses; k++) {
+        double est = type_prims[pair_type_index(kClassL[k][0], kClassL[k][1])] *
+                     type_prims[pair_type_index(kClassL[k][2], kClassL[k][3])] / div;
+        int g = 1;
+        while (g * 2 <= est && g < 32) g *= 2;
+        if (gf && atoi(gf) > 0) g = atoi(gf);
+        c.class_group[k] = std::min(g, class_max_group(k));
+    }
     return 0;
 }
 
@@ -392,6 +416,9 @@ static FockParams fock_params(Context& c)
     P.prim_limit = c.primLimit;
     P.hybrid = c.method == 0 ? 1.0 : (c.method == 1 ? 0.2 : 0.0);
     P.integral_cutoff = c.integralCutoff;
+    P.mixed_cut = c.mixed_cut;
+    P.class_count32 = c.d_class_count32.p;
+    P.class_end = c.d_class_end.p;
     return P;
 }
 
@@ -402,29 +429,34 @@ static int size_quartet_lists(Context& c)
 {
     CK(c.d_screen_cls.alloc(kNumClasses));
     CK(c.d_counts.alloc(kNumClasses));
+    CK(c.d_counts32.alloc(kNumClasses));
     CK(c.d_class_count.alloc(kNumClasses));
+    CK(c.d_class_count32.alloc(kNumClasses));
     CK(c.d_class_offset.alloc(kNumClasses));
+    CK(c.d_class_end.alloc(kNumClasses));
     CK(c.d_overflow.alloc(1));
     CK(cudaMemcpy(c.d_screen_cls.p, c.screen_cls.data(), kNumClasses * sizeof(ScreenClass), cudaMemcpyHostToDevice));
     CK(cudaMemsetAsync(c.d_counts.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
     FockParams P = fock_params(c);
-    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, nullptr};
+    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, nullptr, c.d_counts32.p};
     launch_screen(S, P, kNumClasses, 1, c.nsm, c.stream);
     CK(cudaGetLastError());
     std::vector<unsigned long long> cnt(kNumClasses);
     CK(cudaMemcpyAsync(cnt.data(), c.d_counts.p, kNumClasses * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     long long off = 0;
-    std::vector<long long> offs(kNumClasses);
+    std::vector<long long> offs(kNumClasses), ends(kNumClasses);
     for (int k = 0; k < kNumClasses; k++) {
         c.screen_cls[k].out_offset = off;
         c.screen_cls[k].capacity = (long long)cnt[k];
         offs[k] = off;
         off += (long long)cnt[k];
+        ends[k] = off;
     }
     CK(c.d_quartets.alloc((size_t)std::max<long long>(off, 1)));
     CK(cudaMemcpy(c.d_screen_cls.p, c.screen_cls.data(), kNumClasses * sizeof(ScreenClass), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.d_class_offset.p, offs.data(), kNumClasses * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.d_class_end.p, ends.data(), kNumClasses * sizeof(long long), cudaMemcpyHostToDevice));
     g_sized_cutoff = c.integralCutoff;
     return 0;
 }
@@ -439,13 +471,15 @@ static int screen_quartets(Context& c, std::vector<int>& cnt)
         if (size_quartet_lists(c)) return 2;
     int n = c.nbasis;
     CK(cudaMemsetAsync(c.d_counts.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
+    CK(cudaMemsetAsync(c.d_counts32.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
     CK(cudaMemsetAsync(c.d_overflow.p, 0, sizeof(int), c.stream));
     CK(c.d_dense.alloc((size_t)n * n));
     launch_scale_density(c.d_dense_raw.p, c.d_cons.p, c.d_dense.p, n, c.stream);
     FockParams P = fock_params(c);
-    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p};
+    P.mixed_cut = 0.0;   // the gradient kernels run every quartet in FP64
+    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p, c.d_counts32.p};
     launch_screen(S, P, kNumClasses, 0, c.nsm, c.stream);
-    launch_finish_counts(S, c.d_class_count.p, c.d_overflow.p, kNumClasses, c.stream);
+    launch_finish_counts(S, c.d_class_count.p, c.d_class_count32.p, c.d_overflow.p, kNumClasses, c.stream);
     CK(cudaGetLastError());
     cnt.assign(kNumClasses, 0);
     int ovf = 0;
@@ -489,33 +523,39 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
     CK(c.d_fock.alloc((size_t)n * n));
     CK(cudaMemsetAsync(c.d_fock.p, 0, (size_t)n * n * sizeof(double), c.stream));
     CK(cudaMemsetAsync(c.d_counts.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
+    CK(cudaMemsetAsync(c.d_counts32.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
     CK(cudaMemsetAsync(c.d_overflow.p, 0, sizeof(int), c.stream));
     CK(c.d_dense.alloc((size_t)n * n));
     launch_scale_density(c.d_dense_raw.p, c.d_cons.p, c.d_dense.p, n, c.stream);
     FockParams P = fock_params(c);
-    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p};
+    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p, c.d_counts32.p};
     for (int k = 0; k < 4; k++)
         if (!c.ev[k]) CK(cudaEventCreate(&c.ev[k]));
     CK(cudaEventRecord(c.ev[0], c.stream));
     launch_screen(S, P, kNumClasses, 0, c.nsm, c.stream);
-    launch_finish_counts(S, c.d_class_count.p, c.d_overflow.p, kNumClasses, c.stream);
+    launch_finish_counts(S, c.d_class_count.p, c.d_class_count32.p, c.d_overflow.p, kNumClasses, c.stream);
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[1], c.stream));
-    std::vector<int> cnt(kNumClasses);
+    std::vector<int> cnt(kNumClasses), cnt32(kNumClasses);
     int ovf = 0;
     CK(cudaMemcpyAsync(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(cnt32.data(), c.d_class_count32.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaMemcpyAsync(&ovf, c.d_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     if (ovf) return set_error(3, "quartet list overflow (internal sizing error)"), 3;
-    long long total = 0;
+    long long total = 0, total32 = 0;
     CK(cudaEventRecord(c.ev[2], c.stream));
     for (int k = 0; k < kNumClasses; k++) {
-        if (cnt[k] == 0) continue;
-        total += cnt[k];
-        int block = 128;
-        long long warps = (cnt[k] + 31) / 32;
-        long long grid = std::min<long long>((warps * 32 + block - 1) / block, (long long)c.nsm * 16);
-        launch_class(k, P, (int)std::max<long long>(grid, 1), block, c.stream);
+        for (int f32 = 0; f32 < 2; f32++) {
+            const int nq = f32 ? cnt32[k] : cnt[k];
+            if (nq == 0) continue;
+            (f32 ? total32 : total) += nq;
+            const int G = c.class_group.empty() ? 1 : c.class_group[k];
+            if (f32)
+                launch_class32(k, P, G, nq, c.nsm, c.stream);
+            else
+                launch_class(k, P, G, nq, c.nsm, c.stream);
+        }
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[3], c.stream));
@@ -527,7 +567,8 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
     CK(cudaEventElapsedTime(&ms1, c.ev[2], c.ev[3]));
     c.last_ms_screen = ms0;
     c.last_ms_eri = ms1;
-    c.last_quartets = total;
+    c.last_quartets = total + total32;
+    c.last_quartets32 = total32;
     return 0;
 }
 
@@ -617,9 +658,12 @@ void gpu_shutdown_(void)
     c.d_pair_AB.release();
     c.d_screen_cls.release();
     c.d_counts.release();
+    c.d_counts32.release();
     c.d_class_count.release();
+    c.d_class_count32.release();
     c.d_overflow.release();
     c.d_class_offset.release();
+    c.d_class_end.release();
     c.d_quartets.release();
     for (auto& e : c.ev)
         if (e) cudaEventDestroy(e), e = nullptr;
@@ -868,6 +912,15 @@ int qb_last_xc_stats(long long* npts, long long* nchunks, double* ms, double* ms
     return 0;
 }
 
+int qb_last_xc_work(double* bytes, double* flops, double* gemm_flops)
+{
+    Context& c = ctx();
+    *bytes = c.last_xc.alg_bytes;
+    *flops = c.last_xc.alg_flops;
+    *gemm_flops = c.last_xc.gemm_flops;
+    return 0;
+}
+
 long long qb_xc_grid(double* xyzw, long long cap) { return xc_grid_points(xyzw, cap); }
 
 int qb_xc_functional(int method, int n, const double* rho, const double* sigma, double* out)
@@ -890,6 +943,21 @@ int qb_xc_functional(int method, int n, const double* rho, const double* sigma, 
     s.release();
     o.release();
     return rc;
+}
+
+int qb_set_mixed_precision(double cut)
+{
+    if (!(cut >= 0.0)) return set_error(1, "qb_set_mixed_precision: cut must be >= 0"), 1;
+    ctx().mixed_cut = cut;
+    return 0;
+}
+
+int qb_last_fock_split(long long* quartets_fp64, long long* quartets_fp32)
+{
+    Context& c = ctx();
+    *quartets_fp32 = c.last_quartets32;
+    *quartets_fp64 = c.last_quartets - c.last_quartets32;
+    return 0;
 }
 
 int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen)
@@ -1193,6 +1261,7 @@ int session_view(SessionView* v)
     P.fock = nullptr;
     v->P = P;
     v->cls = c.screen_cls;
+    v->group = c.class_group;
     v->cons = c.d_cons.p;
     v->nsm = c.nsm;
     v->stream = c.stream;

@@ -83,6 +83,7 @@ class VRR:
         self.memo = {}
         self.lines = []
         self.prec = prec
+        self.sfx = "f" if prec == "float" else ""
         self.nflops = 0
 
     def get(self, e, f, m):
@@ -107,11 +108,11 @@ class VRR:
                 f2 = sub(f, i, 2)
                 c = self.get(e, f2, m)
                 d = self.get(e, f2, m + 1)
-                terms.append("%d.0*o2q*(%s - rq*%s)" % (f1[i], c, d) if f1[i] > 1 else "o2q*(%s - rq*%s)" % (c, d))
+                terms.append("%d.0%s*o2q*(%s - rq*%s)" % (f1[i], self.sfx, c, d) if f1[i] > 1 else "o2q*(%s - rq*%s)" % (c, d))
                 self.nflops += 4
             if e[i] > 0:
                 g = self.get(sub(e, i), f1, m + 1)
-                terms.append("%s*%s" % ("%d.0*o2pq" % e[i] if e[i] > 1 else "o2pq", g))
+                terms.append("%s*%s" % ("%d.0%s*o2pq" % (e[i], self.sfx) if e[i] > 1 else "o2pq", g))
                 self.nflops += 2
             self.nflops += 4
         else:
@@ -125,7 +126,7 @@ class VRR:
                 e2 = sub(e, i, 2)
                 c = self.get(e2, f, m)
                 d = self.get(e2, f, m + 1)
-                terms.append("%d.0*o2p*(%s - rp*%s)" % (e1[i], c, d) if e1[i] > 1 else "o2p*(%s - rp*%s)" % (c, d))
+                terms.append("%d.0%s*o2p*(%s - rp*%s)" % (e1[i], self.sfx, c, d) if e1[i] > 1 else "o2p*(%s - rp*%s)" % (c, d))
                 self.nflops += 4
             self.nflops += 4
         name = "v%s_%s_%d" % (nm(e), nm(f), m)
@@ -137,10 +138,11 @@ class VRR:
 class HRR:
     """(ab|cd) from contracted (e0|f0) accumulators c_<e>_<f>."""
 
-    def __init__(self):
+    def __init__(self, prec="double"):
         self.memo = {}
         self.lines = []
         self.nflops = 0
+        self.prec = prec
 
     def get(self, a, b, c, d):
         key = (a, b, c, d)
@@ -162,22 +164,41 @@ class HRR:
             return name
         self.nflops += 2
         name = "h%s_%s_%s_%s" % (nm(a), nm(b), nm(c), nm(d))
-        self.lines.append("const double %s = %s;" % (name, expr))
+        self.lines.append("const %s %s = %s;" % (self.prec, name, expr))
         self.memo[key] = name
         return name
 
 
-def gen_class(la, lb, lc, ld):
+def group_sizes(la, lb, lc, ld):
+    """Lanes per shell quartet compiled for a class: the light classes, whose
+    cost is the primitive loop, get sub-warp groups up to a whole warp; the
+    heavy ones, whose cost is the recurrences, one lane per quartet."""
     L = la + lb + lc + ld
+    if L <= 2:
+        return [1, 2, 4, 8, 16, 32]
+    if L <= 4:
+        return [1, 2, 4, 8]
+    return [1]
+
+
+def gen_class(la, lb, lc, ld, prec="double"):
+    """One angular class of the Fock build.  prec = "float": the FP32 variant
+    of the mixed-precision split (vertical and horizontal recurrences,
+    contraction and Boys function in FP32 from FP64 pair data and geometry;
+    the digestion into the Fock matrix stays FP64)."""
+    L = la + lb + lc + ld
+    f32 = prec == "float"
+    R = prec
+    sfx = "f" if f32 else ""
     tag = "%d%d%d%d" % (la, lb, lc, ld)
     ebra = [e for n in range(la, la + lb + 1) for e in carts(n)]
     fket = [f for n in range(lc, lc + ld + 1) for f in carts(n)]
-    vrr = VRR()
+    vrr = VRR(prec)
     targets = []
     for e in ebra:
         for f in fket:
             targets.append((e, f, vrr.get(e, f, 0)))
-    hrr = HRR()
+    hrr = HRR(prec)
     A, B, Cc, D = QUICK_ORDER[la], QUICK_ORDER[lb], QUICK_ORDER[lc], QUICK_ORDER[ld]
     vals = {}
     for ia, a in enumerate(A):
@@ -191,36 +212,71 @@ def gen_class(la, lb, lc, ld):
     w("// generated by gen_eri.py: class (%s %s | %s %s)" % tuple("spdf"[x] for x in (la, lb, lc, ld)))
     w('#include "eri_common.cuh"')
     w("namespace qb {")
-    w("template <> __device__ __forceinline__ void quartet_class<%d, %d, %d, %d>(const QuartetCtx& q, const FockParams& P)" % (la, lb, lc, ld))
+    ev = "ClassEval32" if f32 else "ClassEval"
+    w("template <> struct %s<%d, %d, %d, %d> {" % (ev, la, lb, lc, ld))
+    w("template <int G>")
+    w("__device__ __forceinline__ static void run(const QuartetCtx& q, const FockParams& P, int sub)")
     w("{")
     w("    constexpr int L = %d;" % L)
     for e, f, _ in targets:
-        w("    double c_%s_%s = 0.0;" % (nm(e), nm(f)))
+        w("    %s c_%s_%s = 0.0%s;" % (R, nm(e), nm(f), sfx))
+    body = []
+    b = body.append
+    b("const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
+    b("if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
+    b("const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
+    if f32:
+        b("PrimQuartet32 s;")
+        b("float Fm[L + 1];")
+        b("prim_quartet32<L>(pb, pk, P, s, Fm);")
+        b("const float PAx = (float)pb.PAx, PAy = (float)pb.PAy, PAz = (float)pb.PAz;")
+        b("const float QCx = (float)pk.PAx, QCy = (float)pk.PAy, QCz = (float)pk.PAz;")
+    else:
+        b("PrimQuartet s;")
+        b("double Fm[L + 1];")
+        b("prim_quartet<L>(pb, pk, P, s, Fm);")
+        b("const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
+        b("const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
+    b("const %s WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;" % R)
+    b("const %s o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;" % R)
+    b("(void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;")
+    b("(void)WQx; (void)WQy; (void)WQz; (void)o2p; (void)o2q; (void)o2pq; (void)rp; (void)rq;")
+    for m in range(L + 1):
+        b("const %s F%d = Fm[%d];" % (R, m, m))
+    body += vrr.lines
+    for e, f, v in targets:
+        b("c_%s_%s += %s;" % (nm(e), nm(f), v))
+    # G == 1: one lane walks the bra x ket primitive double loop
+    w("    if constexpr (G == 1) {")
     w("    for (int ib = 0; ib < q.nbra; ib++) {")
     w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
     w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
     w("        for (int ik = 0; ik < q.nket; ik++) {")
-    w("            const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
-    w("            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
-    w("            const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
-    w("            PrimQuartet s;")
-    w("            double Fm[L + 1];")
-    w("            prim_quartet<L>(pb, pk, P, s, Fm);")
-    w("            const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
-    w("            const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
-    w("            const double WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;")
-    w("            const double o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;")
-    w("            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;")
-    w("            (void)WQx; (void)WQy; (void)WQz; (void)o2p; (void)o2q; (void)o2pq; (void)rp; (void)rq;")
-    for m in range(L + 1):
-        w("            const double F%d = Fm[%d];" % (m, m))
-    for ln in vrr.lines:
+    for ln in body:
         w("            " + ln)
-    for e, f, v in targets:
-        w("            c_%s_%s += %s;" % (nm(e), nm(f), v))
     w("        }")
     w("    }")
-    w("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
+    # G > 1: the G lanes of a group stride over the flattened primitive quartets
+    w("    } else {")
+    w("    const int nk = q.nket, npq = q.nbra * nk;")
+    w("    for (int t = sub; t < npq; t += G) {")
+    w("        const int ib = t / nk, ik = t - ib * nk;")
+    w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
+    w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
+    w("        {")
+    for ln in body:
+        w("            " + ln.replace("continue;", "continue;"))
+    w("        }")
+    w("    }")
+    for e, f, _ in targets:
+        w("    c_%s_%s = group_sum<G>(c_%s_%s);" % (nm(e), nm(f), nm(e), nm(f)))
+    w("    }")
+    w("    QuartetCtx qa = q;")
+    w("    qa.active = q.active && sub == 0;   // the group's first lane digests")
+    if f32:
+        w("    const float ABx = (float)q.ABx, ABy = (float)q.ABy, ABz = (float)q.ABz, CDx = (float)q.CDx, CDy = (float)q.CDy, CDz = (float)q.CDz;")
+    else:
+        w("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
     w("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
     for ln in hrr.lines:
         w("    " + ln)
@@ -267,7 +323,7 @@ def gen_class(la, lb, lc, ld):
         x, y = out_blk
         for i in range(n1):
             for j in range(n2):
-                w("        digest_exchange(P, q, %s+%d, %s+%d, K%s_%d_%d);" % (bases[x], i, bases[y], j, out_blk, i, j))
+                w("        digest_exchange(P, qa, %s+%d, %s+%d, K%s_%d_%d);" % (bases[x], i, bases[y], j, out_blk, i, j))
     w("    }")
     # Coulomb
     for ia in range(na):
@@ -278,18 +334,27 @@ def gen_class(la, lb, lc, ld):
         for id_ in range(nd):
             terms = ["Dab_%d_%d*%s" % (ia, ib, vals[(ia, ib, ic, id_)]) for ia in range(na) for ib in range(nb)]
             w("    const double Jcd_%d_%d = %s;" % (ic, id_, " + ".join(terms)))
-    w("    const bool bra_uniform = warp_bra_uniform(q);")
+    w("    const bool bra_uniform = warp_bra_uniform(qa);")
     for ia in range(na):
         for ib in range(nb):
-            w("    digest_coulomb_bra(P, q, a0+%d, b0+%d, Jab_%d_%d, bra_uniform);" % (ia, ib, ia, ib))
+            w("    digest_coulomb_bra(P, qa, a0+%d, b0+%d, Jab_%d_%d, bra_uniform);" % (ia, ib, ia, ib))
     for ic in range(nc):
         for id_ in range(nd):
-            w("    digest_coulomb(P, q, c0+%d, d0+%d, Jcd_%d_%d);" % (ic, id_, ic, id_))
+            w("    digest_coulomb(P, qa, c0+%d, d0+%d, Jcd_%d_%d);" % (ic, id_, ic, id_))
     w("}")
-    w("void launch_%s(const FockParams& P, int cls, int grid, int block, cudaStream_t st)" % tag)
+    w("};")
+    gs = group_sizes(la, lb, lc, ld)
+    kname = "fock_class_kernel32" if f32 else "fock_class_kernel"
+    w("// lanes per shell quartet compiled for this class: %s" % ", ".join(str(g) for g in gs))
+    w("int launch_%s%s(const FockParams& P, int cls, int G, int nq, int nsm, cudaStream_t st)" % (tag, "_f32" if f32 else ""))
     w("{")
-    w("    auto kern = fock_class_kernel<%d, %d, %d, %d>;" % (la, lb, lc, ld))
-    w("    QB_LAUNCH(kern, grid, block, 0, st, P, cls);")
+    w("    switch (G) {")
+    for g in gs:
+        w("    case %d: { auto kern = %s<%d, %d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, %d, nsm), 128, 0, st, P, cls); return %d; }"
+          % (g, kname, la, lb, lc, ld, g, g, g))
+    w("    default: { auto kern = %s<%d, %d, %d, %d, 1>; QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, 0, st, P, cls); return 1; }"
+      % (kname, la, lb, lc, ld))
+    w("    }")
     w("}")
     w("}  // namespace qb")
     stats = dict(vrr_flops=vrr.nflops, vrr_nodes=len(vrr.lines), hrr_flops=hrr.nflops, targets=len(targets),
@@ -562,20 +627,28 @@ def main(outdir, lmax=2):
     for c in cls:
         src, st = gen_class(*c)
         stats[c] = st
-        path = os.path.join(outdir, "eri_%d%d%d%d.cu" % c)
-        old = open(path).read() if os.path.exists(path) else None
-        if old != src:
-            with open(path, "w") as fh:
-                fh.write(src)
+        write_if_changed(os.path.join(outdir, "eri_%d%d%d%d.cu" % c), src)
+        src32, _ = gen_class(*c, prec="float")
+        write_if_changed(os.path.join(outdir, "eri32_%d%d%d%d.cu" % c), src32)
     # launch table
     lt = ['#include "eri_common.cuh"', '#include "eri_classes.h"', "namespace qb {"]
     for c in cls:
-        lt.append("void launch_%d%d%d%d(const FockParams& P, int cls, int grid, int block, cudaStream_t st);" % c)
-    lt += ["void launch_class(int cls, const FockParams& P, int grid, int block, cudaStream_t st)", "{",
+        lt.append("int launch_%d%d%d%d(const FockParams& P, int cls, int G, int nq, int nsm, cudaStream_t st);" % c)
+        lt.append("int launch_%d%d%d%d_f32(const FockParams& P, int cls, int G, int nq, int nsm, cudaStream_t st);" % c)
+    lt += ["int launch_class(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st)", "{",
            "    switch (cls) {"]
     for k, c in enumerate(cls):
-        lt.append("    case %d: launch_%d%d%d%d(P, %d, grid, block, st); break;" % ((k,) + c + (k,)))
-    lt += ["    default: break;", "    }", "}", "}  // namespace qb"]
+        lt.append("    case %d: return launch_%d%d%d%d(P, %d, G, nq, nsm, st);" % ((k,) + c + (k,)))
+    lt += ["    default: return 0;", "    }", "}"]
+    lt += ["int launch_class32(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st)", "{",
+           "    switch (cls) {"]
+    for k, c in enumerate(cls):
+        lt.append("    case %d: return launch_%d%d%d%d_f32(P, %d, G, nq, nsm, st);" % ((k,) + c + (k,)))
+    lt += ["    default: return 0;", "    }", "}"]
+    lt += ["int class_max_group(int cls)", "{", "    switch (cls) {"]
+    for k, c in enumerate(cls):
+        lt.append("    case %d: return %d;" % (k, max(group_sizes(*c))))
+    lt += ["    default: return 1;", "    }", "}", "}  // namespace qb"]
     write_if_changed(os.path.join(outdir, "eri_launch.cu"), "\n".join(lt) + "\n")
     import json
     write_if_changed(os.path.join(outdir, "class_flops.json"),

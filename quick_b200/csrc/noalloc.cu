@@ -77,7 +77,9 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
     size_t off = 0;
     auto take = [&](size_t bytes) { unsigned char* p = base + off; off += round256(bytes); return p; };
     auto* counts = (unsigned long long*)take(ncls * sizeof(unsigned long long));
+    auto* counts32 = (unsigned long long*)take(ncls * sizeof(unsigned long long));
     auto* class_count = (int*)take(ncls * sizeof(int));
+    auto* class_count32 = (int*)take(ncls * sizeof(int));
     auto* class_offset = (long long*)take(ncls * sizeof(long long));
     auto* overflow = (int*)take(sizeof(int));
     auto* d_cls = (ScreenClass*)take(ncls * sizeof(ScreenClass));
@@ -95,8 +97,10 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
     for (auto& c : cls) c.out_offset = 0, c.capacity = 0;
     CKS(cudaMemcpyAsync(d_cls, cls.data(), ncls * sizeof(ScreenClass), cudaMemcpyHostToDevice, st));
     CKS(cudaMemsetAsync(counts, 0, ncls * sizeof(unsigned long long), st));
+    CKS(cudaMemsetAsync(counts32, 0, ncls * sizeof(unsigned long long), st));
     FockParams P = v.P;
-    ScreenParams S{d_cls, counts, quartets};
+    P.mixed_cut = 0.0;   // every quartet in FP64 here
+    ScreenParams S{d_cls, counts, quartets, counts32};
     launch_screen(S, P, ncls, 1, v.nsm, st);
     CKS(cudaGetLastError());
     std::vector<unsigned long long> cnt(ncls);
@@ -116,6 +120,7 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
     CKS(cudaMemcpyAsync(d_cls, cls.data(), ncls * sizeof(ScreenClass), cudaMemcpyHostToDevice, st));
     CKS(cudaMemcpyAsync(class_offset, offs.data(), ncls * sizeof(long long), cudaMemcpyHostToDevice, st));
     CKS(cudaMemsetAsync(counts, 0, ncls * sizeof(unsigned long long), st));
+    CKS(cudaMemsetAsync(counts32, 0, ncls * sizeof(unsigned long long), st));
     CKS(cudaMemsetAsync(overflow, 0, sizeof(int), st));
     CKS(cudaMemsetAsync(fock, 0, (size_t)n * n * sizeof(double), st));
 
@@ -124,10 +129,12 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
     P.quartets = quartets;
     P.class_offset = class_offset;
     P.class_count = class_count;
+    P.class_count32 = class_count32;
+    P.class_end = nullptr;   // read only by the FP32 class kernels, which are not launched here
     P.dense = dense;
     P.fock = fock;
     launch_screen(S, P, ncls, 0, v.nsm, st);
-    launch_finish_counts(S, class_count, overflow, ncls, st);
+    launch_finish_counts(S, class_count, class_count32, overflow, ncls, st);
     CKS(cudaGetLastError());
     std::vector<int> ccount(ncls);
     int ovf = 0;
@@ -137,10 +144,7 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
     if (ovf) return fail(3, "qb_fock_device_static: quartet list overflow (internal sizing error)");
     for (int k = 0; k < ncls; k++) {
         if (ccount[k] == 0) continue;
-        const int block = 128;
-        long long warps = (ccount[k] + 31) / 32;
-        long long grid = std::min<long long>((warps * 32 + block - 1) / block, (long long)v.nsm * 16);
-        launch_class(k, P, (int)std::max<long long>(grid, 1), block, st);
+        launch_class(k, P, v.group.empty() ? 1 : v.group[k], ccount[k], v.nsm, st);
     }
     CKS(cudaGetLastError());
     launch_fock_finish(fock, v.cons, d_o_in, d_o_out, n, st);

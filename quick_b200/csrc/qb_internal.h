@@ -17,13 +17,15 @@ struct ScreenClass {
 
 struct ScreenParams {
     const ScreenClass* cls;
-    unsigned long long* counts;
+    unsigned long long* counts;     // FP64 quartets per class (from the front of the region)
     int2* out;
+    unsigned long long* counts32;   // FP32 quartets per class (from the back), mixed precision only
 };
 
 struct SessionView {
     FockParams P;                       // session tables; working-memory pointers null
     std::vector<ScreenClass> cls;       // class ranges of the pair table
+    std::vector<int> group;             // lanes per shell quartet of each class kernel
     const double* cons;
     int nsm;
     cudaStream_t stream;
@@ -32,10 +34,15 @@ int session_view(SessionView* v);
 int report_error(int code, const char* msg);
 
 void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int count_only, int nsm, cudaStream_t st);
-void launch_finish_counts(const ScreenParams& S, int* class_count, int* overflow, int ncls, cudaStream_t st);
+void launch_finish_counts(const ScreenParams& S, int* class_count, int* class_count32, int* overflow, int ncls,
+                          cudaStream_t st);
 void launch_scale_density(const double* D, const double* cons, double* Ds, int n, cudaStream_t st);
 void launch_fock_finish(const double* G, const double* cons, const double* Oin, double* Oout, int n, cudaStream_t st);
-void launch_class(int cls, const FockParams& P, int grid, int block, cudaStream_t st);
+// Class kernels with G lanes per shell quartet (G not compiled for the
+// class: 1); return the G launched.
+int launch_class(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st);
+int launch_class32(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st);
+int class_max_group(int cls);
 void launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st);
 int fma_probe(int fp64, int nsm, double* gflops, cudaStream_t st);
 void launch_count_prims(const FockParams& P, int ncls, unsigned long long* out, int nsm, cudaStream_t st);

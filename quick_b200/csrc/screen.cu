@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const
         for (int k0 = kb; k0 < c.ket_end; k0 += 32) {
             if (!(P.pair_Y[k0] * Ya > cut)) break;      // sorted: the rest fail too
             const int b = k0 + lane;
-            bool pass = false;
+            bool pass = false, low = false;
             if (b < c.ket_end) {
                 const double yy = P.pair_Y[b] * Ya;
                 if (yy > cut) {
@@ -34,36 +34,53 @@ __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const
                         pass = true;
                     } else {
                         const int4 sb = P.pair_sh[b];
-                        const double dn = dn_max(P, sa.x, sa.y, sb.x, sb.y);
-                        pass = yy * dn > cut;
+                        const double bound = yy * dn_max(P, sa.x, sa.y, sb.x, sb.y);
+                        pass = bound > cut;
+                        low = pass && bound < P.mixed_cut;
                     }
                 }
             }
-            const unsigned m = __ballot_sync(FULL, pass);
-            if (m == 0) continue;
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(S.counts + cls, (unsigned long long)__popc(m));
+            const unsigned m = __ballot_sync(FULL, pass && !low);
+            const unsigned m32 = __ballot_sync(FULL, low);
+            if ((m | m32) == 0) continue;
+            unsigned long long base = 0, base32 = 0;
+            if (lane == 0) {
+                if (m) base = atomicAdd(S.counts + cls, (unsigned long long)__popc(m));
+                if (m32) base32 = atomicAdd(S.counts32 + cls, (unsigned long long)__popc(m32));
+            }
             base = __shfl_sync(FULL, base, 0);
+            base32 = __shfl_sync(FULL, base32, 0);
             if (!count_only && pass) {
-                const unsigned long long pos = base + __popc(m & ((1u << lane) - 1u));
-                if (pos < (unsigned long long)c.capacity)
-                    S.out[c.out_offset + pos] = make_int2(a, b);
+                const unsigned below = (1u << lane) - 1u;
+                if (!low) {
+                    const unsigned long long pos = base + __popc(m & below);
+                    if (pos < (unsigned long long)c.capacity) S.out[c.out_offset + pos] = make_int2(a, b);
+                } else {
+                    const unsigned long long pos = base32 + __popc(m32 & below);
+                    if (pos < (unsigned long long)c.capacity)
+                        S.out[c.out_offset + c.capacity - 1 - pos] = make_int2(a, b);
+                }
             }
         }
     }
 }
 
-// Clamp counters to capacities and publish them as int for the class kernels.
-__global__ void finish_counts_kernel(const ScreenParams S, int* class_count, int* overflow, int ncls)
+// Clamp counters to capacities and publish them as int for the class
+// kernels; the FP64 (front) and FP32 (back) lists share a class's region.
+__global__ void finish_counts_kernel(const ScreenParams S, int* class_count, int* class_count32, int* overflow,
+                                     int ncls)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < ncls) {
-        unsigned long long n = S.counts[c];
-        if (n > (unsigned long long)S.cls[c].capacity) {
+        unsigned long long n = S.counts[c], n32 = S.counts32[c];
+        const unsigned long long cap = (unsigned long long)S.cls[c].capacity;
+        if (n + n32 > cap) {
             atomicExch(overflow, 1);
-            n = S.cls[c].capacity;
+            n = n > cap ? cap : n;
+            n32 = n32 > cap - n ? cap - n : n32;
         }
         class_count[c] = (int)n;
+        class_count32[c] = (int)n32;
     }
 }
 
@@ -99,9 +116,10 @@ void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int cou
     QB_LAUNCH(screen_kernel, grid, 256, 0, st, S, P, count_only);
 }
 
-void launch_finish_counts(const ScreenParams& S, int* class_count, int* overflow, int ncls, cudaStream_t st)
+void launch_finish_counts(const ScreenParams& S, int* class_count, int* class_count32, int* overflow, int ncls,
+                          cudaStream_t st)
 {
-    QB_LAUNCH(finish_counts_kernel, (ncls + 63) / 64, 64, 0, st, S, class_count, overflow, ncls);
+    QB_LAUNCH(finish_counts_kernel, (ncls + 63) / 64, 64, 0, st, S, class_count, class_count32, overflow, ncls);
 }
 
 void launch_scale_density(const double* D, const double* cons, double* Ds, int n, cudaStream_t st)

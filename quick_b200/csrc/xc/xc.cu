@@ -13,13 +13,14 @@
 //     is not above the density cutoff are dropped, the rest are sorted into
 //     spatial chunks, and each chunk gets the ascending list of basis
 //     functions whose radius of significance reaches its bounding box.
-//  2. Per call and chunk (P points, nb functions):
-//       basis kernel  -> Phi, dPhi/dx, dPhi/dy, dPhi/dz   (P x nb each)
-//       DGEMM          T = [Phi; dPhi] * U^T, U the upper triangle of D
+//  2. Per call and chunk (P points, nb functions, function index fastest):
+//       basis kernel  -> phi, dphi/dx, dphi/dy, dphi/dz and psi (phi on the
+//                        rows denspt keeps), nb x P each
+//       DGEMMs         T0 = U phi, S = U^T psi, U the upper triangle of D
 //                      with the diagonal halved (denspt's pair order)
-//       point kernel   rho_alpha, grad rho_alpha, the functional, and the
-//                      operator factors chi = w (f_rho/2 phi + f_sig4 g.grad phi)
-//       DGEMM          M = [Phi'; chi']^T [chi; Phi]
+//       point kernel   one warp per point: rho_alpha, grad rho_alpha, the
+//                      functional, and chi = w (f_rho/2 phi + f_sig4 g.grad phi)
+//       DGEMM          M = [phi' | chi'] [chi | phi]^T (operator row screen ')
 //       scatter        V(j, i) += M(i, j) for i <= j
 //  3. Deterministic reductions of the per-point energy and electron count.
 //
@@ -36,6 +37,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -48,9 +50,22 @@
 namespace qb {
 
 constexpr double kXcCut = 1.0e-9;
-constexpr int kXcChunkPoints = 2048;
-constexpr double kXcCell = 4.0;          // bohr, edge of the sorting cells
-constexpr double kXcChunkSpan = 9.0;     // bohr, max bounding-box diagonal of a merged chunk
+// Chunking of the grid (defaults; QB_XC_POINTS, QB_XC_CELL and QB_XC_SPAN
+// override them at the next grid build): at most this many points per chunk,
+// sorting cells of this edge (bohr), and neighbouring cells merged while the
+// chunk's bounding-box diagonal stays below the span (bohr).
+constexpr int kXcChunkPointsDefault = 8192;
+constexpr double kXcCellDefault = 8.0;
+constexpr double kXcChunkSpanDefault = 16.0;
+
+static double env_or(const char* name, double dflt)
+{
+    const char* v = getenv(name);
+    if (!v || !*v) return dflt;
+    char* end = nullptr;
+    double x = strtod(v, &end);
+    return (end && end != v && x > 0) ? x : dflt;
+}
 
 struct XcShell {
     int atom, rad, leb;   // leb: index into kXcLebOrders
@@ -149,6 +164,12 @@ __global__ void xc_grid_kernel(XcGridParams p)
 }
 
 // ---------------------------------------------------------------- per call
+// Per chunk of P points and nb functions, every matrix is column-major with
+// the function index fastest (leading dimension nb), so a point's values are
+// contiguous.  The chunk buffer B holds five nb x P blocks:
+//     [chi | phi | dphi/dx | dphi/dy | dphi/dz],
+// and Psi (phi with denspt's row screen applied) is a separate nb x P block.
+
 // Cartesian factor x^n with its neighbours x^(n-1) and x^(n+1), as pteval
 // uses them (n = 0: 0, 1, x).
 __device__ __forceinline__ void cart_pows(double x, int n, double& xm, double& xi, double& xp)
@@ -165,15 +186,22 @@ __device__ __forceinline__ void cart_pows(double x, int n, double& xm, double& x
     xp = xi * x;
 }
 
-// Phi and its gradient for P points x nb basis functions of one chunk
-// (pteval, gpu_getxc.cu:456-534).  Column a of B5 (leading dimension 5P)
-// holds rows [P, 2P) phi, [2P, 3P) dphi/dx, [3P, 4P) dphi/dy, [4P, 5P) dphi/dz.
+// denspt's row screen (gpu_getxc.cu:551-556)
+__device__ __forceinline__ bool dens_row(double dii, double phi, double dx, double dy, double dz)
+{
+    return fabs(dii) >= kXcCut && fabs(phi + dx + dy + dz) >= kXcCut;
+}
+
+// phi and its gradient (pteval, gpu_getxc.cu:456-534) for one chunk, one
+// thread per (function, point), functions fastest; also Psi = phi on the
+// rows denspt keeps.
 __global__ void xc_basis_kernel(XcBasisParams B, const double4* __restrict__ pts, int P, const int* __restrict__ funcs,
-                                int nb, double* __restrict__ B5)
+                                int nb, const double* __restrict__ dense, int n, double* __restrict__ Bk,
+                                double* __restrict__ Psi)
 {
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)P * nb) return;
-    const int a = (int)(idx / P), g = (int)(idx - (long long)a * P);
+    const int g = (int)(idx / nb), a = (int)(idx - (long long)g * nb);
     const int f = funcs[a];
     const double4 pt = pts[g];
     const double4 c = B.center[f];
@@ -202,15 +230,16 @@ __global__ void xc_basis_kernel(XcBasisParams B, const double4* __restrict__ pts
         dy = sy * xi * zi;
         dz = sz * xi * yi;
     }
-    double* col = B5 + (size_t)a * 5 * P;
-    col[P + g] = phi;
-    col[2 * P + g] = dx;
-    col[3 * P + g] = dy;
-    col[4 * P + g] = dz;
+    const size_t blk = (size_t)nb * P, o = (size_t)g * nb + a;
+    Bk[blk + o] = phi;
+    Bk[2 * blk + o] = dx;
+    Bk[3 * blk + o] = dy;
+    Bk[4 * blk + o] = dz;
+    Psi[o] = dens_row(__ldg(dense + f + (size_t)f * n), phi, dx, dy, dz) ? phi : 0.0;
 }
 
 // U(a, b) = D(f_a, f_b) for b > a, D(f_a, f_a) / 2 for a == b, 0 below:
-// denspt's pair sum (gpu_getxc.cu:551-575) as rho = sum_a phi_a (U Phi)_a.
+// denspt's pair sum (gpu_getxc.cu:551-575) as rho = sum_a psi_a (U phi)_a.
 __global__ void xc_usub_kernel(const double* __restrict__ dense, int n, const int* __restrict__ funcs, int nb,
                                double* __restrict__ U)
 {
@@ -230,59 +259,70 @@ struct XcPointParams {
     const int* funcs;
     const double* dense;
     int n;
-    double* B5;                // ld 5P
-    const double* T;           // ld 4P: (U [Phi; dPhi]^T)^T
-    double* L;                 // ld 2P
+    double* Bk;                // [chi | phi | dphi/dx | dphi/dy | dphi/dz], nb x P each
+    const double* T0;          // nb x P: U phi
+    const double* S;           // nb x P: U^T psi
+    double* L;                 // nb x 2P: [phi' | chi'] (operator-loop row screen)
     double* e_pt;              // chunk's slice of the per-point arrays
     double* n_pt;
     int method;
 };
 
-// One thread per point: rho_alpha and its gradient, the functional, and the
-// operator factors (gpu_grid_xc, gpu_getxc.cu:144-265).
+// One warp per point: rho_alpha = sum psi T0 and grad rho_alpha =
+// sum dphi (S + screened T0) (T0 = U phi, S = U^T psi), the functional, and
+// the operator factors chi = w (f_rho/2 phi + f_sig4 grad rho_alpha . grad phi)
+// (gpu_grid_xc, gpu_getxc.cu:144-265).
 __global__ void xc_point_kernel(XcPointParams q)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (g >= q.P) return;
-    const int P = q.P;
-    const size_t ld5 = 5 * (size_t)P, ld4 = 4 * (size_t)P, ld2 = 2 * (size_t)P;
+    const int nb = q.nb;
+    const size_t blk = (size_t)nb * q.P, o = (size_t)g * nb;
+    double* chiv = q.Bk + o;
+    const double* phiv = q.Bk + blk + o;
+    const double* dxv = q.Bk + 2 * blk + o;
+    const double* dyv = q.Bk + 3 * blk + o;
+    const double* dzv = q.Bk + 4 * blk + o;
+    const double* t0v = q.T0 + o;
+    const double* sv = q.S + o;
     double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-    for (int a = 0; a < q.nb; a++) {
+    for (int a = lane; a < nb; a += 32) {
+        const double phi = phiv[a], dx = dxv[a], dy = dyv[a], dz = dzv[a];
         const int f = q.funcs[a];
-        const double dii = q.dense[f + (size_t)f * q.n];
-        const double* col = q.B5 + a * ld5;
-        const double phi = col[P + g], dx = col[2 * P + g], dy = col[3 * P + g], dz = col[4 * P + g];
-        if (fabs(dii) >= kXcCut && fabs(phi + dx + dy + dz) >= kXcCut) {
-            const double* tc = q.T + a * ld4;
-            const double t0 = tc[g], tx = tc[P + g], ty = tc[2 * P + g], tz = tc[3 * P + g];
-            rho += phi * t0;
-            gx += phi * tx + dx * t0;
-            gy += phi * ty + dy * t0;
-            gz += phi * tz + dz * t0;
-        }
+        const bool keep = dens_row(__ldg(q.dense + f + (size_t)f * q.n), phi, dx, dy, dz);
+        const double k0 = keep ? t0v[a] : 0.0;
+        const double s = sv[a] + k0;
+        rho += phi * k0;
+        gx += dx * s;
+        gy += dy * s;
+        gz += dz * s;
+    }
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+        rho += __shfl_xor_sync(FULL, rho, m);
+        gx += __shfl_xor_sync(FULL, gx, m);
+        gy += __shfl_xor_sync(FULL, gy, m);
+        gz += __shfl_xor_sync(FULL, gz, m);
     }
     const double w = q.pts[g].w;
     const bool ok = rho > kXcCut;
-    double frho = 0.0, fs4 = 0.0;
-    if (ok) {
-        const double sigma = 4.0 * (gx * gx + gy * gy + gz * gz);
-        const double f = xc_eval(q.method, 2.0 * rho, sigma, &frho, &fs4);
-        q.e_pt[g] = f * w;
-        q.n_pt[g] = w * rho;
-    } else {
-        q.e_pt[g] = 0.0;
-        q.n_pt[g] = 0.0;
+    double frho = 0.0, fs4 = 0.0, f = 0.0;
+    if (ok) f = xc_eval(q.method, 2.0 * rho, 4.0 * (gx * gx + gy * gy + gz * gz), &frho, &fs4);
+    if (lane == 0) {
+        q.e_pt[g] = ok ? f * w : 0.0;
+        q.n_pt[g] = ok ? w * rho : 0.0;
     }
     const double hx = fs4 * gx, hy = fs4 * gy, hz = fs4 * gz, hr = 0.5 * frho;
-    for (int a = 0; a < q.nb; a++) {
-        double* col = q.B5 + a * ld5;
-        const double phi = col[P + g], dx = col[2 * P + g], dy = col[3 * P + g], dz = col[4 * P + g];
+    double* lphi = q.L + o;
+    double* lchi = q.L + blk + o;
+    for (int a = lane; a < nb; a += 32) {
+        const double phi = phiv[a], dx = dxv[a], dy = dyv[a], dz = dzv[a];
         const double chi = ok ? w * (hr * phi + hx * dx + hy * dy + hz * dz) : 0.0;
         const bool m = ok && fabs(phi + dx + dy + dz) > kXcCut;
-        col[g] = chi;
-        double* lc = q.L + a * ld2;
-        lc[g] = m ? phi : 0.0;
-        lc[P + g] = m ? chi : 0.0;
+        chiv[a] = chi;
+        lphi[a] = m ? phi : 0.0;
+        lchi[a] = m ? chi : 0.0;
     }
 }
 
@@ -373,12 +413,13 @@ struct XcState {
     long long npts = 0;
     std::vector<XcChunk> chunks;
     int maxP = 0, maxNb = 0;
+    double alg_bytes = 0.0, alg_flops = 0.0, gemm_flops = 0.0;
     XcBuf<double4> d_pts, d_center;
     XcBuf<int4> d_itype;
     XcBuf<double> d_aexp, d_dcoeff;
     XcBuf<int> d_funcs;
     // work
-    XcBuf<double> d_B5, d_T, d_L, d_U, d_M, d_e, d_n, d_sum;
+    XcBuf<double> d_B, d_Psi, d_T0, d_S, d_L, d_U, d_M, d_e, d_n, d_sum;
     cublasHandle_t blas = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
@@ -542,6 +583,9 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
     *ms_grid = ms;
     d_leb.release(); d_leb_off.release(); d_atoms.release(); d_arad.release(); d_shells.release(); d_all.release();
 
+    const long long kXcChunkPoints = std::min<long long>((long long)env_or("QB_XC_POINTS", kXcChunkPointsDefault), 16384);
+    const double kXcCell = env_or("QB_XC_CELL", kXcCellDefault);
+    const double kXcChunkSpan = env_or("QB_XC_SPAN", kXcChunkSpanDefault);
     // keep points with weight above the cutoff, sort them into cells
     std::vector<double4> kept;
     kept.reserve(total);
@@ -550,7 +594,7 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
     const long long np = (long long)kept.size();
     std::vector<unsigned long long> key(np);
     for (long long i = 0; i < np; i++) {
-        auto cell = [](double v) {
+        auto cell = [kXcCell](double v) {
             long long c = (long long)floor(v / kXcCell) + (1LL << 20);
             return (unsigned long long)std::min<long long>(std::max<long long>(c, 0), (1LL << 21) - 1);
         };
@@ -636,6 +680,13 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
         S.maxP = std::max(S.maxP, ch.P);
         S.maxNb = std::max(S.maxNb, nbc);
     }
+    S.alg_bytes = S.alg_flops = S.gemm_flops = 0.0;
+    for (const XcChunk& ch : S.chunks) {
+        const double P = ch.P, nbd = ch.nb;
+        S.alg_bytes += P * nbd * 32.0 + 2.0 * nbd * nbd * 8.0;
+        S.alg_flops += 4.0 * P * nbd * nbd;
+        S.gemm_flops += 8.0 * P * nbd * nbd;
+    }
     // basis tables
     std::vector<double4> center(nb);
     std::vector<int4> itp(nb);
@@ -654,8 +705,10 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
     XCK(S.d_dcoeff.upload(dco, st));
     XCK(S.d_funcs.upload(funcs, st));
     const size_t P = S.maxP, N = S.maxNb;
-    XCK(S.d_B5.alloc(5 * P * N));
-    XCK(S.d_T.alloc(4 * P * N));
+    XCK(S.d_B.alloc(5 * P * N));
+    XCK(S.d_Psi.alloc(P * N));
+    XCK(S.d_T0.alloc(P * N));
+    XCK(S.d_S.alloc(P * N));
     XCK(S.d_L.alloc(2 * P * N));
     XCK(S.d_U.alloc(N * N));
     XCK(S.d_M.alloc(N * N));
@@ -698,17 +751,23 @@ int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResu
         const int P = ch.P, nb = ch.nb;
         const int* funcs = S.d_funcs.p + ch.f0;
         const double4* pts = S.d_pts.p + ch.p0;
-        long long work = (long long)P * nb;
-        xc_basis_kernel<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(bp, pts, P, funcs, nb, S.d_B5.p);
+        const long long work = (long long)P * nb;
+        const size_t blk = (size_t)P * nb;
+        xc_basis_kernel<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(bp, pts, P, funcs, nb, d_dense, n, S.d_B.p,
+                                                                        S.d_Psi.p);
         xc_usub_kernel<<<(nb * nb + 255) / 256, 256, 0, st>>>(d_dense, n, funcs, nb, S.d_U.p);
         g_launches += 2;
-        XBL(cublasDgemm(S.blas, CUBLAS_OP_N, CUBLAS_OP_T, 4 * P, nb, nb, &one, S.d_B5.p + P, 5 * P, S.d_U.p, nb,
-                        &zero, S.d_T.p, 4 * P));
-        XcPointParams q{pts, P, nb, funcs, d_dense, n, S.d_B5.p, S.d_T.p, S.d_L.p, S.d_e.p + ch.p0,
+        // T0 = U phi, S = U^T psi   (nb x P)
+        XBL(cublasDgemm(S.blas, CUBLAS_OP_N, CUBLAS_OP_N, nb, P, nb, &one, S.d_U.p, nb, S.d_B.p + blk, nb, &zero,
+                        S.d_T0.p, nb));
+        XBL(cublasDgemm(S.blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, P, nb, &one, S.d_U.p, nb, S.d_Psi.p, nb, &zero,
+                        S.d_S.p, nb));
+        XcPointParams q{pts, P, nb, funcs, d_dense, n, S.d_B.p, S.d_T0.p, S.d_S.p, S.d_L.p, S.d_e.p + ch.p0,
                         S.d_n.p + ch.p0, in.method};
-        xc_point_kernel<<<(P + 127) / 128, 128, 0, st>>>(q);
+        xc_point_kernel<<<(unsigned)((P * 32 + 127) / 128), 128, 0, st>>>(q);
         ++g_launches;
-        XBL(cublasDgemm(S.blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, nb, 2 * P, &one, S.d_L.p, 2 * P, S.d_B5.p, 5 * P, &zero,
+        // M = [phi' | chi'] [chi | phi]^T   (nb x nb, k = 2P)
+        XBL(cublasDgemm(S.blas, CUBLAS_OP_N, CUBLAS_OP_T, nb, nb, 2 * P, &one, S.d_L.p, nb, S.d_B.p, nb, &zero,
                         S.d_M.p, nb));
         xc_scatter_kernel<<<(nb * nb + 255) / 256, 256, 0, st>>>(S.d_M.p, nb, funcs, n, d_v);
         ++g_launches;
@@ -727,6 +786,9 @@ int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResu
     out->npts = S.npts;
     out->nchunks = (long long)S.chunks.size();
     out->ms = ms;
+    out->alg_bytes = S.alg_bytes;
+    out->alg_flops = S.alg_flops;
+    out->gemm_flops = S.gemm_flops;
     return 0;
 }
 
@@ -754,7 +816,8 @@ void xc_release()
     if (!g_xc) return;
     XcState& S = *g_xc;
     S.d_pts.release(); S.d_center.release(); S.d_itype.release(); S.d_aexp.release(); S.d_dcoeff.release();
-    S.d_funcs.release(); S.d_B5.release(); S.d_T.release(); S.d_L.release(); S.d_U.release(); S.d_M.release();
+    S.d_funcs.release(); S.d_B.release(); S.d_Psi.release(); S.d_T0.release(); S.d_S.release(); S.d_L.release();
+    S.d_U.release(); S.d_M.release();
     S.d_e.release(); S.d_n.release(); S.d_sum.release();
     S.valid = false;
 }

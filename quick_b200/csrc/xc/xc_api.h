@@ -26,6 +26,11 @@ struct XcResult {
     long long nchunks = 0;  // point chunks with at least one significant basis function
     double ms = 0.0;        // device time of the per-call phase
     double ms_grid = 0.0;   // device time of the grid build (0 when cached)
+    // algorithmic work of one call, summed over chunks of P points and nb
+    // functions: bytes = P nb (phi, grad phi: 4 x 8 B) + 2 nb^2 x 8 B (D and
+    // V tiles); flops = 4 P nb^2 (2 P nb^2 for rho, the same for V);
+    // gemm_flops = what the three DGEMMs execute (8 P nb^2).
+    double alg_bytes = 0.0, alg_flops = 0.0, gemm_flops = 0.0;
 };
 
 // Accumulates V_xc into the lower triangle of d_v (column-major nbasis^2,
