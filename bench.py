@@ -440,11 +440,15 @@ def run_xc(args, ws, rank, local, sess=None):
                    "chunks": st["nchunks"], "grid_build_ms": grid_ms, "l2": "flushed (256 MB write) before every call"},
         "e2e": {"value": st["npts"] * ws / (e2e_ms * 1e-3), "unit": "points/s", "ms_per_call": e2e_ms,
                 "h2d_bytes_per_step": int(2 * n * n * 8 + n * 8), "d2h_bytes_per_step": int(n * n * 8)},
-        "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
-                     "traffic": None, "peak_source": hbm_src,
-                     "bytes_per_call": st["alg_bytes"],
-                     "fp64_gemm_tflops": tfl, "fp64_peak_tflops": peak64.value / 1e3,
-                     "fp64_frac": tfl / (peak64.value / 1e3) if peak64.value else None},
+        # the three FP64 DGEMMs per chunk take over half the time (profiles/
+        # xc_quadrature_water32_631gss.md), so the bound is the FP64 pipe:
+        # achieved = the FLOPs those GEMMs execute per call / call time
+        "roofline": {"bound": "fp64", "achieved": tfl, "peak": peak64.value / 1e3, "unit": "TFLOP/s",
+                     "frac": tfl / (peak64.value / 1e3) if peak64.value else None, "traffic": None,
+                     "peak_source": "measured: FP64 FMA-chain probe run in this process (qb_fma_peak)",
+                     "gemm_flops_per_call": st["gemm_flops"], "alg_flops_per_call": st["alg_flops"],
+                     "hbm_gbs_of_alg_bytes": gbs, "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_src,
+                     "alg_bytes_per_call": st["alg_bytes"]},
         "gpu_launches": int(launches),
         "exc": exc.value,
     }

@@ -164,15 +164,33 @@ def shell_quartet(basis, xyz_bohr, ii, jj, kk, ll, I, J, K, L):
 _ref = None
 
 
-def ref_available():
-    return os.path.exists(os.path.join(LIBDIR, "libquickref.so"))
+_ref_spdf = None
 
 
-def ref_lib():
+_ref_variants = {}
+
+
+def _ref_dir(spdf):
+    """spdf: False (default build), True (CUDA_SPDF: QUICK's f-shell kernels)
+    or "boys" (CUDA_SPDF with QUICK's FmT replaced by an accurate Boys
+    function, build_ref.py --accurate-boys)."""
+    return {False: LIBDIR, True: os.path.join(LIBDIR, "spdf"), "boys": os.path.join(LIBDIR, "spdf_boys")}[spdf]
+
+
+def ref_available(spdf=False):
+    return os.path.exists(os.path.join(_ref_dir(spdf), "libquickref.so"))
+
+
+def ref_lib(spdf=False):
+    """QUICK's host build (see _ref_dir for the variants)."""
     global _ref
-    if _ref is None:
-        _ref = C.CDLL(os.path.join(LIBDIR, "libquickref.so"))
-    return _ref
+    if spdf is False:
+        if _ref is None:
+            _ref = C.CDLL(os.path.join(LIBDIR, "libquickref.so"))
+        return _ref
+    if spdf not in _ref_variants:
+        _ref_variants[spdf] = C.CDLL(os.path.join(_ref_dir(spdf), "libquickref.so"))
+    return _ref_variants[spdf]
 
 
 @contextlib.contextmanager
@@ -203,11 +221,11 @@ def _d(v):
 _ref_nshell = 0
 
 
-def ref_upload_molecule(mol, basis, YCutoff, cutPrim, threads=None):
+def ref_upload_molecule(mol, basis, YCutoff, cutPrim, threads=None, spdf=False):
     """QUICK's start-up upload sequence (src/main.f90:84-177)."""
     global _ref_nshell
     _ref_nshell = basis.nshell
-    r = ref_lib()
+    r = ref_lib(spdf)
     if threads:
         r.qref_set_threads(int(threads))
     b = basis
@@ -252,10 +270,10 @@ def ref_pairlist():
                 sorted_Q=q[:nq].copy(), sorted_Qnumber=qn[:nq].copy())
 
 
-def ref_get2e(O, dense, cutMatrix, integral_cutoff, prim_limit, method=0):
+def ref_get2e(O, dense, cutMatrix, integral_cutoff, prim_limit, method=0, spdf=False):
     """One QUICK Fock build: upload_method/calculated/cutoff + gpu_get2e_
     (src/hfoperator.f90:76-98).  Returns the new O."""
-    r = ref_lib()
+    r = ref_lib(spdf)
     n = O.shape[0]
     o = np.array(O, order="F", dtype=np.float64)
     co = np.zeros((n, n), order="F")

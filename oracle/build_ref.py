@@ -5,7 +5,7 @@ The sources are read where they lie in the QUICK tree (``src/cuda``); the
 shim in ``oracle/ref_shim`` supplies a host stand-in for the CUDA runtime and
 the launch geometry.  Build outputs go to ``oracle/_ref`` only.
 
-    python oracle/build_ref.py [--quick-root /root/reference] [--spdf]
+    python oracle/build_ref.py [--quick-root /root/reference] [--spdf] [--accurate-boys]
 """
 import argparse
 import os
@@ -20,7 +20,16 @@ OUT = os.path.join(HERE, "_ref")
 CUDA_INC = "/usr/local/cuda/include"
 
 
-def build(quick_root, spdf=False, jobs=8, opt="-O2"):
+def build(quick_root, spdf=False, accurate_boys=False, jobs=8, opt="-O2"):
+    """spdf: QUICK's f-shell kernels too (CUDA_SPDF), into oracle/_ref/spdf/.
+    accurate_boys (with spdf): QUICK's kernels with its Boys function FmT
+    replaced by an accurate one (qref_boys_accurate in ref_kernels.cpp), into
+    oracle/_ref/spdf_boys/ -- QUICK's upward recursion loses most digits for
+    small T and high m, and this build separates that from everything else."""
+    if accurate_boys:
+        OUT = os.path.join(HERE, "_ref", "spdf_boys")
+    else:
+        OUT = os.path.join(HERE, "_ref", "spdf") if spdf else os.path.join(HERE, "_ref")
     src = os.path.join(quick_root, "src", "cuda")
     if not os.path.isdir(src):
         raise FileNotFoundError("QUICK sources not found at %s" % src)
@@ -40,6 +49,23 @@ def build(quick_root, spdf=False, jobs=8, opt="-O2"):
     assert n == 1, "expected one getxc_kernel launch"
     with open(os.path.join(OUT, "gpu_getxc_host.cu"), "w") as fh:
         fh.write(xc)
+    if accurate_boys:
+        # build-directory copies: gpu_get2e.cu (so that its quoted includes
+        # look here first) and gpu_get2e_subs.h with QUICK's FmT renamed and
+        # an FmT that calls the accurate Boys function in its place
+        with open(os.path.join(src, "gpu_get2e.cu")) as fh:
+            g2 = fh.read()
+        with open(os.path.join(OUT, "gpu_get2e.cu"), "w") as fh:
+            fh.write(g2)
+        with open(os.path.join(src, "gpu_get2e_subs.h")) as fh:
+            sub = fh.read()
+        decl = "__device__ __forceinline__ void FmT(int MaxM, QUICKDouble X, QUICKDouble* YVerticalTemp)"
+        assert sub.count(decl) == 1, "expected one FmT definition"
+        sub = sub.replace(decl, "__device__ __forceinline__ void FmT(int MaxM, QUICKDouble X, QUICKDouble* YVerticalTemp)\n"
+                                "{ qref_boys_accurate(MaxM, X, YVerticalTemp); }\n"
+                                "__device__ __forceinline__ void FmT_quick(int MaxM, QUICKDouble X, QUICKDouble* YVerticalTemp)")
+        with open(os.path.join(OUT, "gpu_get2e_subs.h"), "w") as fh:
+            fh.write(sub)
     flags = [opt, "-fPIC", "-std=c++17", "-w", "-include", os.path.join(SHIM, "qref_shim.h"),
              "-I" + SHIM, "-I" + os.path.join(OUT, "inc"), "-I" + OUT, "-I" + src, "-I" + CUDA_INC]
     units = ["ref_bridge", "ref_kernels", "ref_type", "ref_xc"]
@@ -65,5 +91,6 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick-root", default="/root/reference")
     ap.add_argument("--spdf", action="store_true")
+    ap.add_argument("--accurate-boys", action="store_true")
     a = ap.parse_args()
-    print(build(a.quick_root, a.spdf))
+    print(build(a.quick_root, a.spdf or a.accurate_boys, a.accurate_boys))

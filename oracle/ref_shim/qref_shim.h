@@ -40,6 +40,10 @@ static inline unsigned int atomicAdd(unsigned int* a, unsigned int v)
     return __atomic_fetch_add(a, v, __ATOMIC_RELAXED);
 }
 
+/* F_m(x), m = 0..maxm, to full double precision (ref_kernels.cpp); the
+   accurate-Boys checker build calls it in place of QUICK's FmT. */
+void qref_boys_accurate(int maxm, double x, double* out);
+
 /* Runs the kernel named in a QUICK_SAFE_CALL launch expression on host
    threads (defined in ref_kernels.cpp). */
 void qref_launch(const char* launch_expression);

@@ -74,3 +74,44 @@ void qref_launch(const char* expr)
     }
     for (auto& th : pool) th.join();
 }
+
+/* QUICK's Boys function FmT (gpu_get2e_subs.h) at one argument, for checking
+   its accuracy: out[m] = F_m(x) for m = 0..maxm. */
+extern "C" void qref_fmt(int maxm, double x, double* out)
+{
+    QUICKDouble tmp[VDIM3];
+    FmT(maxm, x, tmp);
+    for (int m = 0; m <= maxm; m++) out[m] = tmp[m];
+}
+
+/* Boys function F_m(x) = int_0^1 t^(2m) exp(-x t^2) dt for m = 0..maxm,
+   in long double: for x < 35 the series F_M = e^-x sum_k (2x)^k /
+   ((2M+1)(2M+3)...(2M+2k+1)) for the top order and the stable downward
+   recursion F_m = (2x F_(m+1) + e^-x) / (2m+1); above, F_0 =
+   sqrt(pi/x) erf(sqrt x) / 2 and the (there stable) upward recursion. */
+void qref_boys_accurate(int maxm, double xd, double* out)
+{
+    const long double x = xd;
+    const long double e = expl(-x);
+    if (x < 35.0L) {
+        long double term = 1.0L / (2 * maxm + 1), sum = term;
+        for (int k = 1; k < 2000; k++) {
+            term *= 2.0L * x / (2 * maxm + 2 * k + 1);
+            sum += term;
+            if (term < 1e-22L * sum) break;
+        }
+        long double f = e * sum;
+        out[maxm] = (double)f;
+        for (int m = maxm - 1; m >= 0; m--) {
+            f = (2.0L * x * f + e) / (2 * m + 1);
+            out[m] = (double)f;
+        }
+    } else {
+        long double f = 0.5L * sqrtl(3.14159265358979323846264338327950288L / x) * erfl(sqrtl(x));
+        out[0] = (double)f;
+        for (int m = 1; m <= maxm; m++) {
+            f = ((2 * m - 1) * f - e) / (2.0L * x);
+            out[m] = (double)f;
+        }
+    }
+}

@@ -504,7 +504,9 @@ static int grad_build(Context& c)
         int block = 128;
         long long warps = (cnt[k] + 31) / 32;
         long long grid = std::min<long long>((warps * 32 + block - 1) / block, (long long)c.nsm * 16);
-        launch_grad_class(k, P, G, (int)std::max<long long>(grid, 1), block, c.stream);
+        if (launch_grad_class(k, P, G, (int)std::max<long long>(grid, 1), block, c.stream) < 0)
+            return set_error(5, "gpu_grad_: no gradient kernel for class (%d%d|%d%d): f shells are not built for "
+                                "the gradient", kClassL[k][0], kClassL[k][1], kClassL[k][2], kClassL[k][3]), 5;
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c.stream));
@@ -551,10 +553,10 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
             if (nq == 0) continue;
             (f32 ? total32 : total) += nq;
             const int G = c.class_group.empty() ? 1 : c.class_group[k];
-            if (f32)
-                launch_class32(k, P, G, nq, c.nsm, c.stream);
-            else
-                launch_class(k, P, G, nq, c.nsm, c.stream);
+            const int rc = f32 ? launch_class32(k, P, G, nq, c.nsm, c.stream) : launch_class(k, P, G, nq, c.nsm, c.stream);
+            if (rc < 0)
+                return set_error(5, "class (%d%d|%d%d) needs more shared memory than this GPU offers",
+                                 kClassL[k][0], kClassL[k][1], kClassL[k][2], kClassL[k][3]), 5;
         }
     }
     CK(cudaGetLastError());
@@ -1152,7 +1154,9 @@ int gpu_schwarz_(double* YCutoff, double* cutPrim)
     for (int t = 0; t < kNumPairTypes; t++) {
         if (tend[t] <= tbeg[t]) continue;
         int n = tend[t] - tbeg[t];
-        launch_schwarz(t, S, tbeg[t], tend[t], 0, std::min((n + 127) / 128, c.nsm * 8), 128, c.stream);
+        if (launch_schwarz(t, S, tbeg[t], tend[t], 0, std::min((n + 127) / 128, c.nsm * 8), 128, c.stream) < 0)
+            return set_error(5, "gpu_schwarz_: no Schwarz kernel for pair type (%d%d): f shells take YCutoff and "
+                                "cutPrim from the host", kPairTypeL[t][0], kPairTypeL[t][1]), 5;
         int np = pbf[tend[t] - 1].z + pbf[tend[t] - 1].w - pbf[tbeg[t]].z;
         launch_schwarz(t, S, tbeg[t], tend[t], 1, std::min((np + 127) / 128, c.nsm * 8), 128, c.stream);
     }

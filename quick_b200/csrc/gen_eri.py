@@ -612,14 +612,40 @@ def write_if_changed(path, src):
             fh.write(src)
 
 
-def main(outdir, lmax=2):
+def class_stats(la, lb, lc, ld):
+    """FLOP counts of a class without emitting code (for the classes the
+    generic kernel runs)."""
+    vrr = VRR()
+    for n1 in range(la, la + lb + 1):
+        for e in carts(n1):
+            for n2 in range(lc, lc + ld + 1):
+                for f in carts(n2):
+                    vrr.get(e, f, 0)
+    hrr = HRR()
+    A, B, Cc, D = QUICK_ORDER[la], QUICK_ORDER[lb], QUICK_ORDER[lc], QUICK_ORDER[ld]
+    for a in A:
+        for b in B:
+            for c in Cc:
+                for d in D:
+                    hrr.get(a, b, c, d)
+    ntar = sum(len(carts(n)) for n in range(la, la + lb + 1)) * sum(len(carts(n)) for n in range(lc, lc + ld + 1))
+    return dict(vrr_flops=vrr.nflops, vrr_nodes=len(vrr.lines), hrr_flops=hrr.nflops, targets=ntar,
+                ncomp=len(A) * len(B) * len(Cc) * len(D))
+
+
+def main(outdir, lmax=2, lmax_all=3):
+    """Straight-line kernels for the classes with every shell <= lmax; the
+    class table covers shells up to lmax_all (the rest run the generic
+    kernel, eri_generic.cu)."""
     os.makedirs(outdir, exist_ok=True)
+    cls_all = classes(lmax_all)
     cls = classes(lmax)
     lines = ["// generated by gen_eri.py", "#pragma once", "namespace qb {",
-             "static const int kNumClasses = %d;" % len(cls),
-             "static const int kClassL[%d][4] = {%s};" % (len(cls), ", ".join("{%d,%d,%d,%d}" % c for c in cls)),
-             "static const int kNumPairTypes = %d;" % len(pair_types(lmax)),
-             "static const int kPairTypeL[%d][2] = {%s};" % (len(pair_types(lmax)), ", ".join("{%d,%d}" % p for p in pair_types(lmax))),
+             "static const int kNumClasses = %d;" % len(cls_all),
+             "static const int kClassL[%d][4] = {%s};" % (len(cls_all), ", ".join("{%d,%d,%d,%d}" % c for c in cls_all)),
+             "static const int kNumPairTypes = %d;" % len(pair_types(lmax_all)),
+             "static const int kPairTypeL[%d][2] = {%s};" % (len(pair_types(lmax_all)), ", ".join("{%d,%d}" % p for p in pair_types(lmax_all))),
+             "static const int kGeneratedLmax = %d;   // classes above run the generic kernel" % lmax,
              "}"]
     with open(os.path.join(outdir, "eri_classes.h"), "w") as fh:
         fh.write("\n".join(lines) + "\n")
@@ -635,22 +661,34 @@ def main(outdir, lmax=2):
     for c in cls:
         lt.append("int launch_%d%d%d%d(const FockParams& P, int cls, int G, int nq, int nsm, cudaStream_t st);" % c)
         lt.append("int launch_%d%d%d%d_f32(const FockParams& P, int cls, int G, int nq, int nsm, cudaStream_t st);" % c)
+    lt.append("int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm, "
+              "int fp32_list, cudaStream_t st);")
+    gen_set = set(cls)
     lt += ["int launch_class(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st)", "{",
            "    switch (cls) {"]
-    for k, c in enumerate(cls):
-        lt.append("    case %d: return launch_%d%d%d%d(P, %d, G, nq, nsm, st);" % ((k,) + c + (k,)))
+    for k, c in enumerate(cls_all):
+        if c in gen_set:
+            lt.append("    case %d: return launch_%d%d%d%d(P, %d, G, nq, nsm, st);" % ((k,) + c + (k,)))
+        else:
+            lt.append("    case %d: return launch_generic_class(%d, %d, %d, %d, %d, P, nq, nsm, 0, st);" % ((k, k) + c))
     lt += ["    default: return 0;", "    }", "}"]
     lt += ["int launch_class32(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st)", "{",
            "    switch (cls) {"]
-    for k, c in enumerate(cls):
-        lt.append("    case %d: return launch_%d%d%d%d_f32(P, %d, G, nq, nsm, st);" % ((k,) + c + (k,)))
+    for k, c in enumerate(cls_all):
+        if c in gen_set:
+            lt.append("    case %d: return launch_%d%d%d%d_f32(P, %d, G, nq, nsm, st);" % ((k,) + c + (k,)))
+        else:
+            lt.append("    case %d: return launch_generic_class(%d, %d, %d, %d, %d, P, nq, nsm, 1, st);" % ((k, k) + c))
     lt += ["    default: return 0;", "    }", "}"]
     lt += ["int class_max_group(int cls)", "{", "    switch (cls) {"]
-    for k, c in enumerate(cls):
-        lt.append("    case %d: return %d;" % (k, max(group_sizes(*c))))
+    for k, c in enumerate(cls_all):
+        lt.append("    case %d: return %d;" % (k, max(group_sizes(*c)) if c in gen_set else 1))
     lt += ["    default: return 1;", "    }", "}", "}  // namespace qb"]
     write_if_changed(os.path.join(outdir, "eri_launch.cu"), "\n".join(lt) + "\n")
     import json
+    for c in cls_all:
+        if c not in stats:
+            stats[c] = class_stats(*c)
     write_if_changed(os.path.join(outdir, "class_flops.json"),
                      json.dumps({"%d%d%d%d" % c: s for c, s in stats.items()}, indent=1))
     # gradient kernels, one per class
@@ -668,13 +706,16 @@ def main(outdir, lmax=2):
             gstats[tg] = st_
             write_if_changed(os.path.join(outdir, "grad_%s.cu" % tg), src)
             gl.append("void launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int grid, int block, cudaStream_t st);" % tg)
-    gl += ["void launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st)",
+    gl += ["// returns 0, or -1 for a class without a gradient kernel (f shells)",
+           "int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st)",
            "{", "    switch (cls) {"]
-    for k, c in enumerate(cls):
+    for k, c in enumerate(cls_all):
+        if c not in parts:
+            continue
         calls = " ".join("launch_grad_%s(P, G, %d, grid, block, st);" % ("%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1]), k)
                          for pt in parts[c])
-        gl.append("    case %d: %s break;" % (k, calls))
-    gl += ["    default: break;", "    }", "}", "}  // namespace qb"]
+        gl.append("    case %d: %s return 0;" % (k, calls))
+    gl += ["    default: return -1;", "    }", "}", "}  // namespace qb"]
     write_if_changed(os.path.join(outdir, "grad_launch.cu"), "\n".join(gl) + "\n")
     write_if_changed(os.path.join(outdir, "grad_flops.json"), json.dumps(gstats, indent=1))
     # Schwarz kernels, one per pair type
@@ -682,11 +723,14 @@ def main(outdir, lmax=2):
     for t in pair_types(lmax):
         write_if_changed(os.path.join(outdir, "sch_%d%d.cu" % t), gen_schwarz(*t))
         st.append("void launch_schwarz_%d%d(const SchwarzParams& S, int begin, int end, int mode, int grid, int block, cudaStream_t st);" % t)
-    st += ["void launch_schwarz(int type, const SchwarzParams& S, int begin, int end, int mode, int grid, int block, cudaStream_t st)",
+    st += ["// returns 0, or -1 for a pair type without a Schwarz kernel (f shells)",
+           "int launch_schwarz(int type, const SchwarzParams& S, int begin, int end, int mode, int grid, int block, cudaStream_t st)",
            "{", "    switch (type) {"]
-    for k, t in enumerate(pair_types(lmax)):
-        st.append("    case %d: launch_schwarz_%d%d(S, begin, end, mode, grid, block, st); break;" % ((k,) + t))
-    st += ["    default: break;", "    }", "}", "}  // namespace qb"]
+    gen_types = set(pair_types(lmax))
+    for k, t in enumerate(pair_types(lmax_all)):
+        if t in gen_types:
+            st.append("    case %d: launch_schwarz_%d%d(S, begin, end, mode, grid, block, st); return 0;" % ((k,) + t))
+    st += ["    default: return -1;", "    }", "}", "}  // namespace qb"]
     write_if_changed(os.path.join(outdir, "sch_launch.cu"), "\n".join(st) + "\n")
     return stats
 

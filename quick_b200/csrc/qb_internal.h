@@ -43,7 +43,7 @@ void launch_fock_finish(const double* G, const double* cons, const double* Oin, 
 int launch_class(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st);
 int launch_class32(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st);
 int class_max_group(int cls);
-void launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st);
+int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st);
 int fma_probe(int fp64, int nsm, double* gflops, cudaStream_t st);
 void launch_count_prims(const FockParams& P, int ncls, unsigned long long* out, int nsm, cudaStream_t st);
 

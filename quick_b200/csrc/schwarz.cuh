@@ -47,6 +47,6 @@ __global__ void __launch_bounds__(128) schwarz_kernel(const SchwarzParams S, int
     }
 }
 
-void launch_schwarz(int type, const SchwarzParams& S, int begin, int end, int mode, int grid, int block, cudaStream_t st);
+int launch_schwarz(int type, const SchwarzParams& S, int begin, int end, int mode, int grid, int block, cudaStream_t st);
 
 }  // namespace qb

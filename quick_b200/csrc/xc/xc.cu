@@ -680,6 +680,11 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
         S.maxP = std::max(S.maxP, ch.P);
         S.maxNb = std::max(S.maxNb, nbc);
     }
+    // largest chunks first (the per-chunk sequence is serial on one stream;
+    // the biggest ones set the pace and are the ones worth profiling)
+    std::stable_sort(S.chunks.begin(), S.chunks.end(), [](const XcChunk& a, const XcChunk& b) {
+        return (double)a.P * a.nb * a.nb > (double)b.P * b.nb * b.nb;
+    });
     S.alg_bytes = S.alg_flops = S.gemm_flops = 0.0;
     for (const XcChunk& ch : S.chunks) {
         const double P = ch.P, nbd = ch.nb;
