@@ -91,6 +91,7 @@ struct Context {
     DevBuf<int2> d_quartets;
     std::vector<ScreenClass> screen_cls;
     std::vector<int> class_group;        // lanes per shell quartet of each class kernel
+    int generic_min_l = 99;              // classes with L sum >= this run the generic kernel (QB_GENERIC_MIN_L)
     // per-iteration
     std::vector<double> o_host;          // O as uploaded (one-electron part)
     std::vector<double> dense_host;
@@ -152,7 +153,7 @@ static int require(bool cond, const char* what)
 // downward recursion, which is stable.
 static void boys_table(std::vector<double>& tab)
 {
-    tab.assign((size_t)kBoysPoints * kBoysCols, 0.0);
+    tab.assign(kBoysTableSize, 0.0);
     for (int k = 0; k < kBoysPoints; k++) {
         long double T = (long double)k / kBoysPerUnit;
         int mmax = kBoysExpCol - 1;
@@ -171,6 +172,13 @@ static void boys_table(std::vector<double>& tab)
             tab[(size_t)k * kBoysCols + m] = (double)f;
         }
     }
+    // per-order records (eri_common.cuh: kBoysLOff)
+    for (int L = 0; L <= kBoysLMax; L++)
+        for (int k = 0; k < kBoysPoints; k++) {
+            double* r = tab.data() + kBoysLOff + ((size_t)L * kBoysPoints + k) * 8;
+            for (int j = 0; j < 7; j++) r[j] = tab[(size_t)k * kBoysCols + L + j];
+            r[7] = tab[(size_t)k * kBoysCols + kBoysExpCol];
+        }
 }
 
 // ------------------------------------------------------------- pair list
@@ -384,6 +392,8 @@ static int build_tables(Context& c)
     const char* gd = getenv("QB_FOCK_GDIV");
     const char* gf = getenv("QB_FOCK_G");
     const double div = gd && atof(gd) > 0 ? atof(gd) : 2.0;
+    const char* gm = getenv("QB_GENERIC_MIN_L");
+    c.generic_min_l = gm && atoi(gm) > 0 ? atoi(gm) : 99;
     c.class_group.assign(kNumClasses, 1);
     for (int k = 0; k < kNumClasses; k++) {
         double est = type_prims[pair_type_index(kClassL[k][0], kClassL[k][1])] *
@@ -553,7 +563,11 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
             if (nq == 0) continue;
             (f32 ? total32 : total) += nq;
             const int G = c.class_group.empty() ? 1 : c.class_group[k];
-            const int rc = f32 ? launch_class32(k, P, G, nq, c.nsm, c.stream) : launch_class(k, P, G, nq, c.nsm, c.stream);
+            const int* Lk = kClassL[k];
+            const bool gen = Lk[0] + Lk[1] + Lk[2] + Lk[3] >= c.generic_min_l;
+            const int rc = gen ? launch_generic_class(k, Lk[0], Lk[1], Lk[2], Lk[3], P, nq, c.nsm, f32, c.stream)
+                               : (f32 ? launch_class32(k, P, G, nq, c.nsm, c.stream)
+                                      : launch_class(k, P, G, nq, c.nsm, c.stream));
             if (rc < 0)
                 return set_error(5, "class (%d%d|%d%d) needs more shared memory than this GPU offers",
                                  kClassL[k][0], kClassL[k][1], kClassL[k][2], kClassL[k][3]), 5;

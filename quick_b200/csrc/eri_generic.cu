@@ -8,11 +8,15 @@
 //  * F_m(T), m = 0..LA+LB+LC+LD (lane 0, the table scheme of boys<L>);
 //  * the Obara-Saika vertical recurrence [e0|f0]^(m), |e| <= LA+LB,
 //    |f| <= LC+LD, one level of |f| at a time (three levels kept), the lanes
-//    of the warp sharing each level's entries;
+//    of the warp sharing each level's entries; a per-class program built
+//    once on the host lists every entry with its source offsets in shared
+//    memory, so the device loop is loads and FMAs;
 //  * contraction of [e0|f0]^(0) for LA <= |e|, LC <= |f| over the primitive
 //    quartets that pass QUICK's primitive screen;
 //  * the horizontal recurrence in closed form,
-//    (a b| = sum_k prod_i C(b_i, k_i) AB_i^(b_i - k_i) (a + k, 0|, on both sides;
+//    (a b| = sum_k prod_i C(b_i, k_i) AB_i^(b_i - k_i) (a + k, 0|, first on the
+//    ket side for all e, then on the bra side per integral (term lists from
+//    the same program);
 //  * the Coulomb/exchange digestion into six shared-memory blocks, flushed to
 //    the Fock matrix once per quartet with the weights of the generated
 //    kernels (digest_coulomb / digest_exchange).
@@ -20,6 +24,8 @@
 // QUICK's own spdf path (gpu_get2e_subs.h:413-850 with int.h's
 // vertical_spdf* and the 84 x 84 `store`) computes the same integrals.
 #include <algorithm>
+#include <map>
+#include <vector>
 
 #include "eri_common.cuh"
 #include "qb_internal.h"
@@ -32,14 +38,14 @@ __host__ __device__ constexpr int g_ncart(int l) { return l < 0 ? 0 : (l + 1) * 
 // number of Cartesians of all levels <= l
 __host__ __device__ constexpr int g_ncum(int l) { return l < 0 ? 0 : (l + 1) * (l + 2) * (l + 3) / 6; }
 
-// position of (x, y, z) inside its level (x descending, then y descending)
-__device__ __forceinline__ int g_lidx(int x, int y, int z)
+// ------------------------------------------------------------ host side
+static int h_lidx(int x, int y, int z)
 {
-    const int t = (x + y + z) - x;
-    (void)y;
+    const int t = y + z;
+    (void)x;
     return t * (t + 1) / 2 + z;
 }
-__device__ __forceinline__ void g_cart(int l, int idx, int& x, int& y, int& z)
+static void h_cart(int l, int idx, int& x, int& y, int& z)
 {
     int t = 0;
     while ((t + 1) * (t + 2) / 2 <= idx) t++;
@@ -47,35 +53,49 @@ __device__ __forceinline__ void g_cart(int l, int idx, int& x, int& y, int& z)
     x = l - t;
     y = t - z;
 }
-
-// QUICK's Cartesian order of a shell's components (basis.f90:546-643)
-__constant__ signed char c_quick_cart[4][10][3] = {
+static const int kQuickCartH[4][10][3] = {
     {{0, 0, 0}},
     {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}},
     {{2, 0, 0}, {1, 1, 0}, {0, 2, 0}, {1, 0, 1}, {0, 1, 1}, {0, 0, 2}},
     {{3, 0, 0}, {2, 1, 0}, {1, 2, 0}, {0, 3, 0}, {2, 0, 1}, {1, 1, 1}, {0, 2, 1}, {1, 0, 2}, {0, 1, 2}, {0, 0, 3}},
 };
 
-// Shared-memory layout of one class (doubles), computed on the host.
+// Shared-memory layout of one class (doubles).
 struct GenLayout {
     int la, lb, lc, ld;
     int lab, lcd, lt;
-    int level_size[13];   // entries of VRR level k = |f| (all e, all m)
-    int lvl_off[3];       // three rotating level buffers
+    int lvl_off[3];       // three rotating VRR level buffers (level 0 starts with F_m)
     int acc_off, ne, nf;  // contracted [e0|f0], |e| in [la, lab], |f| in [lc, lcd]
-    int f_off;            // F_m
+    int x_off;            // ket-transformed block X[e][cd] (reuses the level buffers)
+    int pw_off;           // AB and CD powers, 24 values
     int d_off;            // six density blocks
     int j_off;            // six accumulator blocks
     int total;
 };
 
-// entries of level k: for every f of the level, for every |e| = l <= lab,
-// ncart(l) x (lt - l - k + 1) values of m
-static int gen_level_size(int lab, int lt, int k)
+// The per-class program: every recurrence entry with its source offsets.
+struct GenProgram {
+    const int* stage;     // nstage x 3: type (0 bra level, 1 ket level, 2 contraction), first entry, count
+    int nstage;
+    const int4* ent;      // (out, a, c, g) shared-memory offsets; contraction: (acc index, source, -, -)
+    const int* meta;      // direction | mul_c << 2 | mul_g << 6 | nm << 10
+    const int* kstart;    // ket horizontal terms of component pair cd: [kstart[cd], kstart[cd+1])
+    const int4* kterm;    // (f local index, powers of C-D packed 4 bits each, binomial product, -)
+    const int* bstart;    // bra horizontal terms of component pair ab
+    const int4* bterm;    // (e local index, powers of A-B, binomial product, -)
+};
+
+static int level_per_f(int lab, int lt, int k)
 {
     int per_f = 0;
     for (int l = 0; l <= lab; l++) per_f += g_ncart(l) * std::max(0, lt - l - k + 1);
-    return per_f * g_ncart(k);
+    return per_f;
+}
+static int h_eoff(int lt, int k, int l, int idx)
+{
+    int off = 0;
+    for (int j = 0; j < l; j++) off += g_ncart(j) * (lt - j - k + 1);
+    return off + idx * (lt - l - k + 1);
 }
 
 static GenLayout gen_layout(int la, int lb, int lc, int ld)
@@ -86,19 +106,22 @@ static GenLayout gen_layout(int la, int lb, int lc, int ld)
     G.lcd = lc + ld;
     G.lt = G.lab + G.lcd;
     int mx = 0;
-    for (int k = 0; k <= G.lcd; k++) {
-        G.level_size[k] = gen_level_size(G.lab, G.lt, k);
-        mx = std::max(mx, G.level_size[k]);
-    }
-    int off = 0;
-    for (int j = 0; j < 3; j++) G.lvl_off[j] = off, off += mx;
+    for (int k = 0; k <= G.lcd; k++) mx = std::max(mx, level_per_f(G.lab, G.lt, k) * g_ncart(k));
     G.ne = g_ncum(G.lab) - g_ncum(la - 1);
     G.nf = g_ncum(G.lcd) - g_ncum(lc - 1);
+    const int nc = g_ncart(lc), nd = g_ncart(ld);
+    const int region = std::max(3 * mx, G.ne * nc * nd);
+    int off = 0;
+    G.lvl_off[0] = 0;
+    G.lvl_off[1] = mx;
+    G.lvl_off[2] = 2 * mx;
+    G.x_off = 0;
+    off = region;
     G.acc_off = off;
     off += G.ne * G.nf;
-    G.f_off = off;
-    off += G.lt + 8;
-    const int na = g_ncart(la), nb = g_ncart(lb), nc = g_ncart(lc), nd = g_ncart(ld);
+    G.pw_off = off;
+    off += 24;
+    const int na = g_ncart(la), nb = g_ncart(lb);
     const int blocks = na * nb + nc * nd + na * nc + na * nd + nb * nc + nb * nd;
     G.d_off = off;
     off += blocks;
@@ -108,19 +131,117 @@ static GenLayout gen_layout(int la, int lb, int lc, int ld)
     return G;
 }
 
-// offset of the (e, m = 0) entry of level k inside one f's block, for e of
-// level l at position idx: sum_{j<l} ncart(j)(lt - j - k + 1) + idx (lt - l - k + 1)
-__device__ __forceinline__ int g_eoff(const GenLayout& G, int k, int l, int idx)
+struct GenProgramHost {
+    std::vector<int> stage, meta, kstart, bstart;
+    std::vector<int4> ent, kterm, bterm;
+};
+
+static void gen_program(const GenLayout& G, GenProgramHost& H)
 {
-    int off = 0;
-    for (int j = 0; j < l; j++) off += g_ncart(j) * (G.lt - j - k + 1);
-    return off + idx * (G.lt - l - k + 1);
-}
-__device__ __forceinline__ int g_fblock(const GenLayout& G, int k)
-{
-    return G.level_size[k] / g_ncart(k);
+    const int lt = G.lt, lab = G.lab;
+    auto buf = [&](int k) { return G.lvl_off[k % 3]; };
+    auto meta = [](int i, int mc, int mg, int nm) { return i | (mc << 2) | (mg << 6) | (nm << 10); };
+    auto push_stage = [&](int type, int start) { H.stage.push_back(type); H.stage.push_back(start);
+                                                 H.stage.push_back((int)H.ent.size() - start); };
+    // contraction of level k into acc
+    auto contract = [&](int k) {
+        const int start = (int)H.ent.size();
+        const int per_f = level_per_f(lab, lt, k);
+        for (int eg = g_ncum(G.la - 1); eg < g_ncum(lab); eg++) {
+            int l = 0;
+            while (g_ncum(l) <= eg) l++;
+            const int eidx = eg - g_ncum(l - 1);
+            for (int fidx = 0; fidx < g_ncart(k); fidx++) {
+                const int ei = eg - g_ncum(G.la - 1);
+                const int fl = g_ncum(k - 1) - g_ncum(G.lc - 1) + fidx;
+                const int src = buf(k) + fidx * per_f + h_eoff(lt, k, l, eidx);
+                H.ent.push_back(make_int4(ei * G.nf + fl, src, 0, 0));
+                H.meta.push_back(0);
+            }
+        }
+        push_stage(2, start);
+    };
+    // bra levels of level 0: [e0|00]^(m)
+    for (int l = 1; l <= lab; l++) {
+        const int start = (int)H.ent.size();
+        for (int idx = 0; idx < g_ncart(l); idx++) {
+            int e[3];
+            h_cart(l, idx, e[0], e[1], e[2]);
+            const int i = e[0] ? 0 : (e[1] ? 1 : 2);
+            int e1[3] = {e[0], e[1], e[2]};
+            e1[i]--;
+            const int a = buf(0) + h_eoff(lt, 0, l - 1, h_lidx(e1[0], e1[1], e1[2]));
+            int c = -1;
+            if (e1[i] > 0) {
+                int e2[3] = {e1[0], e1[1], e1[2]};
+                e2[i]--;
+                c = buf(0) + h_eoff(lt, 0, l - 2, h_lidx(e2[0], e2[1], e2[2]));
+            }
+            H.ent.push_back(make_int4(buf(0) + h_eoff(lt, 0, l, idx), a, c, -1));
+            H.meta.push_back(meta(i, e1[i], 0, lt - l + 1));
+        }
+        push_stage(0, start);
+    }
+    if (G.lc == 0) contract(0);
+    // ket levels
+    for (int k = 1; k <= G.lcd; k++) {
+        const int start = (int)H.ent.size();
+        const int pf0 = level_per_f(lab, lt, k), pf1 = level_per_f(lab, lt, k - 1);
+        const int pf2 = k >= 2 ? level_per_f(lab, lt, k - 2) : 0;
+        for (int fidx = 0; fidx < g_ncart(k); fidx++) {
+            int f[3];
+            h_cart(k, fidx, f[0], f[1], f[2]);
+            const int i = f[0] ? 0 : (f[1] ? 1 : 2);
+            int f1[3] = {f[0], f[1], f[2]};
+            f1[i]--;
+            const int f1idx = h_lidx(f1[0], f1[1], f1[2]);
+            for (int l = 0; l <= lab; l++)
+                for (int eidx = 0; eidx < g_ncart(l); eidx++) {
+                    int e[3];
+                    h_cart(l, eidx, e[0], e[1], e[2]);
+                    const int a = buf(k - 1) + f1idx * pf1 + h_eoff(lt, k - 1, l, eidx);
+                    int c = -1, g = -1;
+                    if (f1[i] > 0) {
+                        int f2[3] = {f1[0], f1[1], f1[2]};
+                        f2[i]--;
+                        c = buf(k - 2) + h_lidx(f2[0], f2[1], f2[2]) * pf2 + h_eoff(lt, k - 2, l, eidx);
+                    }
+                    if (e[i] > 0) {
+                        int e1[3] = {e[0], e[1], e[2]};
+                        e1[i]--;
+                        g = buf(k - 1) + f1idx * pf1 + h_eoff(lt, k - 1, l - 1, h_lidx(e1[0], e1[1], e1[2]));
+                    }
+                    H.ent.push_back(make_int4(buf(k) + fidx * pf0 + h_eoff(lt, k, l, eidx), a, c, g));
+                    H.meta.push_back(meta(i, f1[i], e[i], lt - l - k + 1));
+                }
+        }
+        push_stage(1, start);
+        if (k >= G.lc) contract(k);
+    }
+    // horizontal terms, closed binomial form
+    auto binom = [](int n, int k) { int r = 1; for (int j = 1; j <= k; j++) r = r * (n - k + j) / j; return r; };
+    auto terms = [&](int l1, int l2, std::vector<int>& start, std::vector<int4>& out) {
+        for (int i1 = 0; i1 < g_ncart(l1); i1++)
+            for (int i2 = 0; i2 < g_ncart(l2); i2++) {
+                start.push_back((int)out.size());
+                const int* A = kQuickCartH[l1][i1];
+                const int* B = kQuickCartH[l2][i2];
+                for (int kx = 0; kx <= B[0]; kx++)
+                    for (int ky = 0; ky <= B[1]; ky++)
+                        for (int kz = 0; kz <= B[2]; kz++) {
+                            const int x = A[0] + kx, y = A[1] + ky, z = A[2] + kz;
+                            const int loc = g_ncum(x + y + z - 1) + h_lidx(x, y, z) - g_ncum(l1 - 1);
+                            const int pw = (B[0] - kx) | ((B[1] - ky) << 4) | ((B[2] - kz) << 8);
+                            out.push_back(make_int4(loc, pw, binom(B[0], kx) * binom(B[1], ky) * binom(B[2], kz), 0));
+                        }
+            }
+        start.push_back((int)out.size());
+    };
+    terms(G.lc, G.ld, H.kstart, H.kterm);
+    terms(G.la, G.lb, H.bstart, H.bterm);
 }
 
+// ------------------------------------------------------------ device side
 // F_m(T) times pref for m = 0..L with a runtime L (the scheme of boys<L>).
 __device__ void boys_rt(const double* __restrict__ tab, double T, double pref, double* F, int L)
 {
@@ -153,25 +274,12 @@ __device__ void boys_rt(const double* __restrict__ tab, double T, double pref, d
     for (int m = 0; m <= L; m++) F[m] *= pref;
 }
 
-__device__ __forceinline__ double ipow(double x, int n)
+// One shell quartet with the 32 lanes of a warp: primitive loop with the
+// vertical recurrence and contraction, program-driven.
+__device__ void generic_quartet(const QuartetCtx& q, const FockParams& P, const GenLayout& G, const GenProgram& R,
+                                double* sm, int lane)
 {
-    double r = 1.0;
-    for (int i = 0; i < n; i++) r *= x;
-    return r;
-}
-__device__ __forceinline__ double binom(int n, int k)
-{
-    double r = 1.0;
-    for (int i = 1; i <= k; i++) r = r * (n - k + i) / i;
-    return r;
-}
-
-// One shell quartet with the 32 lanes of a warp.
-__device__ void generic_quartet(const QuartetCtx& q, const FockParams& P, const GenLayout& G, double* sm, int lane)
-{
-    const int lab = G.lab, lt = G.lt;
     double* acc = sm + G.acc_off;
-    double* F = sm + G.f_off;
     for (int i = lane; i < G.ne * G.nf; i += 32) acc[i] = 0.0;
     __syncwarp();
     for (int ib = 0; ib < q.nbra; ib++) {
@@ -185,117 +293,72 @@ __device__ void generic_quartet(const QuartetCtx& q, const FockParams& P, const 
             const double sq = rsqrt(pq);
             const double ipq = sq * sq;
             const double rho = pb.p * pk.p * ipq;
-            const double PQ[3] = {pb.Px - pk.Px, pb.Py - pk.Py, pb.Pz - pk.Pz};
-            const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-            const double WP[3] = {-pk.p * ipq * PQ[0], -pk.p * ipq * PQ[1], -pk.p * ipq * PQ[2]};
-            const double WQ[3] = {pb.p * ipq * PQ[0], pb.p * ipq * PQ[1], pb.p * ipq * PQ[2]};
+            const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
+            const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double fp = -pk.p * ipq, fq = pb.p * ipq;
+            const double WP[3] = {fp * PQx, fp * PQy, fp * PQz};
+            const double WQ[3] = {fq * PQx, fq * PQy, fq * PQz};
             const double PA[3] = {pb.PAx, pb.PAy, pb.PAz};
             const double QC[3] = {pk.PAx, pk.PAy, pk.PAz};
             const double o2p = pb.o2p, o2q = pk.o2p, o2pq = 0.5 * ipq;
             const double rp = pk.p * ipq, rq = pb.p * ipq;
-            if (lane == 0) boys_rt(P.boys, T, pb.K * pk.K * sq, F, lt);
+            if (lane == 0) boys_rt(P.boys, T, pb.K * pk.K * sq, sm + G.lvl_off[0], G.lt);
             __syncwarp();
-            // level 0: [e0|00]^(m), |e| <= lab, m <= lt - |e|, by |e|
-            double* L0 = sm + G.lvl_off[0];
-            for (int m = lane; m <= lt; m += 32) L0[m] = F[m];
-            __syncwarp();
-            for (int l = 1; l <= lab; l++) {
-                const int nm = lt - l + 1, cnt = g_ncart(l) * nm;
-                for (int t = lane; t < cnt; t += 32) {
-                    const int idx = t / nm, m = t - idx * nm;
-                    int e[3];
-                    g_cart(l, idx, e[0], e[1], e[2]);
-                    const int i = e[0] ? 0 : (e[1] ? 1 : 2);
-                    int e1[3] = {e[0], e[1], e[2]};
-                    e1[i]--;
-                    const double* a = L0 + g_eoff(G, 0, l - 1, g_lidx(e1[0], e1[1], e1[2]));
-                    double v = PA[i] * a[m] + WP[i] * a[m + 1];
-                    if (e1[i] > 0) {
-                        int e2[3] = {e1[0], e1[1], e1[2]};
-                        e2[i]--;
-                        const double* c = L0 + g_eoff(G, 0, l - 2, g_lidx(e2[0], e2[1], e2[2]));
-                        v += e1[i] * o2p * (c[m] - rp * c[m + 1]);
-                    }
-                    L0[g_eoff(G, 0, l, idx) + m] = v;
-                }
-                __syncwarp();
-            }
-            // levels k = 1..lcd: [e0|f0]^(m) from levels k-1 and k-2
-            for (int k = 0; k <= G.lcd; k++) {
-                double* Lk = sm + G.lvl_off[k % 3];
-                if (k > 0) {
-                    const double* L1 = sm + G.lvl_off[(k + 2) % 3];   // level k-1
-                    const double* L2 = sm + G.lvl_off[(k + 1) % 3];   // level k-2
-                    const int fb1 = g_fblock(G, k - 1), fb0 = g_fblock(G, k);
-                    const int fb2 = k >= 2 ? g_fblock(G, k - 2) : 0;
-                    const int per_f = fb0;
-                    const int cnt = g_ncart(k) * per_f;
+            for (int s = 0; s < R.nstage; s++) {
+                const int type = R.stage[3 * s], first = R.stage[3 * s + 1], cnt = R.stage[3 * s + 2];
+                if (type == 2) {
                     for (int t = lane; t < cnt; t += 32) {
-                        const int fidx = t / per_f;
-                        int r = t - fidx * per_f;
-                        // locate (e level l, e idx, m) inside the f block
-                        int l = 0;
-                        while (r >= g_ncart(l) * (lt - l - k + 1)) r -= g_ncart(l) * (lt - l - k + 1), l++;
-                        const int nm = lt - l - k + 1;
-                        const int eidx = r / nm, m = r - eidx * nm;
-                        int e[3], f[3];
-                        g_cart(l, eidx, e[0], e[1], e[2]);
-                        g_cart(k, fidx, f[0], f[1], f[2]);
-                        const int i = f[0] ? 0 : (f[1] ? 1 : 2);
-                        int f1[3] = {f[0], f[1], f[2]};
-                        f1[i]--;
-                        const double* a = L1 + g_lidx(f1[0], f1[1], f1[2]) * fb1 + g_eoff(G, k - 1, l, eidx);
-                        double v = QC[i] * a[m] + WQ[i] * a[m + 1];
-                        if (f1[i] > 0) {
-                            int f2[3] = {f1[0], f1[1], f1[2]};
-                            f2[i]--;
-                            const double* c = L2 + g_lidx(f2[0], f2[1], f2[2]) * fb2 + g_eoff(G, k - 2, l, eidx);
-                            v += f1[i] * o2q * (c[m] - rq * c[m + 1]);
-                        }
-                        if (e[i] > 0) {
-                            int e1[3] = {e[0], e[1], e[2]};
-                            e1[i]--;
-                            const double* c = L1 + g_lidx(f1[0], f1[1], f1[2]) * fb1 +
-                                              g_eoff(G, k - 1, l - 1, g_lidx(e1[0], e1[1], e1[2]));
-                            v += e[i] * o2pq * c[m + 1];
-                        }
-                        Lk[fidx * fb0 + g_eoff(G, k, l, eidx) + m] = v;
+                        const int4 e = R.ent[first + t];
+                        acc[e.x] += sm[e.y];
                     }
-                    __syncwarp();
-                }
-                // contract the targets of this level
-                if (k >= G.lc) {
-                    const int fb0 = g_fblock(G, k);
-                    const int nfl = g_ncart(k);
-                    const int e0 = g_ncum(G.la - 1);
-                    const int ntar = G.ne * nfl;
-                    for (int t = lane; t < ntar; t += 32) {
-                        const int ei = t / nfl, fidx = t - ei * nfl;
-                        const int eg = e0 + ei;   // global e index
-                        int l = 0;
-                        while (g_ncum(l) <= eg) l++;
-                        const int eidx = eg - g_ncum(l - 1);
-                        const int fl = g_ncum(k - 1) - g_ncum(G.lc - 1) + fidx;
-                        acc[ei * G.nf + fl] += Lk[fidx * fb0 + g_eoff(G, k, l, eidx)];
+                } else {
+                    for (int t = lane; t < cnt; t += 32) {
+                        const int4 e = R.ent[first + t];
+                        const int mt = R.meta[first + t];
+                        const int i = mt & 3, mc = (mt >> 2) & 15, mg = (mt >> 6) & 15, nm = mt >> 10;
+                        const double* a = sm + e.y;
+                        double* o = sm + e.x;
+                        const double ci = type == 0 ? PA[i] : QC[i];
+                        const double wi = type == 0 ? WP[i] : WQ[i];
+                        const double cm = mc * (type == 0 ? o2p : o2q), r = type == 0 ? rp : rq;
+                        const double* c = sm + (e.z >= 0 ? e.z : 0);
+                        const double* gg = sm + (e.w >= 0 ? e.w : 0);
+                        const double gm = mg * o2pq;
+                        for (int m = 0; m < nm; m++) {
+                            double v = ci * a[m] + wi * a[m + 1];
+                            if (e.z >= 0) v += cm * (c[m] - r * c[m + 1]);
+                            if (e.w >= 0) v += gm * gg[m + 1];
+                            o[m] = v;
+                        }
                     }
                 }
                 __syncwarp();
             }
         }
     }
-    (void)lab;
 }
 
-// Digestion of the contracted block: closed-form horizontal recurrence per
-// integral, six shared-memory accumulators, one flush per quartet.
-__device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const GenLayout& G, double* sm, int lane)
+// Horizontal recurrence in closed form (ket side into X, then bra side per
+// integral) and the Coulomb/exchange digestion into six shared-memory
+// blocks, flushed once per quartet with the weights of digest_coulomb /
+// digest_exchange.
+__device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const GenLayout& G, const GenProgram& R,
+                               double* sm, int lane)
 {
-    const int la = G.la, lb = G.lb, lc = G.lc, ld = G.ld;
-    const int na = g_ncart(la), nb = g_ncart(lb), nc = g_ncart(lc), nd = g_ncart(ld);
+    const int na = g_ncart(G.la), nb = g_ncart(G.lb), nc = g_ncart(G.lc), nd = g_ncart(G.ld);
+    const int ncd = nc * nd;
     const double* acc = sm + G.acc_off;
+    double* X = sm + G.x_off;
+    double* pw = sm + G.pw_off;
     double* Db = sm + G.d_off;
     double* Jb = sm + G.j_off;
-    // density blocks: ab, cd, ac, ad, bc, bd
+    if (lane < 24) {
+        const double AB[3] = {q.ABx, q.ABy, q.ABz}, CD[3] = {q.CDx, q.CDy, q.CDz};
+        const double base = lane < 12 ? AB[lane / 4] : CD[(lane - 12) / 4];
+        double v = 1.0;
+        for (int k = 0; k < (lane & 3); k++) v *= base;
+        pw[lane] = v;
+    }
     const int o_ab = 0, o_cd = o_ab + na * nb, o_ac = o_cd + nc * nd, o_ad = o_ac + na * nc, o_bc = o_ad + na * nd,
               o_bd = o_bc + nb * nc, nblk = o_bd + nb * nd;
     const double* Dm = P.dense;
@@ -313,36 +376,27 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         Jb[t] = 0.0;
     }
     __syncwarp();
-    const double AB[3] = {q.ABx, q.ABy, q.ABz}, CD[3] = {q.CDx, q.CDy, q.CDz};
-    const bool exch = P.hybrid != 0.0;
-    const int nout = na * nb * nc * nd;
-    const int e0 = g_ncum(la - 1), f0 = g_ncum(lc - 1);
-    for (int o = lane; o < nout; o += 32) {
-        const int id = o % nd, ic = (o / nd) % nc, ib = (o / (nd * nc)) % nb, ia = o / (nd * nc * nb);
-        const signed char* A = c_quick_cart[la][ia];
-        const signed char* B = c_quick_cart[lb][ib];
-        const signed char* Cc = c_quick_cart[lc][ic];
-        const signed char* D = c_quick_cart[ld][id];
+    // ket side: X[e][cd] = sum_k C * CD^pw * acc[e][f]
+    for (int t = lane; t < G.ne * ncd; t += 32) {
+        const int e = t / ncd, cd = t - e * ncd;
         double v = 0.0;
-        for (int kx = 0; kx <= B[0]; kx++)
-            for (int ky = 0; ky <= B[1]; ky++)
-                for (int kz = 0; kz <= B[2]; kz++) {
-                    const double cb = binom(B[0], kx) * binom(B[1], ky) * binom(B[2], kz) * ipow(AB[0], B[0] - kx) *
-                                      ipow(AB[1], B[1] - ky) * ipow(AB[2], B[2] - kz);
-                    const int ex = A[0] + kx, ey = A[1] + ky, ez = A[2] + kz;
-                    const int eg = g_ncum(ex + ey + ez - 1) + g_lidx(ex, ey, ez) - e0;
-                    double s = 0.0;
-                    for (int jx = 0; jx <= D[0]; jx++)
-                        for (int jy = 0; jy <= D[1]; jy++)
-                            for (int jz = 0; jz <= D[2]; jz++) {
-                                const double cd = binom(D[0], jx) * binom(D[1], jy) * binom(D[2], jz) *
-                                                  ipow(CD[0], D[0] - jx) * ipow(CD[1], D[1] - jy) * ipow(CD[2], D[2] - jz);
-                                const int fx = Cc[0] + jx, fy = Cc[1] + jy, fz = Cc[2] + jz;
-                                const int fg = g_ncum(fx + fy + fz - 1) + g_lidx(fx, fy, fz) - f0;
-                                s += cd * acc[eg * G.nf + fg];
-                            }
-                    v += cb * s;
-                }
+        for (int j = R.kstart[cd]; j < R.kstart[cd + 1]; j++) {
+            const int4 k = R.kterm[j];
+            v += k.z * pw[12 + (k.y & 15)] * pw[16 + ((k.y >> 4) & 15)] * pw[20 + (k.y >> 8)] * acc[e * G.nf + k.x];
+        }
+        X[t] = v;
+    }
+    __syncwarp();
+    const bool exch = P.hybrid != 0.0;
+    const int nout = na * nb * ncd;
+    for (int o = lane; o < nout; o += 32) {
+        const int ab = o / ncd, cd = o - ab * ncd;
+        const int ia = ab / nb, ib = ab - ia * nb, ic = cd / nd, id = cd - ic * nd;
+        double v = 0.0;
+        for (int j = R.bstart[ab]; j < R.bstart[ab + 1]; j++) {
+            const int4 k = R.bterm[j];
+            v += k.z * pw[k.y & 15] * pw[4 + ((k.y >> 4) & 15)] * pw[8 + (k.y >> 8)] * X[k.x * ncd + cd];
+        }
         atomicAdd(Jb + o_ab + ia * nb + ib, Db[o_cd + ic * nd + id] * v);
         atomicAdd(Jb + o_cd + ic * nd + id, Db[o_ab + ia * nb + ib] * v);
         if (exch) {
@@ -353,7 +407,6 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         }
     }
     __syncwarp();
-    // flush with the weights of digest_coulomb / digest_exchange
     const double wj = 2.0 * q.w, wk = -0.5 * P.hybrid * q.w;
     for (int t = lane; t < (exch ? nblk : o_ac); t += 32) {
         int r, c;
@@ -370,8 +423,9 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
 }
 
 // One warp (one block) per shell quartet; fp32_list: walk the class's FP32
-// list (mixed precision) — these classes compute in FP64 either way.
-__global__ void __launch_bounds__(32) fock_generic_kernel(const FockParams P, int cls, const GenLayout G, int fp32_list)
+// list (mixed precision) -- these classes compute in FP64 either way.
+__global__ void __launch_bounds__(32) fock_generic_kernel(const FockParams P, int cls, const GenLayout G,
+                                                         const GenProgram R, int fp32_list)
 {
     extern __shared__ double sm[];
     const int lane = threadIdx.x;
@@ -380,24 +434,71 @@ __global__ void __launch_bounds__(32) fock_generic_kernel(const FockParams P, in
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
         QuartetCtx q;
         load_quartet(P, list[i], true, q);
-        generic_quartet(q, P, G, sm, lane);
-        generic_digest(q, P, G, sm, lane);
+        generic_quartet(q, P, G, R, sm, lane);
+        generic_digest(q, P, G, R, sm, lane);
     }
+}
+
+// ------------------------------------------------------------ launch
+struct GenCached {
+    GenLayout G;
+    GenProgram R;
+    void* mem = nullptr;
+    int dev = -1;
+};
+
+static GenCached* gen_cached(int la, int lb, int lc, int ld)
+{
+    static std::map<int, GenCached> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int key = ((la * 4 + lb) * 4 + lc) * 4 + ld + 256 * dev;
+    auto it = cache.find(key);
+    if (it != cache.end()) return &it->second;
+    GenCached c;
+    c.G = gen_layout(la, lb, lc, ld);
+    GenProgramHost H;
+    gen_program(c.G, H);
+    const size_t b_stage = H.stage.size() * sizeof(int), b_meta = H.meta.size() * sizeof(int);
+    const size_t b_ent = H.ent.size() * sizeof(int4), b_kt = H.kterm.size() * sizeof(int4),
+                 b_bt = H.bterm.size() * sizeof(int4);
+    const size_t b_ks = H.kstart.size() * sizeof(int), b_bs = H.bstart.size() * sizeof(int);
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t total = up(b_stage) + up(b_meta) + up(b_ent) + up(b_kt) + up(b_bt) + up(b_ks) + up(b_bs);
+    if (cudaMalloc(&c.mem, total) != cudaSuccess) return nullptr;
+    char* p = (char*)c.mem;
+    auto put = [&](const void* src, size_t bytes) {
+        void* dst = p;
+        if (bytes) cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+        p += up(bytes);
+        return dst;
+    };
+    c.R.stage = (const int*)put(H.stage.data(), b_stage);
+    c.R.nstage = (int)H.stage.size() / 3;
+    c.R.meta = (const int*)put(H.meta.data(), b_meta);
+    c.R.ent = (const int4*)put(H.ent.data(), b_ent);
+    c.R.kterm = (const int4*)put(H.kterm.data(), b_kt);
+    c.R.bterm = (const int4*)put(H.bterm.data(), b_bt);
+    c.R.kstart = (const int*)put(H.kstart.data(), b_ks);
+    c.R.bstart = (const int*)put(H.bstart.data(), b_bs);
+    c.dev = dev;
+    return &(cache[key] = c);
 }
 
 int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm, int fp32_list,
                          cudaStream_t st)
 {
     if (nq <= 0) return 0;
-    const GenLayout G = gen_layout(la, lb, lc, ld);
-    const size_t bytes = (size_t)G.total * sizeof(double);
+    const GenCached* gc = gen_cached(la, lb, lc, ld);
+    if (!gc) return -1;
+    const size_t bytes = (size_t)gc->G.total * sizeof(double);
     int dev = 0, maxsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (bytes > (size_t)maxsm) return -1;
-    static size_t configured = 0;
-    if (bytes > 48 * 1024 && bytes > configured) {
-        if (cudaFuncSetAttribute(fock_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxsm) !=
+    static int configured = 0;
+    if (bytes > 48 * 1024 && configured < maxsm) {
+        if (cudaFuncSetAttribute(fock_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm) !=
             cudaSuccess)
             return -1;
         configured = maxsm;
@@ -405,7 +506,7 @@ int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockPara
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fock_generic_kernel, 32, bytes);
     const int grid = std::max(1, std::min(nq, nsm * std::max(per_sm, 1)));
-    QB_LAUNCH(fock_generic_kernel, grid, 32, bytes, st, P, cls, G, fp32_list);
+    QB_LAUNCH(fock_generic_kernel, grid, 32, bytes, st, P, cls, gc->G, gc->R, fp32_list);
     return 32;
 }
 

@@ -273,6 +273,9 @@ def gen_class(la, lb, lc, ld, prec="double"):
     w("    }")
     w("    QuartetCtx qa = q;")
     w("    qa.active = q.active && sub == 0;   // the group's first lane digests")
+    dg = []
+    w_run = w
+    w = dg.append
     if f32:
         w("    const float ABx = (float)q.ABx, ABy = (float)q.ABy, ABz = (float)q.ABz, CDx = (float)q.CDx, CDy = (float)q.CDy, CDz = (float)q.CDz;")
     else:
@@ -341,6 +344,9 @@ def gen_class(la, lb, lc, ld, prec="double"):
     for ic in range(nc):
         for id_ in range(nd):
             w("    digest_coulomb(P, qa, c0+%d, d0+%d, Jcd_%d_%d);" % (ic, id_, ic, id_))
+    w = w_run
+    for ln in dg:
+        w(ln)
     w("}")
     w("};")
     gs = group_sizes(la, lb, lc, ld)
@@ -639,7 +645,11 @@ def main(outdir, lmax=2, lmax_all=3):
     kernel, eri_generic.cu)."""
     os.makedirs(outdir, exist_ok=True)
     cls_all = classes(lmax_all)
-    cls = classes(lmax)
+    # straight-line kernels: every class up to lmax, and the f classes whose
+    # total angular momentum is at most 6 (the larger ones run the generic
+    # kernel; their straight-line code would take hours to compile)
+    cls = [c for c in cls_all if max(c) <= lmax or sum(c) <= 6]
+    cls_grad = classes(lmax)
     lines = ["// generated by gen_eri.py", "#pragma once", "namespace qb {",
              "static const int kNumClasses = %d;" % len(cls_all),
              "static const int kClassL[%d][4] = {%s};" % (len(cls_all), ", ".join("{%d,%d,%d,%d}" % c for c in cls_all)),
@@ -695,7 +705,7 @@ def main(outdir, lmax=2, lmax_all=3):
     gl = ['#include "eri_common.cuh"', '#include "grad_common.cuh"', '#include "eri_classes.h"', "namespace qb {"]
     gstats = {}
     parts = {}
-    for c in cls:
+    for c in cls_grad:
         # classes with total angular momentum >= 7 get one kernel per
         # derivative centre (A, B, C): a third of the code each, which keeps
         # the compile time of the largest classes in minutes

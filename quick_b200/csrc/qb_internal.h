@@ -43,6 +43,11 @@ void launch_fock_finish(const double* G, const double* cons, const double* Oin, 
 int launch_class(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st);
 int launch_class32(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st);
 int class_max_group(int cls);
+// The warp-per-quartet kernel of eri_generic.cu for any class (shells <= f);
+// fp32_list: walk the class's FP32 list.  Returns -1 if the class needs more
+// shared memory than the GPU offers.
+int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm, int fp32_list,
+                         cudaStream_t st);
 int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st);
 int fma_probe(int fp64, int nsm, double* gflops, cudaStream_t st);
 void launch_count_prims(const FockParams& P, int ncls, unsigned long long* out, int nsm, cudaStream_t st);

@@ -690,7 +690,7 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
         const double P = ch.P, nbd = ch.nb;
         S.alg_bytes += P * nbd * 32.0 + 2.0 * nbd * nbd * 8.0;
         S.alg_flops += 4.0 * P * nbd * nbd;
-        S.gemm_flops += 8.0 * P * nbd * nbd;
+        S.gemm_flops += 6.0 * P * nbd * nbd;   // two triangular products (nb^2 P each) + the 4 nb^2 P GEMM
     }
     // basis tables
     std::vector<double4> center(nb);
@@ -762,11 +762,11 @@ int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResu
                                                                         S.d_Psi.p);
         xc_usub_kernel<<<(nb * nb + 255) / 256, 256, 0, st>>>(d_dense, n, funcs, nb, S.d_U.p);
         g_launches += 2;
-        // T0 = U phi, S = U^T psi   (nb x P)
-        XBL(cublasDgemm(S.blas, CUBLAS_OP_N, CUBLAS_OP_N, nb, P, nb, &one, S.d_U.p, nb, S.d_B.p + blk, nb, &zero,
-                        S.d_T0.p, nb));
-        XBL(cublasDgemm(S.blas, CUBLAS_OP_T, CUBLAS_OP_N, nb, P, nb, &one, S.d_U.p, nb, S.d_Psi.p, nb, &zero,
-                        S.d_S.p, nb));
+        // T0 = U phi, S = U^T psi   (nb x P; U upper triangular: half a GEMM each)
+        XBL(cublasDtrmm(S.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, P,
+                        &one, S.d_U.p, nb, S.d_B.p + blk, nb, S.d_T0.p, nb));
+        XBL(cublasDtrmm(S.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, nb, P,
+                        &one, S.d_U.p, nb, S.d_Psi.p, nb, S.d_S.p, nb));
         XcPointParams q{pts, P, nb, funcs, d_dense, n, S.d_B.p, S.d_T0.p, S.d_S.p, S.d_L.p, S.d_e.p + ch.p0,
                         S.d_n.p + ch.p0, in.method};
         xc_point_kernel<<<(unsigned)((P * 32 + 127) / 128), 128, 0, st>>>(q);

@@ -29,7 +29,8 @@ struct XcResult {
     // algorithmic work of one call, summed over chunks of P points and nb
     // functions: bytes = P nb (phi, grad phi: 4 x 8 B) + 2 nb^2 x 8 B (D and
     // V tiles); flops = 4 P nb^2 (2 P nb^2 for rho, the same for V);
-    // gemm_flops = what the three DGEMMs execute (8 P nb^2).
+    // gemm_flops = what the two triangular products and the DGEMM
+    // execute (P nb^2 + P nb^2 + 4 P nb^2).
     double alg_bytes = 0.0, alg_flops = 0.0, gemm_flops = 0.0;
 };
 
