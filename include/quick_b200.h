@@ -104,7 +104,12 @@ int qb_build_pairlist_host(int Qshell, const int* sorted_Q, const int* sorted_Qn
 int gpu_schwarz_(double* YCutoff, double* cutPrim);
 
 /* Fock build on device-resident data: D (nbasis^2, device pointer), O_in and O_out (device
-   pointers, may alias).  Uses the cutoffs and density screen from the last gpu_upload_cutoff_. */
+   pointers, may alias).  Uses the cutoffs and density screen from the last gpu_upload_cutoff_.
+   Asynchronous: the work is enqueued on the library stream (qb_set_stream) and O_out is valid
+   once that stream has been synchronised.  After one call with the same molecule and cutoffs
+   (which sizes the quartet lists and builds the per-class tables) the call allocates nothing and
+   waits for nothing, so it can be captured into a CUDA graph and replayed; the density and
+   cutMatrix buffers it reads are the ones given / last uploaded. */
 int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out);
 
 /* No counterpart in QUICK.  The same Fock build as qb_fock_device for callers that cannot
@@ -148,7 +153,7 @@ int qb_last_xc_stats(long long* npts, long long* nchunks, double* ms, double* ms
 /* Algorithmic work of the last XC quadrature, summed over its point chunks (P points, nb
    significant functions each): bytes = P nb x 32 (phi and grad phi) + 2 nb^2 x 8 (density and
    operator tiles), flops = 4 P nb^2 (density and operator contractions), gemm_flops = the
-   8 P nb^2 the three DGEMMs execute. */
+   6 P nb^2 the two triangular products and the operator DGEMM execute. */
 int qb_last_xc_work(double* bytes, double* flops, double* gemm_flops);
 
 /* The kept grid points (x, y, z, weight per point) of the last XC grid build; copies up to cap

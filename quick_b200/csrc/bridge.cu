@@ -89,6 +89,7 @@ struct Context {
     DevBuf<int> d_class_count, d_class_count32, d_overflow;
     DevBuf<long long> d_class_offset, d_class_end;
     DevBuf<int2> d_quartets;
+    DevBuf<int2> d_ket_segs;             // constant primitive-count segments of the pair table
     std::vector<ScreenClass> screen_cls;
     std::vector<int> class_group;        // lanes per shell quartet of each class kernel
     int generic_min_l = 99;              // classes with L sum >= this run the generic kernel (QB_GENERIC_MIN_L)
@@ -103,6 +104,7 @@ struct Context {
     bool have_grad = false;
     // stats
     long long last_quartets = 0, last_quartets32 = 0;
+    bool stats_pending = false;          // the last Fock build's counts are still on the device
     double mixed_cut = 0.0;      // Fock builds: quartets with Y Y DNMax below this run in FP32 (0: all FP64)
     XcResult last_xc;
     double last_ms_eri = 0, last_ms_screen = 0;
@@ -284,7 +286,7 @@ static int pair_type_index(int la, int lb)
 static int build_tables(Context& c)
 {
     struct Rec {
-        int type, shA, shB, LA, LB, ref, key;
+        int type, shA, shB, LA, LB, ref, key, np;
         double Y, w;
     };
     std::vector<Rec> recs;
@@ -302,10 +304,16 @@ static int build_tables(Context& c)
         else { e.shA = sy; e.LA = Ly; e.shB = sx; e.LB = Lx; }
         e.type = pair_type_index(e.LA, e.LB);
         if (e.type < 0) return set_error(1, "angular momentum (%d,%d) beyond this build", e.LA, e.LB), 1;
+        e.np = c.kprim[e.shA] * c.kprim[e.shB];
         recs.push_back(e);
     }
+    // by pair type, then primitive-pair count (descending), then Schwarz
+    // bound (descending): the screen walks each constant-count segment in
+    // bound order, so the quartets of one bra come out grouped by the ket's
+    // primitive count and the lanes of a warp run loops of equal length
     std::stable_sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) {
         if (a.type != b.type) return a.type < b.type;
+        if (a.np != b.np) return a.np > b.np;
         return a.Y > b.Y;
     });
     c.npair = (int)recs.size();
@@ -316,6 +324,22 @@ static int build_tables(Context& c)
         while (i < c.npair && recs[i].type == t) i++;
         c.type_end[t] = i;
     }
+    // constant primitive-count segments of each pair type
+    std::vector<int2> segs;
+    std::vector<int> tseg_begin(kNumPairTypes), tseg_end(kNumPairTypes);
+    for (int t = 0; t < kNumPairTypes; t++) {
+        tseg_begin[t] = (int)segs.size();
+        for (int i = c.type_begin[t]; i < c.type_end[t];) {
+            int j = i;
+            while (j < c.type_end[t] && recs[j].np == recs[i].np) j++;
+            segs.push_back(make_int2(i, j));
+            i = j;
+        }
+        tseg_end[t] = (int)segs.size();
+    }
+    CK(c.d_ket_segs.alloc(std::max<size_t>(segs.size(), 1)));
+    if (!segs.empty())
+        CK(cudaMemcpy(c.d_ket_segs.p, segs.data(), segs.size() * sizeof(int2), cudaMemcpyHostToDevice));
     std::vector<int4> pbf(c.npair), psh(c.npair);
     std::vector<double> pY(c.npair);
     std::vector<double4> pAB(c.npair);
@@ -375,6 +399,8 @@ static int build_tables(Context& c)
         s.bra_end = c.type_end[tb];
         s.ket_begin = c.type_begin[tk];
         s.ket_end = c.type_end[tk];
+        s.seg_begin = tseg_begin[tk];
+        s.seg_end = tseg_end[tk];
         s.same_type = tb == tk;
         s.out_offset = 0;
         s.capacity = 0;
@@ -429,6 +455,7 @@ static FockParams fock_params(Context& c)
     P.mixed_cut = c.mixed_cut;
     P.class_count32 = c.d_class_count32.p;
     P.class_end = c.d_class_end.p;
+    P.ket_segs = c.d_ket_segs.p;
     return P;
 }
 
@@ -548,20 +575,16 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
     launch_finish_counts(S, c.d_class_count.p, c.d_class_count32.p, c.d_overflow.p, kNumClasses, c.stream);
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[1], c.stream));
-    std::vector<int> cnt(kNumClasses), cnt32(kNumClasses);
-    int ovf = 0;
-    CK(cudaMemcpyAsync(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaMemcpyAsync(cnt32.data(), c.d_class_count32.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaMemcpyAsync(&ovf, c.d_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaStreamSynchronize(c.stream));
-    if (ovf) return set_error(3, "quartet list overflow (internal sizing error)"), 3;
-    long long total = 0, total32 = 0;
+    // The class kernels read their quartet counts on the device; the host
+    // sizes their grids by the Schwarz-only capacity of each class (an upper
+    // bound), so nothing between screening and digestion waits for the host
+    // and the whole build can be captured in a CUDA graph.
     CK(cudaEventRecord(c.ev[2], c.stream));
     for (int k = 0; k < kNumClasses; k++) {
-        for (int f32 = 0; f32 < 2; f32++) {
-            const int nq = f32 ? cnt32[k] : cnt[k];
-            if (nq == 0) continue;
-            (f32 ? total32 : total) += nq;
+        const long long cap = c.screen_cls[k].capacity;
+        if (cap == 0) continue;
+        const int nq = (int)std::min<long long>(cap, 1LL << 30);
+        for (int f32 = 0; f32 < (c.mixed_cut > 0.0 ? 2 : 1); f32++) {
             const int G = c.class_group.empty() ? 1 : c.class_group[k];
             const int* Lk = kClassL[k];
             const bool gen = Lk[0] + Lk[1] + Lk[2] + Lk[3] >= c.generic_min_l;
@@ -577,7 +600,25 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
     CK(cudaEventRecord(c.ev[3], c.stream));
     launch_fock_finish(c.d_fock.p, c.d_cons.p, d_o_in, d_o_out, n, c.stream);
     CK(cudaGetLastError());
+    c.stats_pending = true;
+    return 0;
+}
+
+// Counts, timings and the overflow flag of the last Fock build, read once
+// it has finished (synchronises the library stream).
+static int fock_stats_resolve(Context& c)
+{
+    if (!c.stats_pending) return 0;
+    c.stats_pending = false;
+    std::vector<int> cnt(kNumClasses), cnt32(kNumClasses);
+    int ovf = 0;
+    CK(cudaMemcpyAsync(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(cnt32.data(), c.d_class_count32.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&ovf, c.d_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    if (ovf) return set_error(3, "quartet list overflow (internal sizing error)"), 3;
+    long long total = 0, total32 = 0;
+    for (int k = 0; k < kNumClasses; k++) total += cnt[k], total32 += cnt32[k];
     float ms0 = 0, ms1 = 0;
     CK(cudaEventElapsedTime(&ms0, c.ev[0], c.ev[1]));
     CK(cudaEventElapsedTime(&ms1, c.ev[2], c.ev[3]));
@@ -681,6 +722,7 @@ void gpu_shutdown_(void)
     c.d_class_offset.release();
     c.d_class_end.release();
     c.d_quartets.release();
+    c.d_ket_segs.release();
     for (auto& e : c.ev)
         if (e) cudaEventDestroy(e), e = nullptr;
     xc_release();
@@ -880,6 +922,7 @@ void gpu_get2e_(double* o)
         set_error(2, "download of the operator failed");
         return;
     }
+    fock_stats_resolve(c);
 }
 
 int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out)
@@ -971,6 +1014,7 @@ int qb_set_mixed_precision(double cut)
 int qb_last_fock_split(long long* quartets_fp64, long long* quartets_fp32)
 {
     Context& c = ctx();
+    if (int rc = fock_stats_resolve(c)) return rc;
     *quartets_fp32 = c.last_quartets32;
     *quartets_fp64 = c.last_quartets - c.last_quartets32;
     return 0;
@@ -979,6 +1023,7 @@ int qb_last_fock_split(long long* quartets_fp64, long long* quartets_fp32)
 int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen)
 {
     Context& c = ctx();
+    if (int rc = fock_stats_resolve(c)) return rc;
     *quartets = c.last_quartets;
     *ms_eri = c.last_ms_eri;
     *ms_screen = c.last_ms_screen;
@@ -1168,10 +1213,15 @@ int gpu_schwarz_(double* YCutoff, double* cutPrim)
     for (int t = 0; t < kNumPairTypes; t++) {
         if (tend[t] <= tbeg[t]) continue;
         int n = tend[t] - tbeg[t];
-        if (launch_schwarz(t, S, tbeg[t], tend[t], 0, std::min((n + 127) / 128, c.nsm * 8), 128, c.stream) < 0)
-            return set_error(5, "gpu_schwarz_: no Schwarz kernel for pair type (%d%d): f shells take YCutoff and "
-                                "cutPrim from the host", kPairTypeL[t][0], kPairTypeL[t][1]), 5;
         int np = pbf[tend[t] - 1].z + pbf[tend[t] - 1].w - pbf[tbeg[t]].z;
+        if (launch_schwarz(t, S, tbeg[t], tend[t], 0, std::min((n + 127) / 128, c.nsm * 8), 128, c.stream) < 0) {
+            // pair types with an f shell: the generic recurrence program
+            if (launch_generic_schwarz(kPairTypeL[t][0], kPairTypeL[t][1], S, tbeg[t], tend[t], 0, c.nsm, c.stream) < 0 ||
+                launch_generic_schwarz(kPairTypeL[t][0], kPairTypeL[t][1], S, tbeg[t], tend[t], 1, c.nsm, c.stream) < 0)
+                return set_error(5, "gpu_schwarz_: pair type (%d%d) needs more shared memory than this GPU offers",
+                                 kPairTypeL[t][0], kPairTypeL[t][1]), 5;
+            continue;
+        }
         launch_schwarz(t, S, tbeg[t], tend[t], 1, std::min((np + 127) / 128, c.nsm * 8), 128, c.stream);
     }
     CK(cudaGetLastError());

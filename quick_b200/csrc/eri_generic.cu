@@ -29,6 +29,7 @@
 
 #include "eri_common.cuh"
 #include "qb_internal.h"
+#include "schwarz.cuh"
 
 namespace qb {
 
@@ -439,6 +440,83 @@ __global__ void __launch_bounds__(32) fock_generic_kernel(const FockParams P, in
     }
 }
 
+// Schwarz records of an f pair type (schwarz_kernel's contract): mode 0,
+// one warp per (shell pair, sub-shell pair) record with all its primitive
+// pairs; mode 1, one warp per primitive pair alone.  The diagonal block
+// (ab|ab) comes from the class (LA LB | LA LB) program; the output is
+// max over components of |(ab|ab)| cons_a^2 cons_b^2.
+__global__ void __launch_bounds__(32) schwarz_generic_kernel(const SchwarzParams S, const FockParams P,
+                                                            const GenLayout G, const GenProgram R, int begin,
+                                                            int end, int mode)
+{
+    extern __shared__ double sm[];
+    const int lane = threadIdx.x;
+    const int na = g_ncart(G.la), nb = g_ncart(G.lb);
+    const int p_begin = S.pair_bf[begin].z;
+    const int4 last = S.pair_bf[end - 1];
+    const int nwork = mode == 0 ? end - begin : last.z + last.w - p_begin;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        int rec = begin + w, p0 = 0, np = 0;
+        if (mode == 0) {
+            np = S.pair_bf[rec].w;
+        } else {
+            const int p = p_begin + w;
+            int lo = begin, hi = end - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (S.pair_bf[mid].z <= p) lo = mid; else hi = mid - 1;
+            }
+            rec = lo;
+            p0 = p - S.pair_bf[rec].z;
+            np = 1;
+        }
+        const int4 info = S.pair_bf[rec];
+        const double4 ab = S.pair_AB[rec];
+        QuartetCtx q{};
+        q.active = true;
+        q.bra_off = q.ket_off = info.z + p0;
+        q.nbra = q.nket = np;
+        q.ABx = q.CDx = ab.x;
+        q.ABy = q.CDy = ab.y;
+        q.ABz = q.CDz = ab.z;
+        q.dnmax = 1.0;
+        q.swap = false;
+        generic_quartet(q, P, G, R, sm, lane);
+        double* pw = sm + G.pw_off;
+        if (lane < 24) {
+            const double base = lane < 12 ? (&ab.x)[lane / 4] : (&ab.x)[(lane - 12) / 4];
+            double v = 1.0;
+            for (int k = 0; k < (lane & 3); k++) v *= base;
+            pw[lane] = v;
+        }
+        __syncwarp();
+        const double* acc = sm + G.acc_off;
+        double mx = 0.0;
+        for (int o = lane; o < na * nb; o += 32) {
+            double v = 0.0;
+            for (int jb = R.bstart[o]; jb < R.bstart[o + 1]; jb++) {
+                const int4 tb = R.bterm[jb];
+                double sk = 0.0;
+                for (int jk = R.kstart[o]; jk < R.kstart[o + 1]; jk++) {
+                    const int4 tk = R.kterm[jk];
+                    sk += tk.z * pw[12 + (tk.y & 15)] * pw[16 + ((tk.y >> 4) & 15)] * pw[20 + (tk.y >> 8)] *
+                          acc[tb.x * G.nf + tk.x];
+                }
+                v += tb.z * pw[tb.y & 15] * pw[4 + ((tb.y >> 4) & 15)] * pw[8 + (tb.y >> 8)] * sk;
+            }
+            const double ca = S.cons[info.x + o / nb], cb = S.cons[info.y + o % nb];
+            mx = fmax(mx, fabs(v) * ca * ca * cb * cb);
+        }
+#pragma unroll
+        for (int k = 16; k > 0; k >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, k));
+        if (lane == 0) {
+            if (mode == 0) S.out_contracted[rec] = mx;
+            else S.out_prim[p_begin + w] = mx;
+        }
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------ launch
 struct GenCached {
     GenLayout G;
@@ -508,6 +586,31 @@ int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockPara
     const int grid = std::max(1, std::min(nq, nsm * std::max(per_sm, 1)));
     QB_LAUNCH(fock_generic_kernel, grid, 32, bytes, st, P, cls, gc->G, gc->R, fp32_list);
     return 32;
+}
+
+int launch_generic_schwarz(int la, int lb, const SchwarzParams& S, int begin, int end, int mode, int nsm,
+                           cudaStream_t st)
+{
+    if (end <= begin) return 0;
+    const GenCached* gc = gen_cached(la, lb, la, lb);
+    if (!gc) return -1;
+    const size_t bytes = (size_t)gc->G.total * sizeof(double);
+    int dev = 0, maxsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (bytes > (size_t)maxsm) return -1;
+    if (bytes > 48 * 1024 &&
+        cudaFuncSetAttribute(schwarz_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm) != cudaSuccess)
+        return -1;
+    FockParams P{};
+    P.prim = S.prim;
+    P.boys = S.boys;
+    P.prim_limit = -1.0;   // every primitive pair counts in the bound
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, schwarz_generic_kernel, 32, bytes);
+    const int grid = std::max(1, nsm * std::max(per_sm, 1));
+    QB_LAUNCH(schwarz_generic_kernel, grid, 32, bytes, st, S, P, gc->G, gc->R, begin, end, mode);
+    return 0;
 }
 
 size_t generic_class_smem(int la, int lb, int lc, int ld)

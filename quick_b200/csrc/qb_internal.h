@@ -11,6 +11,7 @@ struct ScreenClass {
     int bra_begin, bra_end;     // bra pairs (indices into the pair table)
     int ket_begin, ket_end;     // ket pairs
     int same_type;              // bra and ket of the same pair type: kets b >= a only
+    int seg_begin, seg_end;     // the ket type's constant primitive-count segments (FockParams::ket_segs)
     long long out_offset;       // first slot of this class in the quartet buffer
     long long capacity;         // slots reserved for this class
 };

@@ -48,5 +48,8 @@ __global__ void __launch_bounds__(128) schwarz_kernel(const SchwarzParams S, int
 }
 
 int launch_schwarz(int type, const SchwarzParams& S, int begin, int end, int mode, int grid, int block, cudaStream_t st);
+// The same for any pair type up to f with the generic recurrence program (eri_generic.cu).
+int launch_generic_schwarz(int la, int lb, const SchwarzParams& S, int begin, int end, int mode, int nsm,
+                           cudaStream_t st);
 
 }  // namespace qb

@@ -7,9 +7,10 @@
 
 namespace qb {
 
-// One warp per (class, bra pair).  Kets of the class's ket type are sorted
-// by Schwarz bound, descending, so the scan stops at the first ket whose
-// bound product fails.  count_only: Schwarz test only, just count (used once
+// One warp per (class, bra pair).  The kets of the class's ket type come in
+// segments of equal primitive count, each sorted by Schwarz bound,
+// descending, so the scan of a segment stops at the first ket whose bound
+// product fails.  count_only: Schwarz test only, just count (used once
 // per geometry to size the lists).
 __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const FockParams P, int count_only)
 {
@@ -22,12 +23,15 @@ __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const
     for (int a = c.bra_begin + warp; a < c.bra_end; a += nwarps) {
         const double Ya = P.pair_Y[a];
         const int4 sa = P.pair_sh[a];
-        const int kb = c.same_type ? a : c.ket_begin;
-        for (int k0 = kb; k0 < c.ket_end; k0 += 32) {
-            if (!(P.pair_Y[k0] * Ya > cut)) break;      // sorted: the rest fail too
+        for (int sg = c.seg_begin; sg < c.seg_end; sg++) {
+        const int2 seg = P.ket_segs[sg];
+        if (c.same_type && seg.y <= a) continue;
+        const int kb = c.same_type ? max(a, seg.x) : seg.x;
+        for (int k0 = kb; k0 < seg.y; k0 += 32) {
+            if (!(P.pair_Y[k0] * Ya > cut)) break;      // sorted inside the segment: the rest fail too
             const int b = k0 + lane;
             bool pass = false, low = false;
-            if (b < c.ket_end) {
+            if (b < seg.y) {
                 const double yy = P.pair_Y[b] * Ya;
                 if (yy > cut) {
                     if (count_only) {
@@ -61,6 +65,7 @@ __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const
                         S.out[c.out_offset + c.capacity - 1 - pos] = make_int2(a, b);
                 }
             }
+        }
         }
     }
 }

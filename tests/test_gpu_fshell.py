@@ -1,7 +1,8 @@
 """f shells (cc-pVTZ: d on H, f on O): every class with an f shell runs the
 generic warp-per-quartet kernel (eri_generic.cu).  Fock matrices against the
-oracle (itself pinned to QUICK's CUDA_SPDF kernels, tests/test_oracle_spdf.py)
-at 1e-8; f shells have no gradient or Schwarz kernel and say so."""
+oracle (itself pinned to QUICK's CUDA_SPDF kernels where those are right,
+tests/test_oracle_fshell.py) at 1e-8; Schwarz bounds for f pair types on the
+GPU; f shells have no gradient kernel and say so."""
 import numpy as np
 import pytest
 
@@ -58,7 +59,23 @@ def test_fshell_mixed_precision_list(session, oracle_lib):
     assert np.abs(got - ref).max() < 1e-7
 
 
-def test_fshell_gradient_and_schwarz_report_missing_kernels(session, oracle_lib):
+def test_fshell_schwarz_bounds_on_gpu(session, oracle_lib):
+    """gpu_schwarz_ for pair types with an f shell runs the generic
+    recurrence program; YCutoff and cutPrim as QUICK's schwarz.f90 defines
+    them (the oracle's restatement).  The closed-form horizontal recurrence
+    sums in another order than the oracle's, which costs up to 2e-10
+    relative on the smallest d/f bounds (measured; 1e-12 elsewhere), so the
+    tolerance is 1e-9 relative."""
+    m, b = _mol((2, 1, 1))
+    session.upload_molecule(m, b)            # Schwarz bounds from the GPU
+    Yo, cpo = oracle_lib.schwarz(b, m.xyz_bohr)
+    np.testing.assert_allclose(session.YCutoff, Yo, rtol=1e-9, atol=1e-300)
+    # cutPrim of far-apart primitive pairs reaches 1e-160; such values screen
+    # nothing and their last digits are noise in either code
+    np.testing.assert_allclose(session.cutPrim, cpo, rtol=1e-9, atol=1e-30)
+
+
+def test_fshell_gradient_reports_missing_kernel(session, oracle_lib):
     from quick_b200 import capi
     m, b = _mol((1, 1, 1))
     Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
@@ -67,5 +84,3 @@ def test_fshell_gradient_and_schwarz_report_missing_kernels(session, oracle_lib)
     cm = oracle_lib.cutmatrix(b, D)
     with pytest.raises(capi.QuickB200Error, match="f shells"):
         session.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
-    with pytest.raises(capi.QuickB200Error, match="f shells"):
-        session.schwarz()
