@@ -129,6 +129,10 @@ int qb_fock_device_static(const double* d_dense, const double* d_o_in, double* d
    kernels in ms, device time of the screening in ms. */
 int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen);
 
+/* Statistics of the last gpu_grad_: shell quartets differentiated and the device time of the
+   gradient class kernels in ms. */
+int qb_last_grad_stats(long long* quartets, double* ms);
+
 /* Mixed precision for the following Fock builds (no counterpart in QUICK, which is FP64
    throughout): shell quartets whose bound Y_ab Y_cd DNMax (QUICK's own screening product,
    gpu_get2e_subs.h:323-328) is below cut run their Boys function, recurrences and contraction

@@ -188,6 +188,11 @@ class Session:
         lib().qb_last_fock_split(C.byref(a), C.byref(b))
         return dict(fp64=a.value, fp32=b.value)
 
+    def grad_stats(self):
+        q, a = C.c_longlong(0), C.c_double(0)
+        lib().qb_last_grad_stats(C.byref(q), C.byref(a))
+        return dict(quartets=q.value, ms=a.value)
+
     def fock_stats(self):
         q, a, b = C.c_longlong(0), C.c_double(0), C.c_double(0)
         lib().qb_last_fock_stats(C.byref(q), C.byref(a), C.byref(b))

@@ -104,6 +104,8 @@ struct Context {
     bool have_grad = false;
     // stats
     long long last_quartets = 0, last_quartets32 = 0;
+    long long last_grad_quartets = 0;
+    double last_ms_grad = 0.0;
     bool stats_pending = false;          // the last Fock build's counts are still on the device
     double mixed_cut = 0.0;      // Fock builds: quartets with Y Y DNMax below this run in FP32 (0: all FP64)
     XcResult last_xc;
@@ -536,6 +538,11 @@ static int grad_build(Context& c)
     CK(cudaMemsetAsync(c.d_grad.p, 0, 3 * (size_t)c.natom * sizeof(double), c.stream));
     FockParams P = fock_params(c);
     GradExtra G{c.d_shell_atom.p, c.d_pair_sh.p, c.d_grad.p};
+    for (int k = 0; k < 4; k++)
+        if (!c.ev[k]) CK(cudaEventCreate(&c.ev[k]));
+    CK(cudaEventRecord(c.ev[2], c.stream));
+    long long total = 0;
+    for (int k = 0; k < kNumClasses; k++) total += cnt[k];
     for (int k = 0; k < kNumClasses; k++) {
         if (cnt[k] == 0) continue;
         int block = 128;
@@ -546,7 +553,12 @@ static int grad_build(Context& c)
                                 "the gradient", kClassL[k][0], kClassL[k][1], kClassL[k][2], kClassL[k][3]), 5;
     }
     CK(cudaGetLastError());
+    CK(cudaEventRecord(c.ev[3], c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c.ev[2], c.ev[3]));
+    c.last_ms_grad = ms;
+    c.last_grad_quartets = total;
     return 0;
 }
 
@@ -1002,6 +1014,14 @@ int qb_xc_functional(int method, int n, const double* rho, const double* sigma, 
     s.release();
     o.release();
     return rc;
+}
+
+int qb_last_grad_stats(long long* quartets, double* ms)
+{
+    Context& c = ctx();
+    *quartets = c.last_grad_quartets;
+    *ms = c.last_ms_grad;
+    return 0;
 }
 
 int qb_set_mixed_precision(double cut)

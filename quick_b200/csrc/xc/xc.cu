@@ -42,6 +42,7 @@
 #include <numeric>
 #include <vector>
 
+#include "../../include/quick_b200.h"
 #include "gen/xc_tables.h"
 #include "qb_internal.h"
 #include "xc/xc_api.h"
@@ -421,6 +422,13 @@ struct XcState {
     // work
     XcBuf<double> d_B, d_Psi, d_T0, d_S, d_L, d_U, d_M, d_e, d_n, d_sum;
     cublasHandle_t blas = nullptr;
+    XcBuf<unsigned char> d_blas_ws;   // cuBLAS workspace (no allocation inside a capture)
+    cudaGraphExec_t graph_exec = nullptr;
+    const double* graph_dense = nullptr;
+    double* graph_v = nullptr;
+    int graph_method = 0;
+    bool graph_failed = false;
+    unsigned long long graph_launches = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -729,25 +737,10 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
     return 0;
 }
 
-int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResult* out)
+// Everything one quadrature enqueues on the stream after the grid exists.
+static int xc_enqueue(XcState& S, const XcInputs& in, const double* d_dense, double* d_v, cudaStream_t st)
 {
-    XcState& S = xc_state();
-    cudaStream_t st = in.stream;
-    if (in.method != 1 && in.method != 2)
-        return xc_fail(1, "gpu_getxc_: method %d has no XC functional (1 = B3LYP, 2 = BLYP)", in.method);
-    if (!S.ev[0])
-        for (auto& e : S.ev) XCK(cudaEventCreate(&e));
-    if (!S.blas) XBL(cublasCreate(&S.blas));
-    XBL(cublasSetStream(S.blas, st));
-    out->ms_grid = 0.0;
-    bool same = S.valid && S.geom_version == in.geom_version && S.nbasis == in.nbasis &&
-                std::equal(S.sigrad2.begin(), S.sigrad2.end(), in.sigrad2);
-    if (!same) {
-        S.valid = false;
-        if (int rc = xc_build_grid(S, in, &out->ms_grid)) return rc;
-    }
     const int n = in.nbasis;
-    XCK(cudaEventRecord(S.ev[0], st));
     XCK(cudaMemsetAsync(S.d_e.p, 0, std::max<long long>(S.npts, 1) * sizeof(double), st));
     XCK(cudaMemsetAsync(S.d_n.p, 0, std::max<long long>(S.npts, 1) * sizeof(double), st));
     XcBasisParams bp{S.d_center.p, S.d_itype.p, S.d_aexp.p, S.d_dcoeff.p, in.maxcontract};
@@ -780,6 +773,64 @@ int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResu
     xc_reduce_kernel<<<1, 1024, 0, st>>>(S.d_e.p, S.d_n.p, S.npts, S.d_sum.p);
     ++g_launches;
     XCK(cudaGetLastError());
+    return 0;
+}
+
+int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResult* out)
+{
+    XcState& S = xc_state();
+    cudaStream_t st = in.stream;
+    if (in.method != 1 && in.method != 2)
+        return xc_fail(1, "gpu_getxc_: method %d has no XC functional (1 = B3LYP, 2 = BLYP)", in.method);
+    if (!S.ev[0])
+        for (auto& e : S.ev) XCK(cudaEventCreate(&e));
+    if (!S.blas) {
+        XBL(cublasCreate(&S.blas));
+        XCK(S.d_blas_ws.alloc((size_t)32 << 20));
+        XBL(cublasSetWorkspace(S.blas, S.d_blas_ws.p, (size_t)32 << 20));
+    }
+    XBL(cublasSetStream(S.blas, st));
+    out->ms_grid = 0.0;
+    bool same = S.valid && S.geom_version == in.geom_version && S.nbasis == in.nbasis &&
+                std::equal(S.sigrad2.begin(), S.sigrad2.end(), in.sigrad2);
+    if (!same) {
+        S.valid = false;
+        if (S.graph_exec) cudaGraphExecDestroy(S.graph_exec), S.graph_exec = nullptr;
+        if (int rc = xc_build_grid(S, in, &out->ms_grid)) return rc;
+    }
+    XCK(cudaEventRecord(S.ev[0], st));
+    // the per-call sequence (about 6 launches per chunk) replays from a CUDA
+    // graph captured on the first call for these buffers; the legacy
+    // default stream cannot be captured, so it enqueues directly
+    const bool use_graph = st != nullptr && !S.graph_failed;
+    if (use_graph && !(S.graph_exec && S.graph_dense == d_dense && S.graph_v == d_v && S.graph_method == in.method)) {
+        if (S.graph_exec) cudaGraphExecDestroy(S.graph_exec), S.graph_exec = nullptr;
+        const unsigned long long l0 = g_launches;
+        cudaGraph_t graph = nullptr;
+        bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        int rc = ok ? xc_enqueue(S, in, d_dense, d_v, st) : 0;
+        ok = (cudaStreamEndCapture(st, &graph) == cudaSuccess) && ok && rc == 0 && graph != nullptr;
+        if (ok) ok = cudaGraphInstantiate(&S.graph_exec, graph, 0) == cudaSuccess;
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();   // a refused capture leaves no sticky error
+        if (!ok) {
+            S.graph_exec = nullptr;
+            S.graph_failed = true;
+            qb_clear_error();   // a refused capture is not an error: the direct path runs instead
+        } else {
+            S.graph_launches = g_launches - l0;
+            g_launches = l0;
+            S.graph_dense = d_dense;
+            S.graph_v = d_v;
+            S.graph_method = in.method;
+        }
+    }
+    if (use_graph && S.graph_exec) {
+        XCK(cudaGraphLaunch(S.graph_exec, st));
+        g_launches += S.graph_launches;
+    } else {
+        if (int rc = xc_enqueue(S, in, d_dense, d_v, st)) return rc;
+    }
     XCK(cudaEventRecord(S.ev[1], st));
     double sums[2];
     XCK(cudaMemcpyAsync(sums, S.d_sum.p, sizeof sums, cudaMemcpyDeviceToHost, st));
@@ -824,6 +875,8 @@ void xc_release()
     S.d_funcs.release(); S.d_B.release(); S.d_Psi.release(); S.d_T0.release(); S.d_S.release(); S.d_L.release();
     S.d_U.release(); S.d_M.release();
     S.d_e.release(); S.d_n.release(); S.d_sum.release();
+    if (S.graph_exec) cudaGraphExecDestroy(S.graph_exec), S.graph_exec = nullptr;
+    S.graph_failed = false;
     S.valid = false;
 }
 
