@@ -26,14 +26,16 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 
 
 def _extra_flags(src):
-    """Per-file ptxas options.  For the generated classes with total angular
-    momentum >= 6, ptxas at its default -O3 falls back to a 32-register
-    allocation that spills nearly everything; -O1 keeps 255 registers and
-    spills about a quarter as much (measured with -Xptxas -v)."""
+    """Per-file ptxas options.  For the generated Fock classes with total
+    angular momentum >= 6, and the gradient classes with total angular
+    momentum >= 4, ptxas at its default -O3 falls back to a 32-register
+    allocation that spills nearly everything (grad_2110: 32 registers and a
+    10.5 KB stack frame); -O1 keeps 255 registers and spills about a third as
+    much (measured with -Xptxas -v for every class)."""
     b = os.path.basename(src)
-    for pre in ("eri_", "eri32_", "grad_"):
+    for pre, lim in (("eri_", 6), ("eri32_", 6), ("grad_", 4)):
         if b.startswith(pre) and b[len(pre):len(pre) + 4].isdigit():
-            if sum(int(ch) for ch in b[len(pre):len(pre) + 4]) + (1 if pre == "grad_" else 0) >= 6:
+            if sum(int(ch) for ch in b[len(pre):len(pre) + 4]) >= lim:
                 return ["-Xptxas", "-O1"]
     return []
 

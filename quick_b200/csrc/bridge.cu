@@ -537,7 +537,8 @@ static int grad_build(Context& c)
     CK(c.d_grad.alloc(3 * (size_t)c.natom));
     CK(cudaMemsetAsync(c.d_grad.p, 0, 3 * (size_t)c.natom * sizeof(double), c.stream));
     FockParams P = fock_params(c);
-    GradExtra G{c.d_shell_atom.p, c.d_pair_sh.p, c.d_grad.p};
+    // per-block shared accumulation while 3 natom doubles fit the default 48 KB
+    GradExtra G{c.d_shell_atom.p, c.d_pair_sh.p, c.d_grad.p, c.natom, 3 * c.natom * 8 <= 48 * 1024 ? 1 : 0};
     for (int k = 0; k < 4; k++)
         if (!c.ev[k]) CK(cudaEventCreate(&c.ev[k]));
     CK(cudaEventRecord(c.ev[2], c.stream));

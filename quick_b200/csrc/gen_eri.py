@@ -497,7 +497,7 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     w("void launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int grid, int block, cudaStream_t st)" % tag)
     w("{")
     w("    auto kern = grad_class_kernel<%d, %d, %d, %d, %d>;" % (la, lb, lc, ld, part))
-    w("    QB_LAUNCH(kern, grid, block, 0, st, P, G, cls);")
+    w("    QB_LAUNCH(kern, grid, block, grad_smem(G), st, P, G, cls);")
     w("}")
     w("}  // namespace qb")
     return "\n".join(o) + "\n", dict(vrr_flops=vrr.nflops, hrr_flops=sum(h.nflops for h in hrrs.values()),
