@@ -546,10 +546,8 @@ static int grad_build(Context& c)
     for (int k = 0; k < kNumClasses; k++) total += cnt[k];
     for (int k = 0; k < kNumClasses; k++) {
         if (cnt[k] == 0) continue;
-        int block = 128;
-        long long warps = (cnt[k] + 31) / 32;
-        long long grid = std::min<long long>((warps * 32 + block - 1) / block, (long long)c.nsm * 16);
-        if (launch_grad_class(k, P, G, (int)std::max<long long>(grid, 1), block, c.stream) < 0)
+        const int GS = std::min(c.class_group.empty() ? 1 : std::max(c.class_group[k], 1), grad_max_group(k));
+        if (launch_grad_class(k, P, G, GS, cnt[k], c.nsm, c.stream) < 0)
             return set_error(5, "gpu_grad_: no gradient kernel for class (%d%d|%d%d): f shells are not built for "
                                 "the gradient", kClassL[k][0], kClassL[k][1], kClassL[k][2], kClassL[k][3]), 5;
     }

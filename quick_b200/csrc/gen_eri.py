@@ -169,6 +169,17 @@ class HRR:
         return name
 
 
+# gradient classes with total angular momentum >= this get one kernel per
+# derivative centre (two accumulator sets each instead of four)
+GRAD_SPLIT_L = int(os.environ.get("QB_GRAD_SPLIT_L", "4"))
+
+
+def grad_group_sizes(la, lb, lc, ld):
+    """Lanes per shell quartet compiled for a gradient class: sub-warp
+    groups for the light classes (their cost is the primitive loop)."""
+    return [1, 2, 4, 8] if la + lb + lc + ld <= 2 else [1]
+
+
 def group_sizes(la, lb, lc, ld):
     """Lanes per shell quartet compiled for a class: the light classes, whose
     cost is the primitive loop, get sub-warp groups up to a whole warp; the
@@ -426,18 +437,23 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     w('#include "eri_common.cuh"')
     w('#include "grad_common.cuh"')
     w("namespace qb {")
-    w("template <> __device__ __forceinline__ void grad_class<%d, %d, %d, %d, %d>(const QuartetCtx& q, const FockParams& P, const GradExtra& G)" % (la, lb, lc, ld, part))
+    w("template <> struct GradEval<%d, %d, %d, %d, %d> {" % (la, lb, lc, ld, part))
+    w("template <int GS>")
+    w("__device__ __forceinline__ static void run(const QuartetCtx& q, const FockParams& P, const GradExtra& G, int sub)")
     w("{")
     w("    constexpr int L = %d;" % L)
     for k, lst in acc.items():
         for e, f, _ in lst:
             w("    double %s_%s_%s = 0.0;" % (k, nm(e), nm(f)))
-    w("    for (int ib = 0; ib < q.nbra; ib++) {")
+    # GS lanes per quartet stride over the flattened primitive quartets
+    w("    const int nk = q.nket, npq = q.nbra * nk;")
+    w("    for (int t = (GS == 1 ? 0 : sub); t < npq; t += GS) {")
+    w("        const int ib = t / nk, ik = t - ib * nk;")
     w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
     w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
     w("        const double a2 = 2.0 * xb.y;")
     w("        const double b2 = 2.0 * pb.p - a2;")
-    w("        for (int ik = 0; ik < q.nket; ik++) {")
+    w("        {")
     w("            const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
     w("            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
     w("            const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
@@ -461,6 +477,13 @@ def gen_grad_class(la, lb, lc, ld, part=0):
             w("            %s_%s_%s += %s%s;" % (k, nm(e), nm(f), wt[k], v))
     w("        }")
     w("    }")
+    w("    if constexpr (GS > 1) {")
+    for k, lst in acc.items():
+        for e, f, _ in lst:
+            w("        %s_%s_%s = group_sum<GS>(%s_%s_%s);" % (k, nm(e), nm(f), k, nm(e), nm(f)))
+    w("    }")
+    w("    QuartetCtx qa = q;")
+    w("    qa.active = q.active && sub == 0;   // the group's first lane digests")
     w("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
     w("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
     for h in hrrs.values():
@@ -492,12 +515,20 @@ def gen_grad_class(la, lb, lc, ld, part=0):
                         da, db, dc = deriv[(ia, ib, ic, id_, i)]
                         w("        gA[%d] += g*(%s); gB[%d] += g*(%s); gC[%d] += g*(%s);" % (i, da, i, db, i, dc))
                     w("    }")
-    w("    grad_digest<%d>(q, G, gA, gB, gC);" % part)
+    w("    grad_digest<%d>(qa, G, gA, gB, gC);" % part)
     w("}")
-    w("void launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int grid, int block, cudaStream_t st)" % tag)
+    w("};")
+    gs = grad_group_sizes(la, lb, lc, ld)
+    w("// lanes per shell quartet compiled for this class: %s" % ", ".join(str(x) for x in gs))
+    w("int launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int GS, int nq, int nsm, cudaStream_t st)" % tag)
     w("{")
-    w("    auto kern = grad_class_kernel<%d, %d, %d, %d, %d>;" % (la, lb, lc, ld, part))
-    w("    QB_LAUNCH(kern, grid, block, grad_smem(G), st, P, G, cls);")
+    w("    switch (GS) {")
+    for x in gs:
+        w("    case %d: { auto kern = grad_class_kernel<%d, %d, %d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, %d, nsm), 128, grad_smem(G), st, P, G, cls); return %d; }"
+          % (x, la, lb, lc, ld, part, x, x, x))
+    w("    default: { auto kern = grad_class_kernel<%d, %d, %d, %d, %d, 1>; QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, grad_smem(G), st, P, G, cls); return 1; }"
+      % (la, lb, lc, ld, part))
+    w("    }")
     w("}")
     w("}  // namespace qb")
     return "\n".join(o) + "\n", dict(vrr_flops=vrr.nflops, hrr_flops=sum(h.nflops for h in hrrs.values()),
@@ -706,26 +737,32 @@ def main(outdir, lmax=2, lmax_all=3):
     gstats = {}
     parts = {}
     for c in cls_grad:
-        # classes with total angular momentum >= 7 get one kernel per
-        # derivative centre (A, B, C): a third of the code each, which keeps
-        # the compile time of the largest classes in minutes
-        parts[c] = [0] if sum(c) < 7 else [1, 2, 3]
+        # classes with total angular momentum >= GRAD_SPLIT_L get one kernel
+        # per derivative centre (A, B, C): a third of the code and half the
+        # accumulators each, which keeps the compile time of the largest
+        # classes in minutes and their register spills down
+        parts[c] = [0] if sum(c) < GRAD_SPLIT_L else [1, 2, 3]
         for pt in parts[c]:
             src, st_ = gen_grad_class(*c, part=pt)
             tg = "%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1])
             gstats[tg] = st_
             write_if_changed(os.path.join(outdir, "grad_%s.cu" % tg), src)
-            gl.append("void launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int grid, int block, cudaStream_t st);" % tg)
+            gl.append("int launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int GS, int nq, int nsm, cudaStream_t st);" % tg)
     gl += ["// returns 0, or -1 for a class without a gradient kernel (f shells)",
-           "int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int grid, int block, cudaStream_t st)",
+           "int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int GS, int nq, int nsm, cudaStream_t st)",
            "{", "    switch (cls) {"]
     for k, c in enumerate(cls_all):
         if c not in parts:
             continue
-        calls = " ".join("launch_grad_%s(P, G, %d, grid, block, st);" % ("%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1]), k)
+        calls = " ".join("launch_grad_%s(P, G, %d, GS, nq, nsm, st);" % ("%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1]), k)
                          for pt in parts[c])
         gl.append("    case %d: %s return 0;" % (k, calls))
-    gl += ["    default: return -1;", "    }", "}", "}  // namespace qb"]
+    gl += ["    default: return -1;", "    }", "}"]
+    gl += ["int grad_max_group(int cls)", "{", "    switch (cls) {"]
+    for k, c in enumerate(cls_all):
+        if c in parts:
+            gl.append("    case %d: return %d;" % (k, max(grad_group_sizes(*c))))
+    gl += ["    default: return 1;", "    }", "}", "}  // namespace qb"]
     write_if_changed(os.path.join(outdir, "grad_launch.cu"), "\n".join(gl) + "\n")
     write_if_changed(os.path.join(outdir, "grad_flops.json"), json.dumps(gstats, indent=1))
     # Schwarz kernels, one per pair type
