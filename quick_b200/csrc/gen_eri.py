@@ -175,9 +175,10 @@ GRAD_SPLIT_L = int(os.environ.get("QB_GRAD_SPLIT_L", "4"))
 
 
 def grad_group_sizes(la, lb, lc, ld):
-    """Lanes per shell quartet compiled for a gradient class: sub-warp
-    groups for the light classes (their cost is the primitive loop)."""
-    return [1, 2, 4, 8] if la + lb + lc + ld <= 2 else [1]
+    """Lanes per shell quartet compiled for a gradient class.  One: measured
+    on (H2O)32/6-31G**, groups of 2-4 lanes for the light classes made the
+    gradient 6% slower (274 vs 259 ms)."""
+    return [1]
 
 
 def group_sizes(la, lb, lc, ld):
@@ -765,6 +766,10 @@ def main(outdir, lmax=2, lmax_all=3):
     gl += ["    default: return 1;", "    }", "}", "}  // namespace qb"]
     write_if_changed(os.path.join(outdir, "grad_launch.cu"), "\n".join(gl) + "\n")
     write_if_changed(os.path.join(outdir, "grad_flops.json"), json.dumps(gstats, indent=1))
+    # per-centre files left over from a build with another split threshold
+    for f in os.listdir(outdir):
+        if f.startswith("grad_") and f.endswith(".cu") and f != "grad_launch.cu" and f[5:-3] not in gstats:
+            os.remove(os.path.join(outdir, f))
     # Schwarz kernels, one per pair type
     st = ['#include "eri_common.cuh"', '#include "schwarz.cuh"', '#include "eri_classes.h"', "namespace qb {"]
     for t in pair_types(lmax):
