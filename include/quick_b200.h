@@ -169,6 +169,30 @@ long long qb_xc_grid(double* xyzw, long long cap);
    out[3k+1] = df/drho, out[3k+2] = 4 df/dsigma (QUICK's b3lyp_e / b3lypf and becke/lyp). */
 int qb_xc_functional(int method, int n, const double* rho, const double* sigma, double* out);
 
+/* One-electron integrals.  QUICK forms these on the host in Fortran; these entry points follow
+   the gpu_* conventions (arguments by pointer, Fortran column-major nbasis^2 matrices) and use
+   the uploaded basis, coordinates and charges (gpu_upload_xyz_, gpu_upload_atom_and_chg_,
+   gpu_upload_basis_).
+   gpu_get1e_: o = H = T + V, the core Hamiltonian of get1e
+     (src/quick_one_electron_integral.f90:1699-1809: kinetic part get1eO :1633-1673 with
+     dcoeff/aexp, attraction attrashell :1816-1925 / nuclearattra src/nuclear.f90:198-221 with
+     gccoeff x cons), full symmetric matrix.
+   gpu_get_overlap_: s = S, the overlap matrix of fullx (:31-46).
+   qb_oneint_device: both at once into device arrays (either may be null), asynchronous on the
+     library stream. */
+int gpu_get1e_(double* o);
+int gpu_get_overlap_(double* s);
+int qb_oneint_device(double* d_S, double* d_H);
+
+/* One-electron and nuclear-repulsion parts of the RHF nuclear gradient (hfgrad,
+   src/gradient.f90:49-249): adds to grad (3 x natom, Fortran order) the nuclear repulsion
+   term, -2 W dS and 2 D dT over basis-function pairs on different atoms and D dV for the
+   nuclear attraction (attrashellopt, src/shell.f90:1747-1830), for the total density D and the
+   energy-weighted density W = 2 sum_occ e_k C_k C_k^T (gradient.f90:84-96), both nbasis^2.
+   qb_grad1e_device takes device pointers and is asynchronous on the library stream. */
+int gpu_grad1e_(double* grad, const double* dense, const double* wdense);
+int qb_grad1e_device(const double* d_dense, const double* d_wdense, double* d_grad);
+
 /* Measured FMA throughput of this GPU in GFLOP/s (FP64 if fp64 != 0, else FP32): a
    register-resident FMA chain over 8 blocks per SM, best of 4 timed runs. */
 int qb_fma_peak(int fp64, double* gflops);

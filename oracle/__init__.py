@@ -170,6 +170,74 @@ _ref_spdf = None
 _ref_variants = {}
 
 
+class _O1Basis(C.Structure):
+    _fields_ = [("natom", C.c_int), ("nbasis", C.c_int), ("nshell", C.c_int), ("maxcontract", C.c_int),
+                ("xyz", _P), ("chg", _P), ("ncontract", _P), ("itype", _P), ("ncenter", _P),
+                ("aexp", _P), ("dcoeff", _P), ("katom", _P), ("kprim", _P), ("Ksumtype", _P),
+                ("Qstart", _P), ("Qfinal", _P), ("Qsbasis", _P), ("Qfbasis", _P), ("KLMN", _P),
+                ("gccoeff", _P), ("gcexpo", _P), ("cons", _P)]
+
+
+class OneElectronInputs:
+    """The arrays oracle_1e.c reads (QUICK's per-function and per-shell basis
+    arrays, coordinates and nuclear charges), kept alive behind the struct."""
+
+    def __init__(self, basis, mol):
+        b = basis
+        I32 = np.int32
+        self.keep = dict(
+            xyz=np.asfortranarray(mol.xyz_bohr, dtype=np.float64),
+            chg=np.ascontiguousarray(mol.atomic_numbers, dtype=np.float64),
+            ncontract=np.ascontiguousarray(b.ncontract, dtype=I32),
+            itype=np.asfortranarray(b.itype, dtype=I32),
+            ncenter=np.ascontiguousarray(b.ncenter, dtype=I32),
+            aexp=np.asfortranarray(b.aexp, dtype=np.float64),
+            dcoeff=np.asfortranarray(b.dcoeff, dtype=np.float64),
+            katom=np.ascontiguousarray(b.katom, dtype=I32),
+            kprim=np.ascontiguousarray(b.kprim, dtype=I32),
+            Ksumtype=np.ascontiguousarray(b.Ksumtype, dtype=I32),
+            Qstart=np.ascontiguousarray(b.Qstart, dtype=I32),
+            Qfinal=np.ascontiguousarray(b.Qfinal, dtype=I32),
+            Qsbasis=np.asfortranarray(b.Qsbasis, dtype=I32),
+            Qfbasis=np.asfortranarray(b.Qfbasis, dtype=I32),
+            KLMN=np.asfortranarray(b.KLMN, dtype=I32),
+            gccoeff=np.asfortranarray(b.gccoeff),
+            gcexpo=np.asfortranarray(b.gcexpo),
+            cons=np.ascontiguousarray(b.cons))
+        k = self.keep
+        self.s = _O1Basis(mol.natom, b.nbasis, b.nshell, b.maxcontract, *[_ptr(k[n]) for n in (
+            "xyz", "chg", "ncontract", "itype", "ncenter", "aexp", "dcoeff", "katom", "kprim", "Ksumtype",
+            "Qstart", "Qfinal", "Qsbasis", "Qfbasis", "KLMN", "gccoeff", "gcexpo", "cons")])
+
+
+def oneint(basis, mol):
+    """Overlap S and core Hamiltonian H = T + V (nbasis x nbasis, symmetric)."""
+    inp = OneElectronInputs(basis, mol)
+    n = basis.nbasis
+    S = np.zeros((n, n), order="F")
+    H = np.zeros((n, n), order="F")
+    lib().oracle_oneint(C.byref(inp.s), _ptr(S), _ptr(H))
+    return S, H
+
+
+def enuc(mol):
+    xyz = np.asfortranarray(mol.xyz_bohr, dtype=np.float64)
+    chg = np.ascontiguousarray(mol.atomic_numbers, dtype=np.float64)
+    f = lib().oracle_enuc
+    f.restype = C.c_double
+    return float(f(C.c_int(mol.natom), _ptr(xyz), _ptr(chg)))
+
+
+def grad1e(basis, mol, dense, wdense):
+    """Nuclear-repulsion and one-electron parts of the RHF gradient, (3 natom)."""
+    inp = OneElectronInputs(basis, mol)
+    g = np.zeros(3 * mol.natom)
+    d = np.asfortranarray(dense, dtype=np.float64)
+    w = np.asfortranarray(wdense, dtype=np.float64)
+    lib().oracle_grad1e(C.byref(inp.s), _ptr(d), _ptr(w), _ptr(g))
+    return g
+
+
 def _ref_dir(spdf):
     """spdf: False (default build), True (CUDA_SPDF: QUICK's f-shell kernels)
     or "boys" (CUDA_SPDF with QUICK's FmT replaced by an accurate Boys

@@ -144,6 +144,27 @@ class Session:
         check()
         return g
 
+    def oneint(self):
+        """(S, H): the overlap of fullx and the core Hamiltonian of get1e."""
+        n = self.nbasis
+        S = np.zeros((n, n), order="F")
+        H = np.zeros((n, n), order="F")
+        r = lib()
+        r.gpu_get_overlap_(_ptr(S))
+        r.gpu_get1e_(_ptr(H))
+        check()
+        return S, H
+
+    def grad1e(self, dense, wdense, grad_in=None):
+        """grad_in + nuclear-repulsion and one-electron gradient (3 natom)."""
+        na = len(self.basis.first_basis_function)
+        g = np.zeros(3 * na) if grad_in is None else np.array(grad_in, dtype=np.float64).ravel(order="F").copy()
+        d = np.asfortranarray(dense, dtype=np.float64)
+        w = np.asfortranarray(wdense, dtype=np.float64)
+        lib().gpu_grad1e_(_ptr(g), _ptr(d), _ptr(w))
+        check()
+        return g
+
     def getxc(self, O, dense, sigrad2, method=1, isg=1, Eelxc=0.0, aelec=0.0, belec=0.0):
         """QUICK's DFT step (src/dft.f90:893-899): upload_method / calculated +
         gpu_getxc_.  Returns (O + V_xc symmetrised, Eelxc, aelec, belec), the

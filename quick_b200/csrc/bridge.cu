@@ -21,6 +21,7 @@
 #include "../../include/quick_b200.h"
 #include "gen/eri_classes.h"
 #include "qb_internal.h"
+#include "oneint.h"
 #include "schwarz.cuh"
 #include "grad_common.cuh"
 #include "xc/xc_api.h"
@@ -90,6 +91,7 @@ struct Context {
     DevBuf<long long> d_class_offset, d_class_end;
     DevBuf<int2> d_quartets;
     DevBuf<int2> d_ket_segs;             // constant primitive-count segments of the pair table
+    DevBuf<double> d_S1, d_H1, d_D1, d_W1, d_g1;   // host-pointer one-electron entry points
     std::vector<ScreenClass> screen_cls;
     std::vector<int> class_group;        // lanes per shell quartet of each class kernel
     int generic_min_l = 99;              // classes with L sum >= this run the generic kernel (QB_GENERIC_MIN_L)
@@ -737,6 +739,12 @@ void gpu_shutdown_(void)
     for (auto& e : c.ev)
         if (e) cudaEventDestroy(e), e = nullptr;
     xc_release();
+    oneint_release();
+    c.d_S1.release();
+    c.d_H1.release();
+    c.d_D1.release();
+    c.d_W1.release();
+    c.d_g1.release();
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
     delete g;
     g = nullptr;
@@ -798,6 +806,7 @@ void gpu_upload_atom_and_chg_(int* atom, double* atom_chg)
     Context& c = ctx();
     c.iattype.assign(atom, atom + c.natom);
     c.chg.assign(atom_chg, atom_chg + c.natom);
+    c.geom_version = ++g_geom_counter;
 }
 
 void gpu_upload_basis_(int* nshell, int* nprim, int* jshell, int* jbasis, int* maxcontract, int* ncontract, int* itype,
@@ -969,6 +978,93 @@ int qb_xc_device(const double* d_dense, const double* sigrad2, double* d_vxc, do
     c.last_xc = r;
     *exc = r.exc;
     *nalpha = r.nalpha;
+    return 0;
+}
+
+static OneIntHost oneint_host(const Context& c)
+{
+    OneIntHost h{};
+    h.natom = c.natom;
+    h.nbasis = c.nbasis;
+    h.nshell = c.nshell;
+    h.maxcontract = c.maxcontract;
+    h.xyz = c.xyz.data();
+    h.chg = c.chg.data();
+    h.kprim = c.kprim.data();
+    h.katom = c.katom.data();
+    h.Ksumtype = c.Ksumtype.data();
+    h.Qstart = c.Qstart.data();
+    h.Qfinal = c.Qfinal.data();
+    h.Qsbasis = c.Qsbasis.data();
+    h.itype = c.itype.data();
+    h.KLMN = c.KLMN.data();
+    h.aexp = c.aexp.data();
+    h.dcoeff = c.dcoeff.data();
+    h.gccoeff = c.gccoeff.data();
+    h.gcexpo = c.gcexpo.data();
+    h.cons = c.cons.data();
+    h.d_boys = c.d_boys.p;
+    h.geom_version = c.geom_version;
+    h.nsm = c.nsm;
+    h.stream = c.stream;
+    return h;
+}
+
+static int oneint_ready(const Context& c, const char* who)
+{
+    char msg[160];
+    snprintf(msg, sizeof msg, "basis, coordinates and charges must be uploaded before %s", who);
+    return require(c.inited && c.have_basis && (int)c.xyz.size() == 3 * c.natom && (int)c.chg.size() == c.natom, msg);
+}
+
+int qb_oneint_device(double* d_S, double* d_H)
+{
+    Context& c = ctx();
+    if (oneint_ready(c, "qb_oneint_device")) return 1;
+    return oneint_run(oneint_host(c), d_S, d_H);
+}
+
+int qb_grad1e_device(const double* d_dense, const double* d_wdense, double* d_grad)
+{
+    Context& c = ctx();
+    if (oneint_ready(c, "qb_grad1e_device")) return 1;
+    return grad1e_run(oneint_host(c), d_dense, d_wdense, d_grad);
+}
+
+// Host-pointer forms: the matrices of fullx (S, quick_one_electron_integral.f90:31-46)
+// and get1e (H = T + V, :1699-1809).
+static int oneint_host_call(double* S, double* H, const char* who)
+{
+    Context& c = ctx();
+    if (oneint_ready(c, who)) return 1;
+    const size_t nn = (size_t)c.nbasis * c.nbasis;
+    if (S) CK(c.d_S1.alloc(nn));
+    if (H) CK(c.d_H1.alloc(nn));
+    if (int rc = oneint_run(oneint_host(c), S ? c.d_S1.p : nullptr, H ? c.d_H1.p : nullptr)) return rc;
+    if (S) CK(cudaMemcpyAsync(S, c.d_S1.p, nn * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    if (H) CK(cudaMemcpyAsync(H, c.d_H1.p, nn * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return 0;
+}
+
+int gpu_get1e_(double* o) { return oneint_host_call(nullptr, o, "gpu_get1e_"); }
+
+int gpu_get_overlap_(double* s) { return oneint_host_call(s, nullptr, "gpu_get_overlap_"); }
+
+int gpu_grad1e_(double* grad, const double* dense, const double* wdense)
+{
+    Context& c = ctx();
+    if (oneint_ready(c, "gpu_grad1e_")) return 1;
+    const size_t nn = (size_t)c.nbasis * c.nbasis, ng = 3 * (size_t)c.natom;
+    CK(c.d_D1.alloc(nn));
+    CK(c.d_W1.alloc(nn));
+    CK(c.d_g1.alloc(ng));
+    CK(cudaMemcpyAsync(c.d_D1.p, dense, nn * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.d_W1.p, wdense, nn * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.d_g1.p, grad, ng * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    if (int rc = grad1e_run(oneint_host(c), c.d_D1.p, c.d_W1.p, c.d_g1.p)) return rc;
+    CK(cudaMemcpyAsync(grad, c.d_g1.p, ng * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
     return 0;
 }
 
