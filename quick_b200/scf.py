@@ -76,11 +76,34 @@ def _density(C, nocc):
     return 2.0 * Co @ Co.T
 
 
+def aufbau_occupations(eps, nelec, tol=1e-4):
+    """Occupation numbers for ``nelec`` electrons over orbital energies
+    ``eps`` (ascending): two per orbital, the last partly filled degenerate
+    set (energies within ``tol``) shared equally, which keeps an atom's
+    density spherical."""
+    occ = np.zeros(len(eps))
+    left = float(nelec)
+    i = 0
+    while left > 1e-12 and i < len(eps):
+        j = i
+        while j + 1 < len(eps) and eps[j + 1] - eps[i] < tol:
+            j += 1
+        g = j - i + 1
+        put = min(left, 2.0 * g)
+        occ[i:j + 1] = put / g
+        left -= put
+        i = j + 1
+    return occ
+
+
 def rhf(engine, nocc, conv=1e-8, max_iter=100, diis_size=10, incremental=False, rebuild_every=8,
-        D0=None, callback=None):
+        D0=None, callback=None, fractional=False):
     """Restricted closed-shell HF.  Converged when the RMS change of the
     density is below ``conv`` and its largest change below 100 ``conv``
-    (electdiis's test, src/scf.f90:594)."""
+    (electdiis's test, src/scf.f90:594).  With ``fractional`` the 2 ``nocc``
+    electrons are spread over degenerate orbitals (aufbau_occupations): the
+    spherically averaged atoms of the superposition-of-atomic-densities
+    guess."""
     t_start = time.perf_counter()
     S, H = engine.overlap_core()
     enuc = engine.enuc()
@@ -90,9 +113,14 @@ def rhf(engine, nocc, conv=1e-8, max_iter=100, diis_size=10, incremental=False, 
         e, Cp = np.linalg.eigh(X.T @ F @ X)
         return e, X @ Cp
 
+    def density(eps, C):
+        if fractional:
+            return (C * aufbau_occupations(eps, 2 * nocc)) @ C.T
+        return _density(C, nocc)
+
     if D0 is None:
         eps, C = diag(H)
-        D = _density(C, nocc)
+        D = density(eps, C)
     else:
         D = np.array(D0)
     fock_s = 0.0
@@ -135,7 +163,7 @@ def rhf(engine, nocc, conv=1e-8, max_iter=100, diis_size=10, incremental=False, 
             except np.linalg.LinAlgError:
                 Fx = F
         eps, C = diag(Fx)
-        D_new = _density(C, nocc)
+        D_new = density(eps, C)
         dD = D_new - D
         drms = float(np.sqrt(np.mean(dD * dD)))
         dmax = float(np.abs(dD).max())
@@ -152,6 +180,21 @@ def rhf(engine, nocc, conv=1e-8, max_iter=100, diis_size=10, incremental=False, 
     return SCFResult(energy=e_elec + enuc, e_elec=e_elec, e_nuc=enuc, converged=converged, iterations=it,
                      D=D_built, C=C, eps=eps, nocc=nocc, history=history, fock_seconds=fock_s,
                      seconds=time.perf_counter() - t_start)
+
+
+def sad_guess(mol, basis, atom_density):
+    """Superposition of atomic densities (QUICK's default guess, getmolsad in
+    src/getMolSad.f90): the block-diagonal density with each atom's block
+    from ``atom_density(symbol)`` (nbf_atom x nbf_atom, the atom alone in the
+    same basis), computed once per element."""
+    D = np.zeros((basis.nbasis, basis.nbasis))
+    cache = {}
+    for i, sym in enumerate(mol.symbols):
+        if sym not in cache:
+            cache[sym] = atom_density(sym)
+        f, l = basis.first_basis_function[i] - 1, basis.last_basis_function[i]
+        D[f:l, f:l] = cache[sym]
+    return D
 
 
 class GpuEngine:
@@ -183,3 +226,45 @@ class GpuEngine:
     def gradient(self, D, W):
         g = self.s.grad1e(D, W)
         return self.s.grad(g, D, shell_cut_matrix(self.basis, D), self.grad_cut, self.plim)
+
+
+def gpu_atom_density(symbol, basis_name, device=0, conv=1e-7):
+    """Spherically averaged atomic density on the GPU (fractional-occupation
+    SCF of the atom alone); opens and closes its own session."""
+    from .basis import build_basis
+    from .capi import Session
+    from .molecule import Molecule
+    m = Molecule([symbol], np.zeros((1, 3)))
+    b = build_basis(m.symbols, basis_name)
+    s = Session(device)
+    try:
+        s.upload_molecule(m, b)
+        r = rhf(GpuEngine(s, m, b, 1e-12, 1e-20), m.n_electrons / 2.0, conv=conv, max_iter=60, fractional=True)
+    finally:
+        s.close()
+    return r.D
+
+
+def run_rhf_gpu(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1e-8, gradient=False,
+                mixed_cut=0.0, incremental=False, device=0, max_iter=100):
+    """Energy (and gradient) of a closed-shell molecule on the GPU: the SAD
+    guess, the DIIS SCF over the GPU Fock build, and the analytic gradient.
+    Returns (SCFResult, gradient or None)."""
+    from .basis import build_basis
+    from .capi import Session
+    b = build_basis(mol.symbols, basis_name)
+    t0 = time.perf_counter()
+    D0 = sad_guess(mol, b, lambda sym: gpu_atom_density(sym, basis_name, device))
+    t_guess = time.perf_counter() - t0
+    s = Session(device)
+    try:
+        s.upload_molecule(mol, b)
+        if mixed_cut:
+            s.set_mixed_precision(mixed_cut)
+        eng = GpuEngine(s, mol, b, integral_cutoff, prim_limit)
+        r = rhf(eng, mol.n_electrons // 2, conv=conv, D0=D0, incremental=incremental, max_iter=max_iter)
+        g = eng.gradient(r.D, r.W) if gradient else None
+    finally:
+        s.close()
+    r.seconds += t_guess
+    return r, g
