@@ -169,6 +169,17 @@ long long qb_xc_grid(double* xyzw, long long cap);
    out[3k+1] = df/drho, out[3k+2] = 4 df/dsigma (QUICK's b3lyp_e / b3lypf and becke/lyp). */
 int qb_xc_functional(int method, int n, const double* rho, const double* sigma, double* out);
 
+/* Device form of gpu_upload_cutoff_: the integral and primitive cutoffs, and QUICK's density
+   screen cutMatrix(I, J) = max |D| over the shell-pair block (densityCutoff / DNscreen,
+   src/schwarz.f90:550-600) computed on the GPU from the device density d_dense (nbasis^2)
+   instead of uploaded from the host.  Asynchronous on the library stream. */
+int qb_upload_cutoff_device(const double* d_dense, double integralCutoff, double primLimit);
+
+/* Device form of gpu_grad_: adds the two-electron gradient for the device density d_dense to
+   d_grad (3 x natom, device), with the cutoffs and density screen last uploaded.  Returns
+   when the gradient kernels have finished (their quartet counts are read back). */
+int qb_grad_device(const double* d_dense, double* d_grad);
+
 /* One-electron integrals.  QUICK forms these on the host in Fortran; these entry points follow
    the gpu_* conventions (arguments by pointer, Fortran column-major nbasis^2 matrices) and use
    the uploaded basis, coordinates and charges (gpu_upload_xyz_, gpu_upload_atom_and_chg_,

@@ -92,6 +92,8 @@ struct Context {
     DevBuf<int2> d_quartets;
     DevBuf<int2> d_ket_segs;             // constant primitive-count segments of the pair table
     DevBuf<double> d_S1, d_H1, d_D1, d_W1, d_g1;   // host-pointer one-electron entry points
+    DevBuf<int> d_shell_first;                      // Ksumtype - 1 (nshell + 1), for the device density screen
+    long long shell_first_version = -1;
     std::vector<ScreenClass> screen_cls;
     std::vector<int> class_group;        // lanes per shell quartet of each class kernel
     int generic_min_l = 99;              // classes with L sum >= this run the generic kernel (QB_GENERIC_MIN_L)
@@ -745,6 +747,7 @@ void gpu_shutdown_(void)
     c.d_D1.release();
     c.d_W1.release();
     c.d_g1.release();
+    c.d_shell_first.release();
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
     delete g;
     g = nullptr;
@@ -952,6 +955,41 @@ int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out)
     CK(c.d_dense_raw.alloc(nn));
     CK(cudaMemcpyAsync(c.d_dense_raw.p, d_dense, nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
     return fock_build(c, d_o_in, d_o_out);
+}
+
+int qb_upload_cutoff_device(const double* d_dense, double integralCutoff, double primLimit)
+{
+    Context& c = ctx();
+    if (require(c.have_basis, "gpu_upload_basis_ must precede qb_upload_cutoff_device")) return 1;
+    c.integralCutoff = integralCutoff;
+    c.primLimit = primLimit;
+    c.DMCutoff = 1e-9;
+    const size_t ns = c.nshell;
+    CK(c.d_cut_matrix.alloc(ns * ns));
+    if (c.shell_first_version != c.geom_version || !c.d_shell_first.p) {
+        std::vector<int> first(ns + 1);
+        for (size_t s = 0; s <= ns; s++) first[s] = c.Ksumtype[s] - 1;
+        CK(c.d_shell_first.alloc(ns + 1));
+        CK(cudaMemcpy(c.d_shell_first.p, first.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice));
+        c.shell_first_version = c.geom_version;
+    }
+    launch_density_screen(d_dense, c.d_shell_first.p, (int)ns, c.nbasis, c.d_cut_matrix.p, c.stream);
+    CK(cudaGetLastError());
+    c.have_cutoff = true;
+    return 0;
+}
+
+int qb_grad_device(const double* d_dense, double* d_grad)
+{
+    Context& c = ctx();
+    if (require(c.have_pairs && c.have_cutoff, "the pair list and cutoffs must be uploaded before qb_grad_device")) return 1;
+    const size_t nn = (size_t)c.nbasis * c.nbasis;
+    CK(c.d_dense_raw.alloc(nn));
+    CK(cudaMemcpyAsync(c.d_dense_raw.p, d_dense, nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    if (int rc = grad_build(c)) return rc;
+    launch_add_vector(c.d_grad.p, d_grad, 3 * c.natom, c.stream);
+    CK(cudaGetLastError());
+    return 0;
 }
 
 int qb_xc_device(const double* d_dense, const double* sigrad2, double* d_vxc, double* exc, double* nalpha)

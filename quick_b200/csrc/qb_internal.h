@@ -39,6 +39,9 @@ void launch_finish_counts(const ScreenParams& S, int* class_count, int* class_co
                           cudaStream_t st);
 void launch_scale_density(const double* D, const double* cons, double* Ds, int n, cudaStream_t st);
 void launch_fock_finish(const double* G, const double* cons, const double* Oin, double* Oout, int n, cudaStream_t st);
+// cut (nshell x nshell) = max |D| per shell-pair block; shell_first has nshell + 1 entries (0-based)
+void launch_density_screen(const double* D, const int* shell_first, int nshell, int n, double* cut, cudaStream_t st);
+void launch_add_vector(const double* x, double* y, int n, cudaStream_t st);
 // Class kernels with G lanes per shell quartet (G not compiled for the
 // class: 1); return the G launched.
 int launch_class(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st);

@@ -139,4 +139,39 @@ void launch_fock_finish(const double* G, const double* cons, const double* Oin, 
     QB_LAUNCH(fock_finish_kernel, (unsigned)((N + 255) / 256), 256, 0, st, G, cons, Oin, Oout, n);
 }
 
+// QUICK's density screen (densityCutoff / DNscreen, src/schwarz.f90:550-600)
+// on the device: cut(I, J) = cut(J, I) = max |D| over the basis functions of
+// shells I and J (shell I spans [first[I], first[I+1])).  One block per shell
+// I, threads over the shells J >= I.
+__global__ void density_screen_kernel(const double* __restrict__ D, const int* __restrict__ first, int nshell, int n,
+                                      double* __restrict__ cut)
+{
+    const int I = blockIdx.x;
+    const int i0 = first[I], i1 = first[I + 1];
+    for (int J = I + threadIdx.x; J < nshell; J += blockDim.x) {
+        const int j0 = first[J], j1 = first[J + 1];
+        double m = 0.0;
+        for (int j = j0; j < j1; j++)
+            for (int i = i0; i < i1; i++) m = fmax(m, fabs(D[i + (size_t)j * n]));
+        cut[I + (size_t)J * nshell] = m;
+        cut[J + (size_t)I * nshell] = m;
+    }
+}
+
+__global__ void add_vector_kernel(const double* __restrict__ x, double* __restrict__ y, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += x[i];
+}
+
+void launch_density_screen(const double* D, const int* shell_first, int nshell, int n, double* cut, cudaStream_t st)
+{
+    QB_LAUNCH(density_screen_kernel, nshell, 128, 0, st, D, shell_first, nshell, n, cut);
+}
+
+void launch_add_vector(const double* x, double* y, int n, cudaStream_t st)
+{
+    QB_LAUNCH(add_vector_kernel, (n + 255) / 256, 256, 0, st, x, y, n);
+}
+
 }  // namespace qb

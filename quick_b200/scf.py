@@ -63,6 +63,8 @@ class SCFResult:
     history: list = field(default_factory=list)   # per iteration: (energy, drms, seconds)
     fock_seconds: float = 0.0
     seconds: float = 0.0
+    fock_builds: int = 0
+    timings: dict = field(default_factory=dict)   # wall seconds per phase (run_rhf_device)
 
     @property
     def W(self):
@@ -267,4 +269,190 @@ def run_rhf_gpu(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1
     finally:
         s.close()
     r.seconds += t_guess
+    return r, g
+
+
+class DeviceRHF:
+    """The SCF with every matrix resident on the GPU.
+
+    The one-electron integrals (qb_oneint_device), the density screen
+    (qb_upload_cutoff_device), the Fock build (qb_fock_device) and the
+    gradients (qb_grad1e_device, qb_grad_device) run through the library's
+    device entry points on the caller's stream; the dense linear algebra of
+    the SCF (orthogonalisation, DIIS, diagonalisation by cuSOLVER) uses torch
+    tensors on the same stream.  Per iteration only the DIIS overlaps and the
+    convergence scalars come back to the host."""
+
+    def __init__(self, session, mol, basis, integral_cutoff=1e-10, prim_limit=1e-20, grad_cutoff=None):
+        import ctypes as C
+
+        import torch
+
+        from . import capi
+        self.torch, self.C, self.capi = torch, C, capi
+        self.lib = capi.lib()
+        self.s, self.mol, self.basis = session, mol, basis
+        self.cut, self.plim = integral_cutoff, prim_limit
+        self.grad_cut = integral_cutoff if grad_cutoff is None else grad_cutoff
+        # a stream of our own: the library treats a null stream as "use the
+        # library's stream", so torch's legacy default stream cannot be shared
+        self.stream = torch.cuda.Stream()
+        self.lib.qb_set_stream(C.c_void_p(self.stream.cuda_stream))
+        n = basis.nbasis
+        self.opts = dict(dtype=torch.float64, device=torch.device("cuda", torch.cuda.current_device()))
+        with torch.cuda.stream(self.stream):
+            self.S = torch.empty((n, n), **self.opts)
+            self.H = torch.empty((n, n), **self.opts)
+            self._rc(self.lib.qb_oneint_device(self._p(self.S), self._p(self.H)))
+        self.nfock = 0
+
+    def _p(self, t):
+        return self.C.c_void_p(t.data_ptr())
+
+    def _rc(self, rc):
+        if rc:
+            self.capi.check()
+            raise self.capi.QuickB200Error(rc, "device SCF call failed")
+
+    def fock(self, Dd, Oin):
+        """Oin + G(Dd), density screen from Dd."""
+        F = self.torch.empty_like(Oin)
+        C = self.C
+        self._rc(self.lib.qb_upload_cutoff_device(self._p(Dd), C.c_double(self.cut), C.c_double(self.plim)))
+        self._rc(self.lib.qb_fock_device(self._p(Dd), self._p(Oin), self._p(F)))
+        self.nfock += 1
+        return F
+
+    def run(self, nocc, D0, conv=1e-8, max_iter=100, diis_size=10, incremental=False, rebuild_every=8):
+        with self.torch.cuda.stream(self.stream):
+            return self._run(nocc, D0, conv, max_iter, diis_size, incremental, rebuild_every)
+
+    def _run(self, nocc, D0, conv, max_iter, diis_size, incremental, rebuild_every):
+        torch = self.torch
+        t_start = time.perf_counter()
+        S, H = self.S, self.H
+        s, U = torch.linalg.eigh(S)
+        keep = s > 1e-4
+        X = U[:, keep] * s[keep].rsqrt()
+        if bool(keep.all()):
+            X = X @ U.T
+        D = torch.as_tensor(np.ascontiguousarray(D0), **self.opts)
+        enuc = self.mol.nuclear_repulsion()
+        focks, errs = [], []
+        B = np.zeros((0, 0))
+        history = []
+        converged = False
+        F = D_built = None
+        e_elec = 0.0
+        it = 0
+        for it in range(1, max_iter + 1):
+            t0 = time.perf_counter()
+            if incremental and F is not None and (it - 1) % rebuild_every != 0:
+                F = self.fock(D - D_built, F)
+            else:
+                F = self.fock(D, H)
+            D_built = D
+            e_t = 0.5 * (D * (H + F)).sum()
+            FDS = F @ D @ S
+            err = X.T @ (FDS - FDS.T) @ X
+            focks.append(F)
+            errs.append(err)
+            if len(focks) > diis_size:
+                focks.pop(0)
+                errs.pop(0)
+                B = B[1:, 1:]
+            row = torch.stack([(e * err).sum() for e in errs]).cpu().numpy()
+            m = len(errs)
+            Bn = np.zeros((m, m))
+            Bn[:m - 1, :m - 1] = B
+            Bn[m - 1, :] = row
+            Bn[:, m - 1] = row
+            B = Bn
+            Fx = F
+            if m > 1:
+                A = -np.ones((m + 1, m + 1))
+                A[m, m] = 0.0
+                A[:m, :m] = B
+                rhs = np.zeros(m + 1)
+                rhs[m] = -1.0
+                try:
+                    c = np.linalg.solve(A, rhs)[:m]
+                    Fx = sum(float(ci) * Fi for ci, Fi in zip(c, focks))
+                except np.linalg.LinAlgError:
+                    Fx = F
+            eps, Cp = torch.linalg.eigh(X.T @ Fx @ X)
+            Co = (X @ Cp)[:, :nocc]
+            D_new = 2.0 * Co @ Co.T
+            dD = D_new - D
+            vals = torch.stack([e_t, dD.square().mean().sqrt(), dD.abs().max()]).cpu().numpy()
+            e_elec, drms, dmax = float(vals[0]), float(vals[1]), float(vals[2])
+            history.append((e_elec + enuc, drms, time.perf_counter() - t0))
+            D = D_new
+            if drms < conv and dmax < 100.0 * conv:
+                converged = True
+                break
+        eps, Cp = torch.linalg.eigh(X.T @ F @ X)
+        Cm = X @ Cp
+        self.D_dev, self.C_dev, self.eps_dev = D_built, Cm, eps
+        torch.cuda.synchronize()
+        return SCFResult(energy=e_elec + enuc, e_elec=e_elec, e_nuc=enuc, converged=converged, iterations=it,
+                         D=D_built.cpu().numpy(), C=Cm.cpu().numpy(), eps=eps.cpu().numpy(), nocc=nocc,
+                         history=history, seconds=time.perf_counter() - t_start)
+
+    def gradient(self):
+        """Full nuclear gradient (3 natom) at the last SCF's density."""
+        with self.torch.cuda.stream(self.stream):
+            return self._gradient()
+
+    def _gradient(self):
+        torch, C = self.torch, self.C
+        nocc = self.mol.n_electrons // 2
+        Co = self.C_dev[:, :nocc]
+        W = 2.0 * (Co * self.eps_dev[:nocc]) @ Co.T
+        D = self.D_dev
+        g = torch.zeros(3 * self.mol.natom, **self.opts)
+        self._rc(self.lib.qb_grad1e_device(self._p(D), self._p(W), self._p(g)))
+        self._rc(self.lib.qb_upload_cutoff_device(self._p(D), C.c_double(self.grad_cut), C.c_double(self.plim)))
+        self._rc(self.lib.qb_grad_device(self._p(D), self._p(g)))
+        return g.cpu().numpy()
+
+
+_ATOM_DENSITY = {}
+
+
+def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1e-8, gradient=True,
+                   mixed_cut=0.0, incremental=False, device=0, max_iter=100):
+    """Energy and gradient with the device-resident SCF (DeviceRHF) from the
+    SAD guess; atomic densities are cached per (element, basis).  Returns
+    (SCFResult, gradient or None); SCFResult.seconds covers guess, SCF and
+    gradient."""
+    from .basis import build_basis
+    from .capi import Session
+    t0 = time.perf_counter()
+    b = build_basis(mol.symbols, basis_name)
+
+    def atom(sym):
+        key = (sym, basis_name)
+        if key not in _ATOM_DENSITY:
+            _ATOM_DENSITY[key] = gpu_atom_density(sym, basis_name, device)
+        return _ATOM_DENSITY[key]
+
+    D0 = sad_guess(mol, b, atom)
+    t1 = time.perf_counter()
+    s = Session(device)
+    try:
+        s.upload_molecule(mol, b)
+        s.set_mixed_precision(mixed_cut)
+        eng = DeviceRHF(s, mol, b, integral_cutoff, prim_limit)
+        eng.torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        r = eng.run(mol.n_electrons // 2, D0, conv=conv, incremental=incremental, max_iter=max_iter)
+        t3 = time.perf_counter()
+        g = eng.gradient() if gradient else None
+        t4 = time.perf_counter()
+        r.fock_builds = eng.nfock
+    finally:
+        s.close()
+    r.seconds = time.perf_counter() - t0
+    r.timings = dict(guess=t1 - t0, setup=t2 - t1, scf=t3 - t2, gradient=t4 - t3)
     return r, g
