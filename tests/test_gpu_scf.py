@@ -157,3 +157,20 @@ def test_incremental_fock_builds():
         s.close()
     assert full.converged and inc.converged
     assert abs(full.energy - inc.energy) < 1e-8
+
+
+def test_device_scf_matches_host_scf():
+    """The device-resident SCF (DeviceRHF: density screen, Fock build,
+    gradients and the SCF algebra on the GPU) against the host-driven SCF
+    through the gpu_* host entry points: energy 1e-9 Eh, gradient 1e-8."""
+    m = water_cluster((2, 2, 1), seed=5)
+    r_h, g_h = scf.run_rhf_gpu(m, "6-31G*", 1e-10, 1e-20, conv=1e-9, gradient=True)
+    r_d, g_d = scf.run_rhf_device(m, "6-31G*", 1e-10, 1e-20, conv=1e-9)
+    assert r_h.converged and r_d.converged
+    assert abs(r_h.energy - r_d.energy) < 1e-9
+    assert np.abs(g_h - g_d).max() < 1e-8
+    # delta-D builds and the mixed split on the device path
+    r_i, g_i = scf.run_rhf_device(m, "6-31G*", 1e-10, 1e-20, conv=1e-9, incremental=True, mixed_cut=1e-3)
+    assert r_i.converged
+    assert abs(r_i.energy - r_d.energy) < 1e-6
+    assert np.abs(g_i - g_d).max() < 1e-5
