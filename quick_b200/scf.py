@@ -110,6 +110,7 @@ def rhf(engine, nocc, conv=1e-8, max_iter=100, diis_size=10, incremental=False, 
     S, H = engine.overlap_core()
     enuc = engine.enuc()
     X = orthogonaliser(S)
+    xc = engine.xc if getattr(engine, "method", 0) else None
 
     def diag(F):
         e, Cp = np.linalg.eigh(X.T @ F @ X)
@@ -142,6 +143,11 @@ def rhf(engine, nocc, conv=1e-8, max_iter=100, diis_size=10, incremental=False, 
         D_built = D
         F = H + G
         e_elec = 0.5 * float(np.sum(D * (H + F)))
+        if xc is not None:
+            # Kohn-Sham: F = H + G(D; hybrid exchange) + V_xc, E = tr DH + tr DG / 2 + E_xc
+            Vxc, Exc = xc(D)
+            F = F + Vxc
+            e_elec += Exc
         err = F @ D @ S - S @ D @ F
         err = X.T @ err @ X
         focks.append(F)
@@ -225,6 +231,15 @@ class GpuEngine:
         return self.s.get2e(np.zeros((n, n), order="F"), D, shell_cut_matrix(self.basis, D), self.cut, self.plim,
                             self.method)
 
+    def xc(self, D):
+        """(V_xc, E_xc) on QUICK's SG1 grid (gpu_getxc_)."""
+        from .basis import sigrad2
+        if not hasattr(self, "_sg"):
+            self._sg = sigrad2(self.basis)
+        n = self.basis.nbasis
+        V, exc, _, _ = self.s.getxc(np.zeros((n, n), order="F"), D, self._sg, method=self.method)
+        return V, exc
+
     def gradient(self, D, W):
         g = self.s.grad1e(D, W)
         return self.s.grad(g, D, shell_cut_matrix(self.basis, D), self.grad_cut, self.plim)
@@ -248,7 +263,7 @@ def gpu_atom_density(symbol, basis_name, device=0, conv=1e-7):
 
 
 def run_rhf_gpu(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1e-8, gradient=False,
-                mixed_cut=0.0, incremental=False, device=0, max_iter=100):
+                mixed_cut=0.0, incremental=False, device=0, max_iter=100, method=0):
     """Energy (and gradient) of a closed-shell molecule on the GPU: the SAD
     guess, the DIIS SCF over the GPU Fock build, and the analytic gradient.
     Returns (SCFResult, gradient or None)."""
@@ -263,7 +278,7 @@ def run_rhf_gpu(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1
         s.upload_molecule(mol, b)
         if mixed_cut:
             s.set_mixed_precision(mixed_cut)
-        eng = GpuEngine(s, mol, b, integral_cutoff, prim_limit)
+        eng = GpuEngine(s, mol, b, integral_cutoff, prim_limit, method=method)
         r = rhf(eng, mol.n_electrons // 2, conv=conv, D0=D0, incremental=incremental, max_iter=max_iter)
         g = eng.gradient(r.D, r.W) if gradient else None
     finally:
@@ -283,7 +298,7 @@ class DeviceRHF:
     tensors on the same stream.  Per iteration only the DIIS overlaps and the
     convergence scalars come back to the host."""
 
-    def __init__(self, session, mol, basis, integral_cutoff=1e-10, prim_limit=1e-20, grad_cutoff=None):
+    def __init__(self, session, mol, basis, integral_cutoff=1e-10, prim_limit=1e-20, grad_cutoff=None, method=0):
         import ctypes as C
 
         import torch
@@ -305,6 +320,23 @@ class DeviceRHF:
             self.H = torch.empty((n, n), **self.opts)
             self._rc(self.lib.qb_oneint_device(self._p(self.S), self._p(self.H)))
         self.nfock = 0
+        # 0 HF, 1 B3LYP, 2 BLYP: the exchange fraction of the Fock build and the functional
+        self.method = method
+        self.lib.gpu_upload_method_(C.byref(C.c_int(method)))
+        if method:
+            from .basis import sigrad2
+            self.sg = np.ascontiguousarray(sigrad2(basis))
+
+    def xc(self, D):
+        """(V_xc symmetrised, E_xc) for the device density D (qb_xc_device)."""
+        torch, C = self.torch, self.C
+        V = torch.zeros_like(D)
+        exc, na = C.c_double(0.0), C.c_double(0.0)
+        self._rc(self.lib.qb_xc_device(self._p(D), self.sg.ctypes.data_as(C.c_void_p), self._p(V), C.byref(exc),
+                                       C.byref(na)))
+        # the library fills V(j, i), j >= i of the column-major matrix: the upper triangle of this view
+        V = torch.triu(V) + torch.triu(V, 1).T
+        return V, exc.value
 
     def _p(self, t):
         return self.C.c_void_p(t.data_ptr())
@@ -342,17 +374,22 @@ class DeviceRHF:
         B = np.zeros((0, 0))
         history = []
         converged = False
-        F = D_built = None
+        F = F2 = D_built = None
         e_elec = 0.0
         it = 0
         for it in range(1, max_iter + 1):
             t0 = time.perf_counter()
-            if incremental and F is not None and (it - 1) % rebuild_every != 0:
-                F = self.fock(D - D_built, F)
+            if incremental and F2 is not None and (it - 1) % rebuild_every != 0:
+                F2 = self.fock(D - D_built, F2)
             else:
-                F = self.fock(D, H)
+                F2 = self.fock(D, H)
             D_built = D
-            e_t = 0.5 * (D * (H + F)).sum()
+            e_t = 0.5 * (D * (H + F2)).sum()
+            F = F2
+            if self.method:
+                Vxc, Exc = self.xc(D)
+                F = F2 + Vxc
+                e_t = e_t + Exc
             FDS = F @ D @ S
             err = X.T @ (FDS - FDS.T) @ X
             focks.append(F)
@@ -421,7 +458,7 @@ _ATOM_DENSITY = {}
 
 
 def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1e-8, gradient=True,
-                   mixed_cut=0.0, incremental=False, device=0, max_iter=100):
+                   mixed_cut=0.0, incremental=False, device=0, max_iter=100, method=0):
     """Energy and gradient with the device-resident SCF (DeviceRHF) from the
     SAD guess; atomic densities are cached per (element, basis).  Returns
     (SCFResult, gradient or None); SCFResult.seconds covers guess, SCF and
@@ -443,12 +480,13 @@ def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
     try:
         s.upload_molecule(mol, b)
         s.set_mixed_precision(mixed_cut)
-        eng = DeviceRHF(s, mol, b, integral_cutoff, prim_limit)
+        eng = DeviceRHF(s, mol, b, integral_cutoff, prim_limit, method=method)
         eng.torch.cuda.synchronize()
         t2 = time.perf_counter()
         r = eng.run(mol.n_electrons // 2, D0, conv=conv, incremental=incremental, max_iter=max_iter)
         t3 = time.perf_counter()
-        g = eng.gradient() if gradient else None
+        # no exchange-correlation gradient exists on QUICK's GPU path: DFT returns no gradient
+        g = eng.gradient() if gradient and not method else None
         t4 = time.perf_counter()
         r.fock_builds = eng.nfock
     finally:

@@ -27,6 +27,20 @@ def main():
         assert r.converged
         out["energies"]["%s/%s" % (name, bs)] = r.energy
         print(name, bs, "%.9f" % r.energy)
+    # Kohn-Sham: water (O-H 0.96 A, 104.5 deg) in 6-31G*, B3LYP (method 1) and
+    # BLYP (method 2), functional and SG1 quadrature from QUICK's own getxc
+    # compiled for the host (oracle/_ref), integral cutoff 1e-11
+    import math
+    import numpy as np
+    from quick_b200.molecule import Molecule
+    t = math.radians(104.5)
+    w = Molecule(["O", "H", "H"], np.array([[0, 0, 0], [0.96, 0, 0], [0.96 * math.cos(t), 0.96 * math.sin(t), 0]]))
+    wb = build_basis(w.symbols, "6-31G*")
+    for method, name in ((1, "B3LYP"), (2, "BLYP")):
+        r = scf.rhf(OracleEngine(w, wb, 1e-11, 1e-20, method=method), w.n_electrons // 2, conv=1e-8)
+        assert r.converged
+        out["energies"]["water/6-31G*/%s" % name] = r.energy
+        print("water", name, "%.10f" % r.energy)
     with open(os.path.join(HERE, "scf_golden.json"), "w") as fh:
         json.dump(out, fh, indent=1)
 

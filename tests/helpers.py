@@ -66,12 +66,25 @@ class OracleEngine:
     """The SCF engine interface of quick_b200.scf over the CPU oracle:
     one-electron integrals, QUICK's Fock build and the full gradient."""
 
-    def __init__(self, mol, basis, integral_cutoff=1e-10, prim_limit=1e-20):
+    def __init__(self, mol, basis, integral_cutoff=1e-10, prim_limit=1e-20, method=0):
         import oracle
         self.o = oracle
         self.mol, self.basis = mol, basis
         self.cut, self.plim = integral_cutoff, prim_limit
         self.Y, self.cp = oracle.schwarz(basis, mol.xyz_bohr)
+        # 0 HF, 1 B3LYP (exchange fraction 0.2), 2 BLYP; the functional from
+        # QUICK's own getxc compiled for the host
+        self.method = method
+        self.hybrid = {0: 1.0, 1: 0.2, 2: 0.0}[method]
+        if method:
+            from quick_b200.basis import sigrad2
+            self.sg = sigrad2(basis)
+            self._keep = oracle.ref_upload_molecule(mol, basis, self.Y, self.cp)
+
+    def xc(self, D):
+        n = self.basis.nbasis
+        V, exc, _, _ = self.o.ref_getxc(np.zeros((n, n), order="F"), D, self.sg, method=self.method)
+        return V, exc
 
     def overlap_core(self):
         return self.o.oneint(self.basis, self.mol)
@@ -81,7 +94,7 @@ class OracleEngine:
 
     def fock2e(self, D):
         G, _ = self.o.fock(self.basis, self.mol.xyz_bohr, self.Y, self.cp, self.o.cutmatrix(self.basis, D), D,
-                           self.cut, self.plim)
+                           self.cut, self.plim, hybrid=self.hybrid)
         return G
 
     def gradient(self, D, W):

@@ -174,3 +174,21 @@ def test_device_scf_matches_host_scf():
     assert r_i.converged
     assert abs(r_i.energy - r_d.energy) < 1e-6
     assert np.abs(g_i - g_d).max() < 1e-5
+
+
+@pytest.mark.parametrize("method,name", [(1, "B3LYP"), (2, "BLYP")])
+def test_kohn_sham_scf(method, name):
+    """Kohn-Sham SCF (hybrid-exchange Fock build + SG1 XC quadrature on the
+    GPU), host-driven and device-resident, against the oracle's SCF with
+    QUICK's own getxc (tests/golden/scf_golden.json): 1e-7 Eh."""
+    import math
+    with open(GOLDEN) as fh:
+        gold = json.load(fh)["energies"]["water/6-31G*/%s" % name]
+    t = math.radians(104.5)
+    m = Molecule(["O", "H", "H"], np.array([[0, 0, 0], [0.96, 0, 0], [0.96 * math.cos(t), 0.96 * math.sin(t), 0]]))
+    r_h, _ = scf.run_rhf_gpu(m, "6-31G*", 1e-11, 1e-20, conv=1e-8, method=method)
+    r_d, g_d = scf.run_rhf_device(m, "6-31G*", 1e-11, 1e-20, conv=1e-8, method=method)
+    assert r_h.converged and r_d.converged
+    assert g_d is None          # no exchange-correlation gradient on this path
+    assert abs(r_h.energy - gold) < 1e-7
+    assert abs(r_d.energy - gold) < 1e-7

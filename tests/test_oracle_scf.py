@@ -154,3 +154,23 @@ def test_aufbau_occupations():
     assert np.allclose(occ, [2, 2, 1, 1, 1, 0])
     occ = scf.aufbau_occupations(np.array([-1.0, -0.5]), 3)
     assert np.allclose(occ, [2, 1])
+
+
+def test_kohn_sham_oracle_scf():
+    """The oracle's Kohn-Sham SCF (QUICK's own getxc on the host) converges,
+    reproduces the committed value and lies within a few mEh of the
+    literature B3LYP/6-31G* water energy (about -76.409 near this geometry)."""
+    import json
+    import os
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("QUICK's host build (oracle/_ref) not available")
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scf_golden.json")) as fh:
+        gold = json.load(fh)["energies"]
+    t = math.radians(104.5)
+    m = Molecule(["O", "H", "H"], np.array([[0, 0, 0], [0.96, 0, 0], [0.96 * math.cos(t), 0.96 * math.sin(t), 0]]))
+    b = build_basis(m.symbols, "6-31G*")
+    r = scf.rhf(OracleEngine(m, b, 1e-11, 1e-20, method=1), m.n_electrons // 2, conv=1e-8)
+    assert r.converged
+    assert abs(r.energy - gold["water/6-31G*/B3LYP"]) < 1e-9
+    assert abs(r.energy - -76.409) < 5e-3
