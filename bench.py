@@ -449,6 +449,42 @@ def run_scf(args, ws, rank, local):
                     "device, one-electron + two-electron gradient on the GPU; wall clock"}
 
 
+def run_batch(args, ws, rank, local, nmol=None):
+    """Molecules/s for many small closed-shell molecules: (H2O)_n clusters,
+    n uniform in 1..12 (seeded), 6-31G*, RHF energy + analytic gradient each,
+    run one after another through one open session (SAD guess, device SCF to
+    density RMS 1e-8, gradient).  Molecules are split across ranks with no
+    collective (weak scaling: each rank takes its own list)."""
+    import torch
+    from quick_b200 import capi, scf
+    from quick_b200.molecule import water_cluster_n
+    torch.cuda.set_device(local)
+    nmol = nmol or args.batch
+    rng = np.random.default_rng(1234)
+    sizes = rng.integers(1, 13, size=nmol)
+    mols = [water_cluster_n(int(k), seed=i) for i, k in enumerate(sizes)]
+    sess = capi.Session(local)
+    try:
+        scf.run_rhf_device(mols[0], "6-31G*", 1e-10, 1e-20, conv=1e-8, device=local, session=sess)   # warm-up
+        barrier(ws)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        iters, nconv = 0, 0
+        for mol in mols:
+            r, g = scf.run_rhf_device(mol, "6-31G*", 1e-10, 1e-20, conv=1e-8, device=local, session=sess)
+            iters += r.iterations
+            nconv += int(r.converged)
+        torch.cuda.synchronize()
+        sec = max_over_ranks(time.perf_counter() - t0, ws)
+    finally:
+        sess.close()
+    return {"metric": "molecules/s (RHF energy + gradient, (H2O)_n n~U[1,12], 6-31G*)", "unit": "molecules/s",
+            "value": nmol * ws / sec, "seconds": sec, "molecules_per_rank": nmol, "n_gpus": ws,
+            "scaling": "weak", "converged": nconv, "mean_iterations": iters / nmol,
+            "basis_functions": [int(19 * k) for k in (sizes.min(), sizes.max())],
+            "note": "one molecule after another in one session (no batched kernel); wall clock, max over ranks"}
+
+
 def run_xc(args, ws, rank, local, sess=None):
     """B3LYP XC quadrature (gpu_getxc_'s work, qb_xc_device) on the workload
     molecule's SG1 grid: device time per call with the grid resident, L2
@@ -566,9 +602,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--classes", action="store_true", help="add per-class quartet counts")
-    ap.add_argument("--part", default="all", choices=["all", "fock", "xc", "scf"],
+    ap.add_argument("--batch", type=int, default=64, help="molecules in the batch line")
+    ap.add_argument("--part", default="all", choices=["all", "fock", "xc", "scf", "batch"],
                     help="fock: the Fock build line only; xc: the XC quadrature line only; "
-                         "scf: the SCF+gradient line only")
+                         "scf: the SCF+gradient line only; batch: the many-small-molecules line only")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     threads = os.cpu_count() or 1
@@ -590,8 +627,8 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    if args.part in ("xc", "scf"):
-        out = (run_xc if args.part == "xc" else run_scf)(args, ws, rank, local)
+    if args.part in ("xc", "scf", "batch"):
+        out = {"xc": run_xc, "scf": run_scf, "batch": run_batch}[args.part](args, ws, rank, local)
         if rank == 0:
             print(json.dumps(out))
         if ws > 1:
@@ -602,6 +639,7 @@ def main():
     if args.part == "all":
         out["xc"] = run_xc(args, ws, rank, local)
         out["scf"] = run_scf(args, ws, rank, local)
+        out["batch"] = run_batch(args, ws, rank, local)
     if rank == 0 and not args.no_cpu_baseline:
         qps, nq, sec = cpu_reference(threads)
         out["cpu_baseline"] = {"value": qps, "unit": "quartets/s", "cores": threads, "kind": "reference",

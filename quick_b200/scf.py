@@ -245,20 +245,22 @@ class GpuEngine:
         return self.s.grad(g, D, shell_cut_matrix(self.basis, D), self.grad_cut, self.plim)
 
 
-def gpu_atom_density(symbol, basis_name, device=0, conv=1e-7):
+def gpu_atom_density(symbol, basis_name, device=0, conv=1e-7, session=None):
     """Spherically averaged atomic density on the GPU (fractional-occupation
-    SCF of the atom alone); opens and closes its own session."""
+    SCF of the atom alone), in ``session`` if given (the atom replaces what
+    was uploaded), else in a session of its own."""
     from .basis import build_basis
     from .capi import Session
     from .molecule import Molecule
     m = Molecule([symbol], np.zeros((1, 3)))
     b = build_basis(m.symbols, basis_name)
-    s = Session(device)
+    s = Session(device) if session is None else session
     try:
         s.upload_molecule(m, b)
         r = rhf(GpuEngine(s, m, b, 1e-12, 1e-20), m.n_electrons / 2.0, conv=conv, max_iter=60, fractional=True)
     finally:
-        s.close()
+        if session is None:
+            s.close()
     return r.D
 
 
@@ -458,11 +460,13 @@ _ATOM_DENSITY = {}
 
 
 def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1e-8, gradient=True,
-                   mixed_cut=0.0, incremental=False, device=0, max_iter=100, method=0):
+                   mixed_cut=0.0, incremental=False, device=0, max_iter=100, method=0, session=None):
     """Energy and gradient with the device-resident SCF (DeviceRHF) from the
     SAD guess; atomic densities are cached per (element, basis).  Returns
     (SCFResult, gradient or None); SCFResult.seconds covers guess, SCF and
-    gradient."""
+    gradient.  ``session``: an open capi.Session to upload into and keep
+    open (molecule after molecule without re-initialising the library); by
+    default a session is opened and closed around the call."""
     from .basis import build_basis
     from .capi import Session
     t0 = time.perf_counter()
@@ -471,12 +475,13 @@ def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
     def atom(sym):
         key = (sym, basis_name)
         if key not in _ATOM_DENSITY:
-            _ATOM_DENSITY[key] = gpu_atom_density(sym, basis_name, device)
+            _ATOM_DENSITY[key] = gpu_atom_density(sym, basis_name, device, session=session)
         return _ATOM_DENSITY[key]
 
     D0 = sad_guess(mol, b, atom)
     t1 = time.perf_counter()
-    s = Session(device)
+    own = session is None
+    s = Session(device) if own else session
     try:
         s.upload_molecule(mol, b)
         s.set_mixed_precision(mixed_cut)
@@ -490,7 +495,12 @@ def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
         t4 = time.perf_counter()
         r.fock_builds = eng.nfock
     finally:
-        s.close()
+        if own:
+            s.close()
+        else:
+            # the engine's stream dies with it: hand the session back its own
+            from .capi import lib
+            lib().qb_set_stream(None)
     r.seconds = time.perf_counter() - t0
     r.timings = dict(guess=t1 - t0, setup=t2 - t1, scf=t3 - t2, gradient=t4 - t3)
     return r, g
