@@ -17,9 +17,11 @@
 //    (a b| = sum_k prod_i C(b_i, k_i) AB_i^(b_i - k_i) (a + k, 0|, first on the
 //    ket side for all e, then on the bra side per integral (term lists from
 //    the same program);
-//  * the Coulomb/exchange digestion into six shared-memory blocks, flushed to
-//    the Fock matrix once per quartet with the weights of the generated
-//    kernels (digest_coulomb / digest_exchange).
+//  * the quartet's integrals stored in shared memory, then contracted with
+//    the density into the six Coulomb/exchange blocks with one lane per
+//    output element (no atomics), flushed to the Fock matrix once per quartet
+//    with the weights of the generated kernels (digest_coulomb /
+//    digest_exchange).
 //
 // QUICK's own spdf path (gpu_get2e_subs.h:413-850 with int.h's
 // vertical_spdf* and the 84 x 84 `store`) computes the same integrals.
@@ -68,6 +70,7 @@ struct GenLayout {
     int lvl_off[3];       // three rotating VRR level buffers (level 0 starts with F_m)
     int acc_off, ne, nf;  // contracted [e0|f0], |e| in [la, lab], |f| in [lc, lcd]
     int x_off;            // ket-transformed block X[e][cd] (reuses the level buffers)
+    int i_off;            // the quartet's integrals I[ab][cd] (after X, same region)
     int pw_off;           // AB and CD powers, 24 values
     int d_off;            // six density blocks
     int j_off;            // six accumulator blocks
@@ -111,12 +114,14 @@ static GenLayout gen_layout(int la, int lb, int lc, int ld)
     G.ne = g_ncum(G.lab) - g_ncum(la - 1);
     G.nf = g_ncum(G.lcd) - g_ncum(lc - 1);
     const int nc = g_ncart(lc), nd = g_ncart(ld);
-    const int region = std::max(3 * mx, G.ne * nc * nd);
+    const int nab = g_ncart(la) * g_ncart(lb);
+    const int region = std::max(3 * mx, (G.ne + nab) * nc * nd);
     int off = 0;
     G.lvl_off[0] = 0;
     G.lvl_off[1] = mx;
     G.lvl_off[2] = 2 * mx;
     G.x_off = 0;
+    G.i_off = G.ne * nc * nd;
     off = region;
     G.acc_off = off;
     off += G.ne * G.nf;
@@ -340,9 +345,9 @@ __device__ void generic_quartet(const QuartetCtx& q, const FockParams& P, const 
 }
 
 // Horizontal recurrence in closed form (ket side into X, then bra side per
-// integral) and the Coulomb/exchange digestion into six shared-memory
-// blocks, flushed once per quartet with the weights of digest_coulomb /
-// digest_exchange.
+// integral into I) and the Coulomb/exchange contraction into six
+// shared-memory blocks, flushed once per quartet with the weights of
+// digest_coulomb / digest_exchange.
 __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const GenLayout& G, const GenProgram& R,
                                double* sm, int lane)
 {
@@ -389,23 +394,49 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
     }
     __syncwarp();
     const bool exch = P.hybrid != 0.0;
-    const int nout = na * nb * ncd;
+    const int nab = na * nb, nout = nab * ncd;
+    // the quartet's integrals I[ab][cd] (bra side of the horizontal recurrence)
+    double* I = sm + G.i_off;
     for (int o = lane; o < nout; o += 32) {
         const int ab = o / ncd, cd = o - ab * ncd;
-        const int ia = ab / nb, ib = ab - ia * nb, ic = cd / nd, id = cd - ic * nd;
         double v = 0.0;
         for (int j = R.bstart[ab]; j < R.bstart[ab + 1]; j++) {
             const int4 k = R.bterm[j];
             v += k.z * pw[k.y & 15] * pw[4 + ((k.y >> 4) & 15)] * pw[8 + (k.y >> 8)] * X[k.x * ncd + cd];
         }
-        atomicAdd(Jb + o_ab + ia * nb + ib, Db[o_cd + ic * nd + id] * v);
-        atomicAdd(Jb + o_cd + ic * nd + id, Db[o_ab + ia * nb + ib] * v);
-        if (exch) {
-            atomicAdd(Jb + o_ac + ia * nc + ic, Db[o_bd + ib * nd + id] * v);
-            atomicAdd(Jb + o_ad + ia * nd + id, Db[o_bc + ib * nc + ic] * v);
-            atomicAdd(Jb + o_bc + ib * nc + ic, Db[o_ad + ia * nd + id] * v);
-            atomicAdd(Jb + o_bd + ib * nd + id, Db[o_ac + ia * nc + ic] * v);
+        I[o] = v;
+    }
+    __syncwarp();
+    // contraction with the density, one lane per output element of each of
+    // the six blocks (no atomics): J_ab = sum_cd D_cd I, J_cd = sum_ab D_ab I,
+    // K_ac = sum_bd D_bd I, K_ad = sum_bc D_bc I, K_bc = sum_ad D_ad I,
+    // K_bd = sum_ac D_ac I
+    for (int t = lane; t < (exch ? nblk : o_ac); t += 32) {
+        double v = 0.0;
+        if (t < o_cd) {
+            const int ab = t - o_ab;
+            for (int cd = 0; cd < ncd; cd++) v += Db[o_cd + cd] * I[ab * ncd + cd];
+        } else if (t < o_ac) {
+            const int cd = t - o_cd;
+            for (int ab = 0; ab < nab; ab++) v += Db[o_ab + ab] * I[ab * ncd + cd];
+        } else if (t < o_ad) {
+            const int ia = (t - o_ac) / nc, ic = (t - o_ac) - ia * nc;
+            for (int ib = 0; ib < nb; ib++)
+                for (int id = 0; id < nd; id++) v += Db[o_bd + ib * nd + id] * I[(ia * nb + ib) * ncd + ic * nd + id];
+        } else if (t < o_bc) {
+            const int ia = (t - o_ad) / nd, id = (t - o_ad) - ia * nd;
+            for (int ib = 0; ib < nb; ib++)
+                for (int ic = 0; ic < nc; ic++) v += Db[o_bc + ib * nc + ic] * I[(ia * nb + ib) * ncd + ic * nd + id];
+        } else if (t < o_bd) {
+            const int ib = (t - o_bc) / nc, ic = (t - o_bc) - ib * nc;
+            for (int ia = 0; ia < na; ia++)
+                for (int id = 0; id < nd; id++) v += Db[o_ad + ia * nd + id] * I[(ia * nb + ib) * ncd + ic * nd + id];
+        } else {
+            const int ib = (t - o_bd) / nd, id = (t - o_bd) - ib * nd;
+            for (int ia = 0; ia < na; ia++)
+                for (int ic = 0; ic < nc; ic++) v += Db[o_ac + ia * nc + ic] * I[(ia * nb + ib) * ncd + ic * nd + id];
         }
+        Jb[t] = v;
     }
     __syncwarp();
     const double wj = 2.0 * q.w, wk = -0.5 * P.hybrid * q.w;
