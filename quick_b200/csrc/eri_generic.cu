@@ -1,14 +1,14 @@
-// Angular classes with an f shell (any shell up to L = 3): one warp per
-// shell quartet, the recurrences in shared memory.
+// Angular classes with an f shell (any shell up to L = 3): one thread block
+// per shell quartet, the recurrences in shared memory.
 //
 // The straight-line generated kernels (gen_eri.py) cover s, p and d; their
 // f counterparts would be tens of thousands of statements per class.  This
 // kernel runs the same algorithm with loops instead:
 //
-//  * F_m(T), m = 0..LA+LB+LC+LD (lane 0, the table scheme of boys<L>);
+//  * F_m(T), m = 0..LA+LB+LC+LD (thread 0, the table scheme of boys<L>);
 //  * the Obara-Saika vertical recurrence [e0|f0]^(m), |e| <= LA+LB,
-//    |f| <= LC+LD, one level of |f| at a time (three levels kept), the lanes
-//    of the warp sharing each level's entries; a per-class program built
+//    |f| <= LC+LD, one level of |f| at a time (three levels kept), the threads
+//    of the block sharing each level's entries; a per-class program built
 //    once on the host lists every entry with its source offsets in shared
 //    memory, so the device loop is loads and FMAs;
 //  * contraction of [e0|f0]^(0) for LA <= |e|, LC <= |f| over the primitive
@@ -18,7 +18,7 @@
 //    ket side for all e, then on the bra side per integral (term lists from
 //    the same program);
 //  * the quartet's integrals stored in shared memory, then contracted with
-//    the density into the six Coulomb/exchange blocks with one lane per
+//    the density into the six Coulomb/exchange blocks with one thread per
 //    output element (no atomics), flushed to the Fock matrix once per quartet
 //    with the weights of the generated kernels (digest_coulomb /
 //    digest_exchange).
@@ -26,6 +26,7 @@
 // QUICK's own spdf path (gpu_get2e_subs.h:413-850 with int.h's
 // vertical_spdf* and the 84 x 84 `store`) computes the same integrals.
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 #include <vector>
 
@@ -280,20 +281,20 @@ __device__ void boys_rt(const double* __restrict__ tab, double T, double pref, d
     for (int m = 0; m <= L; m++) F[m] *= pref;
 }
 
-// One shell quartet with the 32 lanes of a warp: primitive loop with the
+// One shell quartet with the nt threads of a block: primitive loop with the
 // vertical recurrence and contraction, program-driven.
 __device__ void generic_quartet(const QuartetCtx& q, const FockParams& P, const GenLayout& G, const GenProgram& R,
-                                double* sm, int lane)
+                                double* sm, int tid, int nt)
 {
     double* acc = sm + G.acc_off;
-    for (int i = lane; i < G.ne * G.nf; i += 32) acc[i] = 0.0;
-    __syncwarp();
+    for (int i = tid; i < G.ne * G.nf; i += nt) acc[i] = 0.0;
+    __syncthreads();
     for (int ib = 0; ib < q.nbra; ib++) {
         const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);
         const PrimPair pb = load_prim(P, q.bra_off + ib, xb);
         for (int ik = 0; ik < q.nket; ik++) {
             const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);
-            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;   // the same for every lane
+            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;   // the same for every thread
             const PrimPair pk = load_prim(P, q.ket_off + ik, xk);
             const double pq = pb.p + pk.p;
             const double sq = rsqrt(pq);
@@ -308,17 +309,17 @@ __device__ void generic_quartet(const QuartetCtx& q, const FockParams& P, const 
             const double QC[3] = {pk.PAx, pk.PAy, pk.PAz};
             const double o2p = pb.o2p, o2q = pk.o2p, o2pq = 0.5 * ipq;
             const double rp = pk.p * ipq, rq = pb.p * ipq;
-            if (lane == 0) boys_rt(P.boys, T, pb.K * pk.K * sq, sm + G.lvl_off[0], G.lt);
-            __syncwarp();
+            if (tid == 0) boys_rt(P.boys, T, pb.K * pk.K * sq, sm + G.lvl_off[0], G.lt);
+            __syncthreads();
             for (int s = 0; s < R.nstage; s++) {
                 const int type = R.stage[3 * s], first = R.stage[3 * s + 1], cnt = R.stage[3 * s + 2];
                 if (type == 2) {
-                    for (int t = lane; t < cnt; t += 32) {
+                    for (int t = tid; t < cnt; t += nt) {
                         const int4 e = R.ent[first + t];
                         acc[e.x] += sm[e.y];
                     }
                 } else {
-                    for (int t = lane; t < cnt; t += 32) {
+                    for (int t = tid; t < cnt; t += nt) {
                         const int4 e = R.ent[first + t];
                         const int mt = R.meta[first + t];
                         const int i = mt & 3, mc = (mt >> 2) & 15, mg = (mt >> 6) & 15, nm = mt >> 10;
@@ -338,7 +339,7 @@ __device__ void generic_quartet(const QuartetCtx& q, const FockParams& P, const 
                         }
                     }
                 }
-                __syncwarp();
+                __syncthreads();
             }
         }
     }
@@ -349,7 +350,7 @@ __device__ void generic_quartet(const QuartetCtx& q, const FockParams& P, const 
 // shared-memory blocks, flushed once per quartet with the weights of
 // digest_coulomb / digest_exchange.
 __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const GenLayout& G, const GenProgram& R,
-                               double* sm, int lane)
+                               double* sm, int tid, int nt)
 {
     const int na = g_ncart(G.la), nb = g_ncart(G.lb), nc = g_ncart(G.lc), nd = g_ncart(G.ld);
     const int ncd = nc * nd;
@@ -358,19 +359,19 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
     double* pw = sm + G.pw_off;
     double* Db = sm + G.d_off;
     double* Jb = sm + G.j_off;
-    if (lane < 24) {
+    if (tid < 24) {
         const double AB[3] = {q.ABx, q.ABy, q.ABz}, CD[3] = {q.CDx, q.CDy, q.CDz};
-        const double base = lane < 12 ? AB[lane / 4] : CD[(lane - 12) / 4];
+        const double base = tid < 12 ? AB[tid / 4] : CD[(tid - 12) / 4];
         double v = 1.0;
-        for (int k = 0; k < (lane & 3); k++) v *= base;
-        pw[lane] = v;
+        for (int k = 0; k < (tid & 3); k++) v *= base;
+        pw[tid] = v;
     }
     const int o_ab = 0, o_cd = o_ab + na * nb, o_ac = o_cd + nc * nd, o_ad = o_ac + na * nc, o_bc = o_ad + na * nd,
               o_bd = o_bc + nb * nc, nblk = o_bd + nb * nd;
     const double* Dm = P.dense;
     const int n = P.nbasis;
     const int a0 = q.bfA, b0 = q.bfB, c0 = q.bfC, d0 = q.bfD;
-    for (int t = lane; t < nblk; t += 32) {
+    for (int t = tid; t < nblk; t += nt) {
         int r, c;
         if (t < o_cd) r = a0 + (t - o_ab) / nb, c = b0 + (t - o_ab) % nb;
         else if (t < o_ac) r = c0 + (t - o_cd) / nd, c = d0 + (t - o_cd) % nd;
@@ -381,9 +382,9 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         Db[t] = __ldg(Dm + (size_t)r * n + c);
         Jb[t] = 0.0;
     }
-    __syncwarp();
+    __syncthreads();
     // ket side: X[e][cd] = sum_k C * CD^pw * acc[e][f]
-    for (int t = lane; t < G.ne * ncd; t += 32) {
+    for (int t = tid; t < G.ne * ncd; t += nt) {
         const int e = t / ncd, cd = t - e * ncd;
         double v = 0.0;
         for (int j = R.kstart[cd]; j < R.kstart[cd + 1]; j++) {
@@ -392,12 +393,12 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         }
         X[t] = v;
     }
-    __syncwarp();
+    __syncthreads();
     const bool exch = P.hybrid != 0.0;
     const int nab = na * nb, nout = nab * ncd;
     // the quartet's integrals I[ab][cd] (bra side of the horizontal recurrence)
     double* I = sm + G.i_off;
-    for (int o = lane; o < nout; o += 32) {
+    for (int o = tid; o < nout; o += nt) {
         const int ab = o / ncd, cd = o - ab * ncd;
         double v = 0.0;
         for (int j = R.bstart[ab]; j < R.bstart[ab + 1]; j++) {
@@ -406,12 +407,12 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         }
         I[o] = v;
     }
-    __syncwarp();
-    // contraction with the density, one lane per output element of each of
+    __syncthreads();
+    // contraction with the density, one thread per output element of each of
     // the six blocks (no atomics): J_ab = sum_cd D_cd I, J_cd = sum_ab D_ab I,
     // K_ac = sum_bd D_bd I, K_ad = sum_bc D_bc I, K_bc = sum_ad D_ad I,
     // K_bd = sum_ac D_ac I
-    for (int t = lane; t < (exch ? nblk : o_ac); t += 32) {
+    for (int t = tid; t < (exch ? nblk : o_ac); t += nt) {
         double v = 0.0;
         if (t < o_cd) {
             const int ab = t - o_ab;
@@ -438,9 +439,9 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         }
         Jb[t] = v;
     }
-    __syncwarp();
+    __syncthreads();
     const double wj = 2.0 * q.w, wk = -0.5 * P.hybrid * q.w;
-    for (int t = lane; t < (exch ? nblk : o_ac); t += 32) {
+    for (int t = tid; t < (exch ? nblk : o_ac); t += nt) {
         int r, c;
         double wgt;
         if (t < o_cd) r = a0 + (t - o_ab) / nb, c = b0 + (t - o_ab) % nb, wgt = wj;
@@ -451,23 +452,26 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         else r = b0 + (t - o_bd) / nd, c = d0 + (t - o_bd) % nd, wgt = wk;
         fock_add(P.fock, n, r, c, wgt * Jb[t]);
     }
-    __syncwarp();
+    __syncthreads();
 }
 
-// One warp (one block) per shell quartet; fp32_list: walk the class's FP32
-// list (mixed precision) -- these classes compute in FP64 either way.
-__global__ void __launch_bounds__(32) fock_generic_kernel(const FockParams P, int cls, const GenLayout G,
-                                                         const GenProgram R, int fp32_list)
+// One block per shell quartet (its warps share the recurrence stages and
+// the contraction; the shared-memory layout of one quartet bounds the blocks
+// per SM, so more threads per quartet is how occupancy grows); fp32_list:
+// walk the class's FP32 list (mixed precision) -- these classes compute in
+// FP64 either way.
+__global__ void __launch_bounds__(256) fock_generic_kernel(const FockParams P, int cls, const GenLayout G,
+                                                          const GenProgram R, int fp32_list)
 {
     extern __shared__ double sm[];
-    const int lane = threadIdx.x;
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int n = fp32_list ? P.class_count32[cls] : P.class_count[cls];
     const int2* list = fp32_list ? P.quartets + (P.class_end[cls] - n) : P.quartets + P.class_offset[cls];
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
         QuartetCtx q;
         load_quartet(P, list[i], true, q);
-        generic_quartet(q, P, G, R, sm, lane);
-        generic_digest(q, P, G, R, sm, lane);
+        generic_quartet(q, P, G, R, sm, tid, nt);
+        generic_digest(q, P, G, R, sm, tid, nt);
     }
 }
 
@@ -512,7 +516,7 @@ __global__ void __launch_bounds__(32) schwarz_generic_kernel(const SchwarzParams
         q.ABz = q.CDz = ab.z;
         q.dnmax = 1.0;
         q.swap = false;
-        generic_quartet(q, P, G, R, sm, lane);
+        generic_quartet(q, P, G, R, sm, lane, 32);
         double* pw = sm + G.pw_off;
         if (lane < 24) {
             const double base = lane < 12 ? (&ab.x)[lane / 4] : (&ab.x)[(lane - 12) / 4];
@@ -612,11 +616,17 @@ int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockPara
             return -1;
         configured = maxsm;
     }
+    // threads per quartet (QB_GEN_THREADS, default 128)
+    static const int nt = [] {
+        const char* e = getenv("QB_GEN_THREADS");
+        const int v = e ? atoi(e) : 128;
+        return (v == 32 || v == 64 || v == 128 || v == 256) ? v : 128;
+    }();
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fock_generic_kernel, 32, bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fock_generic_kernel, nt, bytes);
     const int grid = std::max(1, std::min(nq, nsm * std::max(per_sm, 1)));
-    QB_LAUNCH(fock_generic_kernel, grid, 32, bytes, st, P, cls, gc->G, gc->R, fp32_list);
-    return 32;
+    QB_LAUNCH(fock_generic_kernel, grid, nt, bytes, st, P, cls, gc->G, gc->R, fp32_list);
+    return nt;
 }
 
 int launch_generic_schwarz(int la, int lb, const SchwarzParams& S, int begin, int end, int mode, int nsm,
