@@ -551,9 +551,12 @@ static int grad_build(Context& c)
     for (int k = 0; k < kNumClasses; k++) {
         if (cnt[k] == 0) continue;
         const int GS = std::min(c.class_group.empty() ? 1 : std::max(c.class_group[k], 1), grad_max_group(k));
-        if (launch_grad_class(k, P, G, GS, cnt[k], c.nsm, c.stream) < 0)
-            return set_error(5, "gpu_grad_: no gradient kernel for class (%d%d|%d%d): f shells are not built for "
-                                "the gradient", kClassL[k][0], kClassL[k][1], kClassL[k][2], kClassL[k][3]), 5;
+        if (launch_grad_class(k, P, G, GS, cnt[k], c.nsm, c.stream) < 0) {
+            const int* Lk = kClassL[k];
+            if (launch_generic_grad_class(k, Lk[0], Lk[1], Lk[2], Lk[3], P, G, cnt[k], c.nsm, c.stream) < 0)
+                return set_error(2, "gpu_grad_: cannot allocate the scratch of class (%d%d|%d%d)", Lk[0], Lk[1],
+                                 Lk[2], Lk[3]), 2;
+        }
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[3], c.stream));
@@ -742,6 +745,7 @@ void gpu_shutdown_(void)
         if (e) cudaEventDestroy(e), e = nullptr;
     xc_release();
     oneint_release();
+    generic_release();
     c.d_S1.release();
     c.d_H1.release();
     c.d_D1.release();

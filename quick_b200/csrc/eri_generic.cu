@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "eri_common.cuh"
+#include "grad_common.cuh"
 #include "qb_internal.h"
 #include "schwarz.cuh"
 
@@ -143,7 +144,7 @@ struct GenProgramHost {
     std::vector<int4> ent, kterm, bterm;
 };
 
-static void gen_program(const GenLayout& G, GenProgramHost& H)
+static void gen_program(const GenLayout& G, GenProgramHost& H, bool with_hrr = true)
 {
     const int lt = G.lt, lab = G.lab;
     auto buf = [&](int k) { return G.lvl_off[k % 3]; };
@@ -244,6 +245,7 @@ static void gen_program(const GenLayout& G, GenProgramHost& H)
             }
         start.push_back((int)out.size());
     };
+    if (!with_hrr) return;   // the gradient program (its shells may exceed f) does its own transfer
     terms(G.lc, G.ld, H.kstart, H.kterm);
     terms(G.la, G.lb, H.bstart, H.bterm);
 }
@@ -560,18 +562,21 @@ struct GenCached {
     int dev = -1;
 };
 
-static GenCached* gen_cached(int la, int lb, int lc, int ld)
+// grad: the layout and recurrence program of the extended range of the
+// gradient kernel (shells may exceed f; no horizontal terms).
+static GenCached* gen_cached(int la, int lb, int lc, int ld, bool grad = false)
 {
     static std::map<int, GenCached> cache;
     int dev = 0;
     cudaGetDevice(&dev);
-    const int key = ((la * 4 + lb) * 4 + lc) * 4 + ld + 256 * dev;
+    const int key = grad ? (1 << 24) + (((la * 8 + lb) * 8 + lc) * 8 + ld) + 4096 * dev
+                         : ((la * 4 + lb) * 4 + lc) * 4 + ld + 256 * dev;
     auto it = cache.find(key);
     if (it != cache.end()) return &it->second;
     GenCached c;
     c.G = gen_layout(la, lb, lc, ld);
     GenProgramHost H;
-    gen_program(c.G, H);
+    gen_program(c.G, H, !grad);
     const size_t b_stage = H.stage.size() * sizeof(int), b_meta = H.meta.size() * sizeof(int);
     const size_t b_ent = H.ent.size() * sizeof(int4), b_kt = H.kterm.size() * sizeof(int4),
                  b_bt = H.bterm.size() * sizeof(int4);
@@ -657,6 +662,278 @@ int launch_generic_schwarz(int la, int lb, const SchwarzParams& S, int begin, in
 size_t generic_class_smem(int la, int lb, int lc, int ld)
 {
     return (size_t)gen_layout(la, lb, lc, ld).total * sizeof(double);
+}
+
+// ------------------------------------------------------------ gradient
+// Two-electron gradient of the classes with an f shell (no straight-line
+// gradient kernels exist for them): one 128-thread block per shell quartet.
+// The vertical recurrence of the class extended by one unit on each side,
+// [e0|f0] with |e| <= LA+LB+1, |f| <= LC+LD+1 (the program of gen_program for
+// that range), is contracted over the primitive quartets into four sums with
+// the weights 1, 2 alpha, 2 beta and 2 gamma (the exponents of A, B and C);
+// then per integral and direction, by the horizontal transfer in closed form
+// on both sides,
+//   d/dA_i (ab|cd) = 2 alpha (a+1_i b|cd) - a_i (a-1_i b|cd),
+//   d/dB_i (ab|cd) = 2 beta  (a b+1_i|cd) - b_i (a b-1_i|cd),
+//   d/dC_i (ab|cd) = 2 gamma (ab|c+1_i d) - c_i (ab|c-1_i d),
+// contracted with the density products of the generated gradient kernels
+// (4 D_ab D_cd - h (D_ac D_bd + D_ad D_bc)), D by translational invariance.
+// The recurrence buffers and sums of the extended range exceed shared memory
+// for the large classes, so each block works in its own slice of a global
+// scratch array (L2-resident for all but the largest classes).
+__constant__ int kQuickCartD[4][10][3] = {
+    {{0, 0, 0}},
+    {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}},
+    {{2, 0, 0}, {1, 1, 0}, {0, 2, 0}, {1, 0, 1}, {0, 1, 1}, {0, 0, 2}},
+    {{3, 0, 0}, {2, 1, 0}, {1, 2, 0}, {0, 3, 0}, {2, 0, 1}, {1, 1, 1}, {0, 2, 1}, {1, 0, 2}, {0, 1, 2}, {0, 0, 3}},
+};
+
+struct GenGradInfo {
+    int la, lb, lc, ld;     // the class
+    int elo, flo;           // lowest |e|, |f| held in the sums
+    int ne, nf;             // extents of the sums (rows |e| in [elo, LA+LB+1], columns |f| in [flo, LC+LD+1])
+    long long per_block;    // scratch doubles per block
+};
+
+__device__ __forceinline__ int gen_gidx(int x, int y, int z, int lo)
+{
+    const int n = x + y + z, t = y + z;
+    return g_ncum(n - 1) - g_ncum(lo - 1) + t * (t + 1) / 2 + z;
+}
+
+__device__ __forceinline__ double gen_ipow(double b, int e)
+{
+    double r = 1.0;
+    for (int i = 0; i < e; i++) r *= b;
+    return r;
+}
+
+__device__ __forceinline__ int gen_binom(int n, int k)
+{
+    int r = 1;
+    for (int j = 1; j <= k; j++) r = r * (n - k + j) / j;
+    return r;
+}
+
+// (a b|c d) = sum_kb sum_kd C(b,kb) AB^(b-kb) C(d,kd) CD^(d-kd) E[a+kb][c+kd]
+__device__ double gen_hrr2(const double* E, const GenGradInfo& I, const int* a, const int* b, const int* c,
+                           const int* d, const double* AB, const double* CD)
+{
+    double s = 0.0;
+    for (int kx = 0; kx <= b[0]; kx++)
+        for (int ky = 0; ky <= b[1]; ky++)
+            for (int kz = 0; kz <= b[2]; kz++) {
+                const double cb = gen_binom(b[0], kx) * gen_binom(b[1], ky) * gen_binom(b[2], kz) *
+                                  gen_ipow(AB[0], b[0] - kx) * gen_ipow(AB[1], b[1] - ky) * gen_ipow(AB[2], b[2] - kz);
+                const double* row = E + (size_t)gen_gidx(a[0] + kx, a[1] + ky, a[2] + kz, I.elo) * I.nf;
+                double t = 0.0;
+                for (int lx = 0; lx <= d[0]; lx++)
+                    for (int ly = 0; ly <= d[1]; ly++)
+                        for (int lz = 0; lz <= d[2]; lz++)
+                            t += gen_binom(d[0], lx) * gen_binom(d[1], ly) * gen_binom(d[2], lz) *
+                                 gen_ipow(CD[0], d[0] - lx) * gen_ipow(CD[1], d[1] - ly) * gen_ipow(CD[2], d[2] - lz) *
+                                 row[gen_gidx(c[0] + lx, c[1] + ly, c[2] + lz, I.flo)];
+                s += cb * t;
+            }
+    return s;
+}
+
+__global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, const GradExtra X, int cls,
+                                                          const GenLayout G, const GenProgram R, const GenGradInfo I,
+                                                          double* scratch)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    double* sm = scratch + (size_t)blockIdx.x * I.per_block;   // this block's recurrence buffers and sums
+    const size_t nacc = (size_t)I.ne * I.nf;
+    double* E1 = sm + G.acc_off;
+    double* Ea = sm + G.total;
+    double* Eb = Ea + nacc;
+    double* Ec = Eb + nacc;
+    __shared__ double red[9][4];
+    const int na = g_ncart(I.la), nb = g_ncart(I.lb), nc = g_ncart(I.lc), nd = g_ncart(I.ld);
+    const int n = P.class_count[cls];
+    const int2* list = P.quartets + P.class_offset[cls];
+    for (int qi = blockIdx.x; qi < n; qi += gridDim.x) {
+        QuartetCtx q;
+        load_quartet(P, list[qi], true, q);
+        for (size_t i = tid; i < nacc; i += nt) E1[i] = Ea[i] = Eb[i] = Ec[i] = 0.0;
+        __syncthreads();
+        for (int ib = 0; ib < q.nbra; ib++) {
+            const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);
+            const PrimPair pb = load_prim(P, q.bra_off + ib, xb);
+            for (int ik = 0; ik < q.nket; ik++) {
+                const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);
+                if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;   // the same for every thread
+                const PrimPair pk = load_prim(P, q.ket_off + ik, xk);
+                const double pq = pb.p + pk.p;
+                const double sq = rsqrt(pq);
+                const double ipq = sq * sq;
+                const double rho = pb.p * pk.p * ipq;
+                const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
+                const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+                const double fp = -pk.p * ipq, fq = pb.p * ipq;
+                const double WP[3] = {fp * PQx, fp * PQy, fp * PQz};
+                const double WQ[3] = {fq * PQx, fq * PQy, fq * PQz};
+                const double PA[3] = {pb.PAx, pb.PAy, pb.PAz};
+                const double QC[3] = {pk.PAx, pk.PAy, pk.PAz};
+                const double o2p = pb.o2p, o2q = pk.o2p, o2pq = 0.5 * ipq;
+                const double rp = pk.p * ipq, rq = pb.p * ipq;
+                // exponent weights of the derivative sums: 2 alpha, 2 beta, 2 gamma
+                const double wa = 2.0 * xb.y, wb = 2.0 * (pb.p - xb.y), wc = 2.0 * xk.y;
+                if (tid == 0) boys_rt(P.boys, T, pb.K * pk.K * sq, sm + G.lvl_off[0], G.lt);
+                __syncthreads();
+                for (int s = 0; s < R.nstage; s++) {
+                    const int type = R.stage[3 * s], first = R.stage[3 * s + 1], cnt = R.stage[3 * s + 2];
+                    if (type == 2) {
+                        for (int t = tid; t < cnt; t += nt) {
+                            const int4 e = R.ent[first + t];
+                            const double v = sm[e.y];
+                            E1[e.x] += v;
+                            Ea[e.x] += wa * v;
+                            Eb[e.x] += wb * v;
+                            Ec[e.x] += wc * v;
+                        }
+                    } else {
+                        for (int t = tid; t < cnt; t += nt) {
+                            const int4 e = R.ent[first + t];
+                            const int mt = R.meta[first + t];
+                            const int i = mt & 3, mc = (mt >> 2) & 15, mg = (mt >> 6) & 15, nm = mt >> 10;
+                            const double* a = sm + e.y;
+                            double* o = sm + e.x;
+                            const double ci = type == 0 ? PA[i] : QC[i];
+                            const double wi = type == 0 ? WP[i] : WQ[i];
+                            const double cm = mc * (type == 0 ? o2p : o2q), r = type == 0 ? rp : rq;
+                            const double* c = sm + (e.z >= 0 ? e.z : 0);
+                            const double* gg = sm + (e.w >= 0 ? e.w : 0);
+                            const double gm = mg * o2pq;
+                            for (int m = 0; m < nm; m++) {
+                                double v = ci * a[m] + wi * a[m + 1];
+                                if (e.z >= 0) v += cm * (c[m] - r * c[m + 1]);
+                                if (e.w >= 0) v += gm * gg[m + 1];
+                                o[m] = v;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+        // derivative integrals contracted with the density products
+        const double AB[3] = {q.ABx, q.ABy, q.ABz}, CD[3] = {q.CDx, q.CDy, q.CDz};
+        const double* Dm = P.dense;
+        const int nbf = P.nbasis;
+        const double hx = P.hybrid;
+        double gs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const int nout = na * nb * nc * nd;
+        for (int o = tid; o < nout; o += nt) {
+            int r = o;
+            const int id = r % nd; r /= nd;
+            const int ic = r % nc; r /= nc;
+            const int ibb = r % nb; r /= nb;
+            const int ia = r;
+            int a[3], b[3], c[3], d[3];
+            for (int k = 0; k < 3; k++) {
+                a[k] = kQuickCartD[I.la][ia][k];
+                b[k] = kQuickCartD[I.lb][ibb][k];
+                c[k] = kQuickCartD[I.lc][ic][k];
+                d[k] = kQuickCartD[I.ld][id][k];
+            }
+            const int fa = q.bfA + ia, fb = q.bfB + ibb, fc = q.bfC + ic, fd = q.bfD + id;
+            const double Dab = __ldg(Dm + (size_t)fa * nbf + fb), Dcd = __ldg(Dm + (size_t)fc * nbf + fd);
+            const double Dac = __ldg(Dm + (size_t)fa * nbf + fc), Dbd = __ldg(Dm + (size_t)fb * nbf + fd);
+            const double Dad = __ldg(Dm + (size_t)fa * nbf + fd), Dbc = __ldg(Dm + (size_t)fb * nbf + fc);
+            const double g = 4.0 * Dab * Dcd - hx * (Dac * Dbd + Dad * Dbc);
+            if (g == 0.0) continue;
+            for (int i = 0; i < 3; i++) {
+                int u[3] = {a[0], a[1], a[2]};
+                u[i]++;
+                double dA = gen_hrr2(Ea, I, u, b, c, d, AB, CD);
+                if (a[i] > 0) {
+                    u[i] -= 2;
+                    dA -= a[i] * gen_hrr2(E1, I, u, b, c, d, AB, CD);
+                }
+                int v[3] = {b[0], b[1], b[2]};
+                v[i]++;
+                double dB = gen_hrr2(Eb, I, a, v, c, d, AB, CD);
+                if (b[i] > 0) {
+                    v[i] -= 2;
+                    dB -= b[i] * gen_hrr2(E1, I, a, v, c, d, AB, CD);
+                }
+                int w[3] = {c[0], c[1], c[2]};
+                w[i]++;
+                double dC = gen_hrr2(Ec, I, a, b, w, d, AB, CD);
+                if (c[i] > 0) {
+                    w[i] -= 2;
+                    dC -= c[i] * gen_hrr2(E1, I, a, b, w, d, AB, CD);
+                }
+                gs[i] += g * dA;
+                gs[3 + i] += g * dB;
+                gs[6 + i] += g * dC;
+            }
+        }
+        // block sum of the nine components
+        const int lane = tid & 31, wid = tid >> 5;
+        for (int k = 0; k < 9; k++) {
+            double x = gs[k];
+            for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+            if (lane == 0) red[k][wid] = x;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double tot[9];
+            for (int k = 0; k < 9; k++) {
+                tot[k] = 0.0;
+                for (int w2 = 0; w2 < (nt >> 5); w2++) tot[k] += red[k][w2];
+            }
+            const int4 bs = __ldg(X.pair_sh + q.bra), ks = __ldg(X.pair_sh + q.ket);
+            const int A = __ldg(X.shell_atom + bs.x), B = __ldg(X.shell_atom + bs.y);
+            const int C = __ldg(X.shell_atom + ks.x), D = __ldg(X.shell_atom + ks.y);
+            if (!(A == B && A == C && A == D)) {   // translational invariance: sums to zero
+                for (int i = 0; i < 3; i++) {
+                    atomicAdd(X.grad + 3 * A + i, q.w * tot[i]);
+                    atomicAdd(X.grad + 3 * B + i, q.w * tot[3 + i]);
+                    atomicAdd(X.grad + 3 * C + i, q.w * tot[6 + i]);
+                    atomicAdd(X.grad + 3 * D + i, -q.w * (tot[i] + tot[3 + i] + tot[6 + i]));
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+static void* g_grad_scratch = nullptr;
+static size_t g_grad_scratch_bytes = 0;
+
+void generic_release()
+{
+    if (g_grad_scratch) cudaFree(g_grad_scratch);
+    g_grad_scratch = nullptr;
+    g_grad_scratch_bytes = 0;
+}
+
+int launch_generic_grad_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, const GradExtra& X, int nq,
+                              int nsm, cudaStream_t st)
+{
+    if (nq <= 0) return 0;
+    const int elo = la > 0 ? la - 1 : 0, flo = lc > 0 ? lc - 1 : 0;
+    const GenCached* gc = gen_cached(elo, la + lb + 1 - elo, flo, lc + ld + 1 - flo, true);
+    if (!gc) return -1;
+    GenGradInfo I{la, lb, lc, ld, elo, flo, gc->G.ne, gc->G.nf, 0};
+    I.per_block = (long long)gc->G.total + 3LL * I.ne * I.nf;
+    // scratch of at most 256 MB: four blocks per SM where it allows
+    const long long budget = (256LL << 20) / (long long)sizeof(double);
+    const long long grid = std::max(1LL, std::min<long long>({(long long)nq, 4LL * nsm, budget / I.per_block}));
+    const size_t need = (size_t)grid * (size_t)I.per_block * sizeof(double);
+    if (need > g_grad_scratch_bytes) {
+        generic_release();
+        if (cudaMalloc(&g_grad_scratch, need) != cudaSuccess) {
+            g_grad_scratch = nullptr;
+            return -1;
+        }
+        g_grad_scratch_bytes = need;
+    }
+    QB_LAUNCH(grad_generic_kernel, (int)grid, 128, 0, st, P, X, cls, gc->G, gc->R, I, (double*)g_grad_scratch);
+    return 128;
 }
 
 }  // namespace qb

@@ -53,6 +53,10 @@ int class_max_group(int cls);
 int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm, int fp32_list,
                          cudaStream_t st);
 int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int GS, int nq, int nsm, cudaStream_t st);
+// The gradient of a class with an f shell (eri_generic.cu); -1 if its scratch cannot be allocated.
+int launch_generic_grad_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, const GradExtra& X, int nq,
+                              int nsm, cudaStream_t st);
+void generic_release();
 int grad_max_group(int cls);
 int fma_probe(int fp64, int nsm, double* gflops, cudaStream_t st);
 void launch_count_prims(const FockParams& P, int ncls, unsigned long long* out, int nsm, cudaStream_t st);

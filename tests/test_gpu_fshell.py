@@ -1,8 +1,9 @@
 """f shells (cc-pVTZ: d on H, f on O): every class with an f shell runs the
-generic warp-per-quartet kernel (eri_generic.cu).  Fock matrices against the
-oracle (itself pinned to QUICK's CUDA_SPDF kernels where those are right,
+generic block-per-quartet kernels (eri_generic.cu).  Fock matrices and the
+two-electron gradient against the oracle (itself pinned to QUICK's CUDA_SPDF
+kernels where those are right and to finite differences,
 tests/test_oracle_fshell.py) at 1e-8; Schwarz bounds for f pair types on the
-GPU; f shells have no gradient kernel and say so."""
+GPU."""
 import numpy as np
 import pytest
 
@@ -75,12 +76,17 @@ def test_fshell_schwarz_bounds_on_gpu(session, oracle_lib):
     np.testing.assert_allclose(session.cutPrim, cpo, rtol=1e-9, atol=1e-30)
 
 
-def test_fshell_gradient_reports_missing_kernel(session, oracle_lib):
-    from quick_b200 import capi
-    m, b = _mol((1, 1, 1))
+@pytest.mark.parametrize("grid", [(1, 1, 1), (2, 1, 1)])
+def test_fshell_gradient_matches_oracle(session, oracle_lib, grid):
+    """The generic f-class gradient kernel (with the straight-line s/p/d
+    gradient classes) against the oracle's two-electron gradient: 1e-8
+    Eh/bohr absolute on gradients of order 1e2."""
+    m, b = _mol(grid)
     Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
     session.upload_molecule(m, b, Y, cp)
     D = random_density(b.nbasis, seed=5, scale=0.05)
     cm = oracle_lib.cutmatrix(b, D)
-    with pytest.raises(capi.QuickB200Error, match="f shells"):
-        session.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
+    session.get2e(np.zeros((b.nbasis, b.nbasis), order="F"), D, cm, 1e-10, 1e-20, method=0)
+    got = session.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
+    ref = oracle_lib.grad2e(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
+    assert np.abs(got - ref).max() < TOL

@@ -122,3 +122,28 @@ def test_quick_fd_ff_zones_are_not_rotationally_covariant():
         oracle.ref_upload_molecule(mol, b, Y, cp, threads=8, spdf="boys")
         return oracle.ref_get2e(Z, Dm, oracle.cutmatrix(b, Dm), 1e-12, 1e-20, spdf="boys")
     assert _rotation_error(fock, m, b, D) > 1e-2
+
+
+def test_oracle_fshell_gradient_matches_finite_differences(oracle_lib):
+    """The oracle's two-electron gradient with f shells (cc-pVTZ water)
+    against central differences (h = 1e-4 bohr) of E2 = Tr[D G(D)]/2 with the
+    density held fixed: the reference the GPU's f-class gradient is held to."""
+    from tests.helpers import random_density
+    m = water_cluster((1, 1, 1), seed=0)
+    b = build_basis(m.symbols, "cc-pVTZ")
+    D = random_density(b.nbasis, seed=5, scale=0.05)
+    cut, plim = 1e-14, 1e-30
+    X = m.xyz_bohr.copy()
+    Y, cp = oracle_lib.schwarz(b, X)
+    cm = oracle_lib.cutmatrix(b, D)
+    g = oracle_lib.grad2e(b, X, Y, cp, cm, D, cut, plim)
+    h = 1e-4
+    for k in (0, 4, 8):
+        xs = []
+        for sgn in (1, -1):
+            v = X.ravel(order="F").copy()
+            v[k] += sgn * h
+            Xd = np.asfortranarray(v.reshape(3, -1, order="F"))
+            Yd, cpd = oracle_lib.schwarz(b, Xd)
+            xs.append(oracle_lib.energy2e(b, Xd, Yd, cpd, cm, D, cut, plim))
+        assert abs((xs[0] - xs[1]) / (2 * h) - g[k]) < 1e-6
