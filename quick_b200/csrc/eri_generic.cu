@@ -693,6 +693,7 @@ struct GenGradInfo {
     int elo, flo;           // lowest |e|, |f| held in the sums
     int ne, nf;             // extents of the sums (rows |e| in [elo, LA+LB+1], columns |f| in [flo, LC+LD+1])
     long long per_block;    // scratch doubles per block
+    long long x_off[5];     // ket-transformed sums: 2a (c,d), 1 (c,d), 2b (c,d), 2g (c+1,d), 1 (c-1,d)
 };
 
 __device__ __forceinline__ int gen_gidx(int x, int y, int z, int lo)
@@ -701,40 +702,51 @@ __device__ __forceinline__ int gen_gidx(int x, int y, int z, int lo)
     return g_ncum(n - 1) - g_ncum(lo - 1) + t * (t + 1) / 2 + z;
 }
 
-__device__ __forceinline__ double gen_ipow(double b, int e)
+__constant__ int kBinomD[6][6] = {{1}, {1, 1}, {1, 2, 1}, {1, 3, 3, 1}, {1, 4, 6, 4, 1}, {1, 5, 10, 10, 5, 1}};
+
+// canonical index of (x, y, z) inside its shell, and back
+__device__ __forceinline__ int gen_canon(int y, int z) { const int t = y + z; return t * (t + 1) / 2 + z; }
+__device__ __forceinline__ void gen_uncanon(int l, int idx, int* e)
 {
-    double r = 1.0;
-    for (int i = 0; i < e; i++) r *= b;
-    return r;
+    int t = 0;
+    while ((t + 1) * (t + 2) / 2 <= idx) t++;
+    e[2] = idx - t * (t + 1) / 2;
+    e[1] = t - e[2];
+    e[0] = l - t;
 }
 
-__device__ __forceinline__ int gen_binom(int n, int k)
+// X[row][c d] = sum_kd C(d,kd) CD^(d-kd) E[row][c+kd] for every row of the
+// sums, c in shell lcx, d in shell ld (canonical order).  CDp[3][8]: powers.
+__device__ void gen_ket_transform(const double* E, double* X, const GenGradInfo& I, int lcx, int ldx,
+                                  const double* CDp, int tid, int nt)
 {
-    int r = 1;
-    for (int j = 1; j <= k; j++) r = r * (n - k + j) / j;
-    return r;
+    const int ncx = g_ncart(lcx), ndx = g_ncart(ldx), cols = ncx * ndx;
+    for (int t = tid; t < I.ne * cols; t += nt) {
+        const int row = t / cols, col = t - row * cols;
+        int c[3], d[3];
+        gen_uncanon(lcx, col / ndx, c);
+        gen_uncanon(ldx, col % ndx, d);
+        const double* Er = E + (size_t)row * I.nf;
+        double v = 0.0;
+        for (int kx = 0; kx <= d[0]; kx++)
+            for (int ky = 0; ky <= d[1]; ky++)
+                for (int kz = 0; kz <= d[2]; kz++)
+                    v += kBinomD[d[0]][kx] * kBinomD[d[1]][ky] * kBinomD[d[2]][kz] * CDp[d[0] - kx] *
+                         CDp[8 + d[1] - ky] * CDp[16 + d[2] - kz] * Er[gen_gidx(c[0] + kx, c[1] + ky, c[2] + kz, I.flo)];
+        X[t] = v;
+    }
 }
 
-// (a b|c d) = sum_kb sum_kd C(b,kb) AB^(b-kb) C(d,kd) CD^(d-kd) E[a+kb][c+kd]
-__device__ double gen_hrr2(const double* E, const GenGradInfo& I, const int* a, const int* b, const int* c,
-                           const int* d, const double* AB, const double* CD)
+// sum_kb C(b,kb) AB^(b-kb) X[a+kb][col]
+__device__ __forceinline__ double gen_bra_sum(const double* X, int cols, int col, const int* a, const int* b,
+                                              const GenGradInfo& I, const double* ABp)
 {
     double s = 0.0;
     for (int kx = 0; kx <= b[0]; kx++)
         for (int ky = 0; ky <= b[1]; ky++)
-            for (int kz = 0; kz <= b[2]; kz++) {
-                const double cb = gen_binom(b[0], kx) * gen_binom(b[1], ky) * gen_binom(b[2], kz) *
-                                  gen_ipow(AB[0], b[0] - kx) * gen_ipow(AB[1], b[1] - ky) * gen_ipow(AB[2], b[2] - kz);
-                const double* row = E + (size_t)gen_gidx(a[0] + kx, a[1] + ky, a[2] + kz, I.elo) * I.nf;
-                double t = 0.0;
-                for (int lx = 0; lx <= d[0]; lx++)
-                    for (int ly = 0; ly <= d[1]; ly++)
-                        for (int lz = 0; lz <= d[2]; lz++)
-                            t += gen_binom(d[0], lx) * gen_binom(d[1], ly) * gen_binom(d[2], lz) *
-                                 gen_ipow(CD[0], d[0] - lx) * gen_ipow(CD[1], d[1] - ly) * gen_ipow(CD[2], d[2] - lz) *
-                                 row[gen_gidx(c[0] + lx, c[1] + ly, c[2] + lz, I.flo)];
-                s += cb * t;
-            }
+            for (int kz = 0; kz <= b[2]; kz++)
+                s += kBinomD[b[0]][kx] * kBinomD[b[1]][ky] * kBinomD[b[2]][kz] * ABp[b[0] - kx] * ABp[8 + b[1] - ky] *
+                     ABp[16 + b[2] - kz] * X[(size_t)gen_gidx(a[0] + kx, a[1] + ky, a[2] + kz, I.elo) * cols + col];
     return s;
 }
 
@@ -818,11 +830,33 @@ __global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, c
                 }
             }
         }
-        // derivative integrals contracted with the density products
-        const double AB[3] = {q.ABx, q.ABy, q.ABz}, CD[3] = {q.CDx, q.CDy, q.CDz};
+        // derivative integrals contracted with the density products: the ket
+        // side of the transfer once per sum, then short bra sums per integral
+        __shared__ double ABp[24], CDp[24];
+        if (tid < 48) {
+            const double base = tid < 24 ? (tid < 8 ? q.ABx : (tid < 16 ? q.ABy : q.ABz))
+                                         : (tid < 32 ? q.CDx : (tid < 40 ? q.CDy : q.CDz));
+            double v = 1.0;
+            for (int k = 0; k < (tid & 7); k++) v *= base;
+            if (tid < 24) ABp[tid] = v;
+            else CDp[tid - 24] = v;
+        }
+        __syncthreads();
+        double* XA = sm + I.x_off[0];
+        double* X1 = sm + I.x_off[1];
+        double* XB = sm + I.x_off[2];
+        double* XCp = sm + I.x_off[3];
+        double* XCm = sm + I.x_off[4];
+        gen_ket_transform(Ea, XA, I, I.lc, I.ld, CDp, tid, nt);
+        gen_ket_transform(E1, X1, I, I.lc, I.ld, CDp, tid, nt);
+        gen_ket_transform(Eb, XB, I, I.lc, I.ld, CDp, tid, nt);
+        gen_ket_transform(Ec, XCp, I, I.lc + 1, I.ld, CDp, tid, nt);
+        if (I.lc > 0) gen_ket_transform(E1, XCm, I, I.lc - 1, I.ld, CDp, tid, nt);
+        __syncthreads();
         const double* Dm = P.dense;
         const int nbf = P.nbasis;
         const double hx = P.hybrid;
+        const int ndd = nd, ccd = nc * nd, ccp = g_ncart(I.lc + 1) * nd, ccm = g_ncart(I.lc - 1) * nd;
         double gs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         const int nout = na * nb * nc * nd;
         for (int o = tid; o < nout; o += nt) {
@@ -844,27 +878,29 @@ __global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, c
             const double Dad = __ldg(Dm + (size_t)fa * nbf + fd), Dbc = __ldg(Dm + (size_t)fb * nbf + fc);
             const double g = 4.0 * Dab * Dcd - hx * (Dac * Dbd + Dad * Dbc);
             if (g == 0.0) continue;
+            const int dcan = gen_canon(d[1], d[2]);
+            const int colcd = gen_canon(c[1], c[2]) * ndd + dcan;
             for (int i = 0; i < 3; i++) {
                 int u[3] = {a[0], a[1], a[2]};
                 u[i]++;
-                double dA = gen_hrr2(Ea, I, u, b, c, d, AB, CD);
+                double dA = gen_bra_sum(XA, ccd, colcd, u, b, I, ABp);
                 if (a[i] > 0) {
                     u[i] -= 2;
-                    dA -= a[i] * gen_hrr2(E1, I, u, b, c, d, AB, CD);
+                    dA -= a[i] * gen_bra_sum(X1, ccd, colcd, u, b, I, ABp);
                 }
                 int v[3] = {b[0], b[1], b[2]};
                 v[i]++;
-                double dB = gen_hrr2(Eb, I, a, v, c, d, AB, CD);
+                double dB = gen_bra_sum(XB, ccd, colcd, a, v, I, ABp);
                 if (b[i] > 0) {
                     v[i] -= 2;
-                    dB -= b[i] * gen_hrr2(E1, I, a, v, c, d, AB, CD);
+                    dB -= b[i] * gen_bra_sum(X1, ccd, colcd, a, v, I, ABp);
                 }
                 int w[3] = {c[0], c[1], c[2]};
                 w[i]++;
-                double dC = gen_hrr2(Ec, I, a, b, w, d, AB, CD);
+                double dC = gen_bra_sum(XCp, ccp, gen_canon(w[1], w[2]) * ndd + dcan, a, b, I, ABp);
                 if (c[i] > 0) {
                     w[i] -= 2;
-                    dC -= c[i] * gen_hrr2(E1, I, a, b, w, d, AB, CD);
+                    dC -= c[i] * gen_bra_sum(XCm, ccm, gen_canon(w[1], w[2]) * ndd + dcan, a, b, I, ABp);
                 }
                 gs[i] += g * dA;
                 gs[3 + i] += g * dB;
@@ -918,8 +954,16 @@ int launch_generic_grad_class(int cls, int la, int lb, int lc, int ld, const Foc
     const int elo = la > 0 ? la - 1 : 0, flo = lc > 0 ? lc - 1 : 0;
     const GenCached* gc = gen_cached(elo, la + lb + 1 - elo, flo, lc + ld + 1 - flo, true);
     if (!gc) return -1;
-    GenGradInfo I{la, lb, lc, ld, elo, flo, gc->G.ne, gc->G.nf, 0};
-    I.per_block = (long long)gc->G.total + 3LL * I.ne * I.nf;
+    GenGradInfo I{la, lb, lc, ld, elo, flo, gc->G.ne, gc->G.nf, 0, {0, 0, 0, 0, 0}};
+    const long long nacc = (long long)I.ne * I.nf, ndd = g_ncart(ld);
+    const long long cols[5] = {g_ncart(lc) * ndd, g_ncart(lc) * ndd, g_ncart(lc) * ndd, g_ncart(lc + 1) * ndd,
+                               g_ncart(lc - 1) * ndd};
+    long long off = (long long)gc->G.total + 3 * nacc;
+    for (int k = 0; k < 5; k++) {
+        I.x_off[k] = off;
+        off += (long long)I.ne * cols[k];
+    }
+    I.per_block = off;
     // scratch of at most 256 MB: four blocks per SM where it allows
     const long long budget = (256LL << 20) / (long long)sizeof(double);
     const long long grid = std::max(1LL, std::min<long long>({(long long)nq, 4LL * nsm, budget / I.per_block}));
