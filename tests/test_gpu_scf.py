@@ -192,3 +192,23 @@ def test_kohn_sham_scf(method, name):
     assert g_d is None          # no exchange-correlation gradient on this path
     assert abs(r_h.energy - gold) < 1e-7
     assert abs(r_d.energy - gold) < 1e-7
+
+
+def test_fshell_full_gradient_vs_finite_differences():
+    """cc-pVTZ water (f on O): the full analytic RHF gradient through the
+    f-class gradient kernel against central differences (h = 1e-3 bohr) of
+    the SCF energy."""
+    import math
+    t = math.radians(103.0)
+    m = Molecule(["O", "H", "H"], np.array([[0, 0, 0], [0.97, 0, 0], [0.97 * math.cos(t), 0.97 * math.sin(t), 0]]))
+    b = build_basis(m.symbols, "cc-pVTZ")
+    r, g = _energy(m, b)
+    h = 1e-3
+    for atom, k in ((0, 0), (1, 1), (2, 0)):
+        e = []
+        for sgn in (1, -1):
+            x = m.xyz_angstrom.copy()
+            x[atom, k] += sgn * h / A_TO_BOHRS
+            e.append(_energy(Molecule(m.symbols, x), b)[0].energy)
+        fd = (e[0] - e[1]) / (2 * h)
+        assert abs(g[3 * atom + k] - fd) < 1e-6, (atom, k, g[3 * atom + k], fd)
