@@ -84,9 +84,10 @@ def build(lmax=2, jobs=None, verbose=False):
         for pre in ("eri_", "eri32_", "grad_"):
             if b.startswith(pre) and b[len(pre):len(pre) + 4].isdigit():
                 ls = [int(ch) for ch in b[len(pre):len(pre) + 4]]
-                # Fock classes: up to lmax, plus the f classes with L sum <= 6
-                # (gen_eri.py); gradient classes: up to lmax
-                if max(ls) > lmax and (pre == "grad_" or sum(ls) > 6):
+                # Fock classes: up to lmax, plus the f classes with L sum <= 6;
+                # gradient classes: up to lmax, plus the f classes with L sum
+                # <= 6 (gen_eri.py)
+                if max(ls) > lmax and sum(ls) > 6:
                     break
         else:
             keep.append(s)

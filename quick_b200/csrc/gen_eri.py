@@ -172,6 +172,7 @@ class HRR:
 # gradient classes with total angular momentum >= this get one kernel per
 # derivative centre (two accumulator sets each instead of four)
 GRAD_SPLIT_L = int(os.environ.get("QB_GRAD_SPLIT_L", "4"))
+GRAD_F_MAX_L = 6
 
 
 def grad_group_sizes(la, lb, lc, ld):
@@ -681,7 +682,10 @@ def main(outdir, lmax=2, lmax_all=3):
     # total angular momentum is at most 6 (the larger ones run the generic
     # kernel; their straight-line code would take hours to compile)
     cls = [c for c in cls_all if max(c) <= lmax or sum(c) <= 6]
-    cls_grad = classes(lmax)
+    # gradient: every class up to lmax, and the f classes with total angular
+    # momentum <= GRAD_F_MAX_L (the larger ones run the generic gradient
+    # kernel, eri_generic.cu, which is slow for the many small quartets)
+    cls_grad = [c for c in cls_all if max(c) <= lmax or sum(c) <= GRAD_F_MAX_L]
     lines = ["// generated by gen_eri.py", "#pragma once", "namespace qb {",
              "static const int kNumClasses = %d;" % len(cls_all),
              "static const int kClassL[%d][4] = {%s};" % (len(cls_all), ", ".join("{%d,%d,%d,%d}" % c for c in cls_all)),
