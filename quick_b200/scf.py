@@ -463,8 +463,8 @@ def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
                    mixed_cut=0.0, incremental=False, device=0, max_iter=100, method=0, session=None):
     """Energy and gradient with the device-resident SCF (DeviceRHF) from the
     SAD guess; atomic densities are cached per (element, basis).  Returns
-    (SCFResult, gradient or None); SCFResult.seconds covers guess, SCF and
-    gradient.  ``session``: an open capi.Session to upload into and keep
+    (SCFResult, gradient or None); SCFResult.seconds covers guess, set-up,
+    SCF and gradient (timings holds each, and the session close apart).  ``session``: an open capi.Session to upload into and keep
     open (molecule after molecule without re-initialising the library); by
     default a session is opened and closed around the call."""
     from .basis import build_basis
@@ -495,12 +495,15 @@ def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
         t4 = time.perf_counter()
         r.fock_builds = eng.nfock
     finally:
+        t5 = time.perf_counter()
         if own:
             s.close()
         else:
             # the engine's stream dies with it: hand the session back its own
             from .capi import lib
             lib().qb_set_stream(None)
-    r.seconds = time.perf_counter() - t0
-    r.timings = dict(guess=t1 - t0, setup=t2 - t1, scf=t3 - t2, gradient=t4 - t3)
+    # the work of one molecule; closing the session (freeing the library's
+    # device memory, which a long-lived session does once) is reported apart
+    r.seconds = t4 - t0
+    r.timings = dict(guess=t1 - t0, setup=t2 - t1, scf=t3 - t2, gradient=t4 - t3, close=time.perf_counter() - t5)
     return r, g
