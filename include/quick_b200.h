@@ -169,6 +169,14 @@ long long qb_xc_grid(double* xyzw, long long cap);
    out[3k+1] = df/drho, out[3k+2] = 4 df/dsigma (QUICK's b3lyp_e / b3lypf and becke/lyp). */
 int qb_xc_functional(int method, int n, const double* rho, const double* sigma, double* out);
 
+/* No counterpart in QUICK.  Autotunes the lanes per shell quartet of each straight-line Fock
+   class: after a Fock build (gpu_get2e_ or qb_fock_device), times every compiled lane-group
+   size of every class on that build's quartet lists (into a scratch matrix; the Fock matrix
+   is untouched) and keeps the fastest for the following builds of the same molecule (a new
+   gpu_upload_cutoff_matrix_ restores the default choice).  Writes the chosen sizes, one per
+   class, to groups (cap entries at most).  Synchronises the library stream. */
+int qb_autotune_classes(int* groups, int cap);
+
 /* Device form of gpu_upload_cutoff_: the integral and primitive cutoffs, and QUICK's density
    screen cutMatrix(I, J) = max |D| over the shell-pair block (densityCutoff / DNscreen,
    src/schwarz.f90:550-600) computed on the GPU from the device density d_dense (nbasis^2)

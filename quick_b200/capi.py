@@ -144,6 +144,14 @@ class Session:
         check()
         return g
 
+    def autotune(self):
+        """Time every lane-group size of every class on the last Fock build's
+        quartet lists and keep the fastest (qb_autotune_classes)."""
+        g = np.zeros(1024, dtype=np.int32)
+        lib().qb_autotune_classes(_ptr(g), 1024)
+        check()
+        return g
+
     def oneint(self):
         """(S, H): the overlap of fullx and the core Hamiltonian of get1e."""
         n = self.nbasis

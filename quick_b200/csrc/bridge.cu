@@ -961,6 +961,55 @@ int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out)
     return fock_build(c, d_o_in, d_o_out);
 }
 
+// Per-class autotuning of the lanes per shell quartet: after a Fock build,
+// every compiled lane-group size of every straight-line class is timed on
+// that build's quartet lists (writing into a scratch Fock matrix), and the
+// fastest is kept for the following builds of this molecule.
+int qb_autotune_classes(int* groups, int cap)
+{
+    Context& c = ctx();
+    if (require(c.have_pairs && c.have_cutoff && c.d_quartets.p != nullptr,
+                "a Fock build must precede qb_autotune_classes"))
+        return 1;
+    const int n = c.nbasis;
+    DevBuf<double> scratch;
+    CK(scratch.alloc((size_t)n * n));
+    CK(cudaMemsetAsync(scratch.p, 0, (size_t)n * n * sizeof(double), c.stream));
+    FockParams P = fock_params(c);
+    P.fock = scratch.p;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int k = 0; k < kNumClasses; k++) {
+        const long long capk = c.screen_cls[k].capacity;
+        const int* Lk = kClassL[k];
+        if (capk == 0 || Lk[0] + Lk[1] + Lk[2] + Lk[3] >= c.generic_min_l || class_max_group(k) <= 1) continue;
+        const int nq = (int)std::min<long long>(capk, 1LL << 30);
+        int best_g = c.class_group[k];
+        float best_t = 1e30f;
+        for (int g = 1; g <= class_max_group(k); g *= 2) {
+            float tmin = 1e30f;
+            for (int rep = 0; rep < 2; rep++) {
+                CK(cudaEventRecord(e0, c.stream));
+                launch_class(k, P, g, nq, c.nsm, c.stream);
+                CK(cudaEventRecord(e1, c.stream));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                tmin = std::min(tmin, ms);
+            }
+            if (tmin < best_t) best_t = tmin, best_g = g;
+        }
+        c.class_group[k] = best_g;
+    }
+    CK(cudaGetLastError());
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    scratch.release();
+    for (int k = 0; k < std::min(cap, kNumClasses); k++) groups[k] = c.class_group[k];
+    return 0;
+}
+
 int qb_upload_cutoff_device(const double* d_dense, double integralCutoff, double primLimit)
 {
     Context& c = ctx();

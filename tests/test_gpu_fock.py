@@ -73,3 +73,28 @@ def test_schwarz_kernel_matches_oracle(session, oracle_lib, name):
     big = cpo > 1e-150
     assert np.array_equal(cp > 0, cpo > 0)
     assert np.max(np.abs(cp[big] - cpo[big]) / cpo[big]) < 1e-12
+
+
+def test_autotuned_lane_groups_keep_the_fock_matrix():
+    """qb_autotune_classes picks, per class, the fastest compiled lane-group
+    size on the last build's quartet lists; the Fock matrix after tuning
+    equals the one before (different summation order only: 1e-10)."""
+    from quick_b200 import capi
+    from quick_b200.molecule import water_cluster
+    from quick_b200.basis import build_basis
+    from quick_b200.scf import shell_cut_matrix
+    m = water_cluster((2, 2, 1), seed=1)
+    b = build_basis(m.symbols, "6-31G**")
+    s = capi.Session(0)
+    try:
+        s.upload_molecule(m, b)
+        D = random_density(b.nbasis, seed=2, scale=0.05)
+        cm = shell_cut_matrix(b, D)
+        O = np.zeros((b.nbasis, b.nbasis), order="F")
+        F0 = s.get2e(O, D, cm, 1e-10, 1e-20)
+        g = s.autotune()
+        F1 = s.get2e(O, D, cm, 1e-10, 1e-20)
+    finally:
+        s.close()
+    assert np.abs(F1 - F0).max() < 1e-10
+    assert set(int(x) for x in g if x) <= {1, 2, 4, 8, 16, 32}
