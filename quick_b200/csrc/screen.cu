@@ -7,11 +7,19 @@
 
 namespace qb {
 
-// One warp per (class, bra pair).  The kets of the class's ket type come in
-// segments of equal primitive count, each sorted by Schwarz bound,
-// descending, so the scan of a segment stops at the first ket whose bound
-// product fails.  count_only: Schwarz test only, just count (used once
-// per geometry to size the lists).
+// One warp per (class, tile of kScreenTile consecutive bra pairs).  The kets
+// of the class's ket type come in segments of equal primitive count, each
+// sorted by Schwarz bound, descending, so the scan of a segment stops at the
+// first chunk of kets whose bound product fails for every bra of the tile.
+// For each chunk of 32 kets the warp tests all bras of the tile and writes
+// their survivors as one contiguous run (bra by bra, kets ascending), so
+// the quartets that share a chunk of ket pairs sit next to each other in the
+// list: a class kernel block that walks a contiguous slice of the list
+// reads each ket pair's primitive data from L1 once per tile instead of once
+// per quartet.  count_only: Schwarz test only, just count (used once per
+// geometry to size the lists).
+constexpr int kScreenTile = 4;
+
 __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const FockParams P, int count_only)
 {
     const int cls = blockIdx.y;
@@ -20,52 +28,74 @@ __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const double cut = P.integral_cutoff;
-    for (int a = c.bra_begin + warp; a < c.bra_end; a += nwarps) {
-        const double Ya = P.pair_Y[a];
-        const int4 sa = P.pair_sh[a];
-        for (int sg = c.seg_begin; sg < c.seg_end; sg++) {
-        const int2 seg = P.ket_segs[sg];
-        if (c.same_type && seg.y <= a) continue;
-        const int kb = c.same_type ? max(a, seg.x) : seg.x;
-        for (int k0 = kb; k0 < seg.y; k0 += 32) {
-            if (!(P.pair_Y[k0] * Ya > cut)) break;      // sorted inside the segment: the rest fail too
-            const int b = k0 + lane;
-            bool pass = false, low = false;
-            if (b < seg.y) {
-                const double yy = P.pair_Y[b] * Ya;
-                if (yy > cut) {
-                    if (count_only) {
-                        pass = true;
-                    } else {
-                        const int4 sb = P.pair_sh[b];
-                        const double bound = yy * dn_max(P, sa.x, sa.y, sb.x, sb.y);
-                        pass = bound > cut;
-                        low = pass && bound < P.mixed_cut;
-                    }
-                }
-            }
-            const unsigned m = __ballot_sync(FULL, pass && !low);
-            const unsigned m32 = __ballot_sync(FULL, low);
-            if ((m | m32) == 0) continue;
-            unsigned long long base = 0, base32 = 0;
-            if (lane == 0) {
-                if (m) base = atomicAdd(S.counts + cls, (unsigned long long)__popc(m));
-                if (m32) base32 = atomicAdd(S.counts32 + cls, (unsigned long long)__popc(m32));
-            }
-            base = __shfl_sync(FULL, base, 0);
-            base32 = __shfl_sync(FULL, base32, 0);
-            if (!count_only && pass) {
-                const unsigned below = (1u << lane) - 1u;
-                if (!low) {
-                    const unsigned long long pos = base + __popc(m & below);
-                    if (pos < (unsigned long long)c.capacity) S.out[c.out_offset + pos] = make_int2(a, b);
-                } else {
-                    const unsigned long long pos = base32 + __popc(m32 & below);
-                    if (pos < (unsigned long long)c.capacity)
-                        S.out[c.out_offset + c.capacity - 1 - pos] = make_int2(a, b);
-                }
-            }
+    const unsigned below = (1u << lane) - 1u;
+    for (int a0 = c.bra_begin + warp * kScreenTile; a0 < c.bra_end; a0 += nwarps * kScreenTile) {
+        const int nt = min(kScreenTile, c.bra_end - a0);
+        double Ya[kScreenTile];
+        int4 sa[kScreenTile];
+        double Ymax = 0.0;
+#pragma unroll
+        for (int t = 0; t < kScreenTile; t++) {
+            Ya[t] = t < nt ? P.pair_Y[a0 + t] : 0.0;
+            sa[t] = t < nt ? P.pair_sh[a0 + t] : make_int4(0, 0, 0, 0);
+            Ymax = fmax(Ymax, Ya[t]);
         }
+        for (int sg = c.seg_begin; sg < c.seg_end; sg++) {
+            const int2 seg = P.ket_segs[sg];
+            if (c.same_type && seg.y <= a0) continue;   // every bra of the tile is >= a0
+            const int kb = c.same_type ? max(a0, seg.x) : seg.x;
+            for (int k0 = kb; k0 < seg.y; k0 += 32) {
+                if (!(P.pair_Y[k0] * Ymax > cut)) break;      // sorted inside the segment: the rest fail too
+                const int b = k0 + lane;
+                const double Yb = b < seg.y ? P.pair_Y[b] : 0.0;
+                int4 sb = make_int4(0, 0, 0, 0);
+                if (!count_only && b < seg.y) sb = P.pair_sh[b];
+                unsigned m[kScreenTile], m32[kScreenTile];
+                int tot = 0, tot32 = 0;
+#pragma unroll
+                for (int t = 0; t < kScreenTile; t++) {
+                    bool pass = false, low = false;
+                    // same pair type: kets b >= a only
+                    if (t < nt && b < seg.y && (!c.same_type || b >= a0 + t)) {
+                        const double yy = Yb * Ya[t];
+                        if (yy > cut) {
+                            if (count_only) {
+                                pass = true;
+                            } else {
+                                const double bound = yy * dn_max(P, sa[t].x, sa[t].y, sb.x, sb.y);
+                                pass = bound > cut;
+                                low = pass && bound < P.mixed_cut;
+                            }
+                        }
+                    }
+                    m[t] = __ballot_sync(FULL, pass && !low);
+                    m32[t] = __ballot_sync(FULL, low);
+                    tot += __popc(m[t]);
+                    tot32 += __popc(m32[t]);
+                }
+                if (tot + tot32 == 0) continue;
+                unsigned long long base = 0, base32 = 0;
+                if (lane == 0) {
+                    if (tot) base = atomicAdd(S.counts + cls, (unsigned long long)tot);
+                    if (tot32) base32 = atomicAdd(S.counts32 + cls, (unsigned long long)tot32);
+                }
+                if (count_only) continue;
+                base = __shfl_sync(FULL, base, 0);
+                base32 = __shfl_sync(FULL, base32, 0);
+#pragma unroll
+                for (int t = 0; t < kScreenTile; t++) {
+                    if ((m[t] >> lane) & 1u) {
+                        const unsigned long long pos = base + __popc(m[t] & below);
+                        if (pos < (unsigned long long)c.capacity) S.out[c.out_offset + pos] = make_int2(a0 + t, b);
+                    } else if ((m32[t] >> lane) & 1u) {
+                        const unsigned long long pos = base32 + __popc(m32[t] & below);
+                        if (pos < (unsigned long long)c.capacity)
+                            S.out[c.out_offset + c.capacity - 1 - pos] = make_int2(a0 + t, b);
+                    }
+                    base += __popc(m[t]);
+                    base32 += __popc(m32[t]);
+                }
+            }
         }
     }
 }
