@@ -106,8 +106,12 @@ def dist_setup():
         import torch
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        # NCCL between the GPUs; gloo where there are none (the CPU tests of
+        # this rank logic)
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
 
 
@@ -122,9 +126,16 @@ def max_over_ranks(x, ws):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def batch_sizes(nmol, rank):
+    """Cluster sizes n (uniform in 1..12) of one rank's molecules in the
+    batch line: seeded by rank, so every rank runs its own list."""
+    return np.random.default_rng(1234 + rank).integers(1, 13, size=nmol)
 
 
 def unique_quartets(b, Y, cm, cutoff):
@@ -484,9 +495,8 @@ def run_batch(args, ws, rank, local, nmol=None):
     from quick_b200.molecule import water_cluster_n
     torch.cuda.set_device(local)
     nmol = nmol or args.batch
-    rng = np.random.default_rng(1234)
-    sizes = rng.integers(1, 13, size=nmol)
-    mols = [water_cluster_n(int(k), seed=i) for i, k in enumerate(sizes)]
+    sizes = batch_sizes(nmol, rank)
+    mols = [water_cluster_n(int(k), seed=1000 * rank + i) for i, k in enumerate(sizes)]
     sess = capi.Session(local)
     try:
         scf.run_rhf_device(mols[0], "6-31G*", 1e-10, 1e-20, conv=1e-8, device=local, session=sess)   # warm-up
