@@ -7,11 +7,20 @@ in HBM.  Metric: shell quartets per second, a shell quartet being one
 Schwarz and density screens.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--part all|fock|xc|scf|batch]
 
 The default workload is (H2O)32 in 6-31G** (800 Cartesian basis functions),
 seeded geometry, CUTOFF=1e-10 semantics (integral cutoff 1e-10, primitive
 limit 1e-20).  For N > 1 every rank builds the Fock matrix of its own replica
 (weak scaling, no collective on the data path); the time is the max over ranks.
+
+The one JSON line also carries: the same build end to end through the host
+entry points (e2e), replayed from a CUDA graph, and with the mixed FP32/FP64
+split; the two-electron gradient; the XC quadrature (xc); SCF + gradient
+seconds per molecule, all-FP64 and mixed, with full and delta-D Fock builds,
+plus a Kohn-Sham and a cc-pVTZ case (scf); molecules per second for many
+small clusters (batch); and the CPU baseline, QUICK's own kernel compiled for
+the host cores.
 """
 import argparse
 import json
