@@ -118,10 +118,14 @@ int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out)
    and takes its working memory from one fixed 64 MiB array compiled into the library, present
    on every GPU that loads it until the process exits.  Molecules whose density, Fock
    accumulator and screened quartet lists do not fit are rejected with an error (use
-   qb_fock_device).  The first call on a device looks up the array's device address and
-   should come before any stream capture.  Calls share the array: calls that overlap on the GPU
-   race and must not be made.  Tables uploaded earlier (gpu_upload_basis_,
-   gpu_upload_cutoff_matrix_, gpu_upload_cutoff_) are used as they are. */
+   qb_fock_device).  The device programs of the f-shell classes that run the generic kernel
+   are copied into the same array.  The first call on a device looks up the array's device
+   address (with the session's device current).  Every call waits for the library stream twice
+   and copies the class counts to host memory, so no call can be recorded into a CUDA graph.
+   Every quartet runs in FP64: the mixed split of qb_set_mixed_precision is not applied here.
+   Calls share the array: calls that overlap on the GPU race and must not be made.  Tables
+   uploaded earlier (gpu_upload_basis_, gpu_upload_cutoff_matrix_, gpu_upload_cutoff_) are used
+   as they are. */
 int qb_fock_device_static(const double* d_dense, const double* d_o_in, double* d_o_out);
 
 /* Statistics of the last Fock build: unique shell quartets evaluated (one per unordered pair of

@@ -5,7 +5,10 @@ The sources are read where they lie in the QUICK tree (``src/cuda``); the
 shim in ``oracle/ref_shim`` supplies a host stand-in for the CUDA runtime and
 the launch geometry.  Build outputs go to ``oracle/_ref`` only.
 
-    python oracle/build_ref.py [--quick-root /root/reference] [--spdf] [--accurate-boys]
+    python oracle/build_ref.py [--quick-root DIR] [--spdf] [--accurate-boys]
+
+The QUICK tree is DIR, else the environment variable QUICK_ROOT, else
+/root/reference (quick_root()).
 """
 import argparse
 import os
@@ -18,6 +21,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SHIM = os.path.join(HERE, "ref_shim")
 OUT = os.path.join(HERE, "_ref")
 CUDA_INC = "/usr/local/cuda/include"
+DEFAULT_QUICK_ROOT = "/root/reference"
+
+
+def quick_root():
+    """The QUICK source tree: $QUICK_ROOT, else the default location."""
+    return os.environ.get("QUICK_ROOT") or DEFAULT_QUICK_ROOT
 
 
 def build(quick_root, spdf=False, accurate_boys=False, jobs=8, opt="-O2"):
@@ -89,8 +98,8 @@ def build(quick_root, spdf=False, accurate_boys=False, jobs=8, opt="-O2"):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--quick-root", default="/root/reference")
+    ap.add_argument("--quick-root", default=None)
     ap.add_argument("--spdf", action="store_true")
     ap.add_argument("--accurate-boys", action="store_true")
     a = ap.parse_args()
-    print(build(a.quick_root, a.spdf or a.accurate_boys, a.accurate_boys))
+    print(build(a.quick_root or quick_root(), a.spdf or a.accurate_boys, a.accurate_boys))

@@ -746,6 +746,7 @@ void gpu_shutdown_(void)
     xc_release();
     oneint_release();
     generic_release();
+    noalloc_reset();
     c.d_S1.release();
     c.d_H1.release();
     c.d_D1.release();
@@ -1538,6 +1539,8 @@ int session_view(SessionView* v)
     v->group = c.class_group;
     v->cons = c.d_cons.p;
     v->nsm = c.nsm;
+    v->dev_id = c.dev_id;
+    v->generic_min_l = c.generic_min_l;
     v->stream = c.stream;
     return 0;
 }

@@ -555,6 +555,56 @@ __global__ void __launch_bounds__(32) schwarz_generic_kernel(const SchwarzParams
 }
 
 // ------------------------------------------------------------ launch
+// The host-side program of one class, built once per process.
+struct GenHost {
+    GenLayout G;
+    GenProgramHost H;
+    size_t bytes = 0;     // its device image, every array 256-byte aligned
+};
+
+static size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static const GenHost* gen_host(int la, int lb, int lc, int ld, bool grad)
+{
+    static std::map<int, GenHost> cache;
+    const int key = grad ? (1 << 24) + (((la * 8 + lb) * 8 + lc) * 8 + ld) : ((la * 4 + lb) * 4 + lc) * 4 + ld;
+    auto it = cache.find(key);
+    if (it != cache.end()) return &it->second;
+    GenHost h;
+    h.G = gen_layout(la, lb, lc, ld);
+    gen_program(h.G, h.H, !grad);
+    const GenProgramHost& H = h.H;
+    h.bytes = up256(H.stage.size() * sizeof(int)) + up256(H.meta.size() * sizeof(int)) +
+              up256(H.ent.size() * sizeof(int4)) + up256(H.kterm.size() * sizeof(int4)) +
+              up256(H.bterm.size() * sizeof(int4)) + up256(H.kstart.size() * sizeof(int)) +
+              up256(H.bstart.size() * sizeof(int));
+    return &(cache[key] = std::move(h));
+}
+
+// Copies the program into device memory at mem (256-byte aligned, at least
+// h.bytes) on stream st and returns the device view of it.
+static int gen_place(const GenHost& h, void* mem, cudaStream_t st, GenProgram* R)
+{
+    char* p = (char*)mem;
+    bool ok = true;
+    auto put = [&](const void* src, size_t bytes) {
+        void* dst = p;
+        if (bytes) ok = ok && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+        p += up256(bytes);
+        return dst;
+    };
+    const GenProgramHost& H = h.H;
+    R->stage = (const int*)put(H.stage.data(), H.stage.size() * sizeof(int));
+    R->nstage = (int)H.stage.size() / 3;
+    R->meta = (const int*)put(H.meta.data(), H.meta.size() * sizeof(int));
+    R->ent = (const int4*)put(H.ent.data(), H.ent.size() * sizeof(int4));
+    R->kterm = (const int4*)put(H.kterm.data(), H.kterm.size() * sizeof(int4));
+    R->bterm = (const int4*)put(H.bterm.data(), H.bterm.size() * sizeof(int4));
+    R->kstart = (const int*)put(H.kstart.data(), H.kstart.size() * sizeof(int));
+    R->bstart = (const int*)put(H.bstart.data(), H.bstart.size() * sizeof(int));
+    return ok ? 0 : -1;
+}
+
 struct GenCached {
     GenLayout G;
     GenProgram R;
@@ -563,7 +613,8 @@ struct GenCached {
 };
 
 // grad: the layout and recurrence program of the extended range of the
-// gradient kernel (shells may exceed f; no horizontal terms).
+// gradient kernel (shells may exceed f; no horizontal terms).  The device
+// copy lives in memory of its own, one per class and device.
 static GenCached* gen_cached(int la, int lb, int lc, int ld, bool grad = false)
 {
     static std::map<int, GenCached> cache;
@@ -573,43 +624,24 @@ static GenCached* gen_cached(int la, int lb, int lc, int ld, bool grad = false)
                          : ((la * 4 + lb) * 4 + lc) * 4 + ld + 256 * dev;
     auto it = cache.find(key);
     if (it != cache.end()) return &it->second;
+    const GenHost* h = gen_host(la, lb, lc, ld, grad);
     GenCached c;
-    c.G = gen_layout(la, lb, lc, ld);
-    GenProgramHost H;
-    gen_program(c.G, H, !grad);
-    const size_t b_stage = H.stage.size() * sizeof(int), b_meta = H.meta.size() * sizeof(int);
-    const size_t b_ent = H.ent.size() * sizeof(int4), b_kt = H.kterm.size() * sizeof(int4),
-                 b_bt = H.bterm.size() * sizeof(int4);
-    const size_t b_ks = H.kstart.size() * sizeof(int), b_bs = H.bstart.size() * sizeof(int);
-    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t total = up(b_stage) + up(b_meta) + up(b_ent) + up(b_kt) + up(b_bt) + up(b_ks) + up(b_bs);
-    if (cudaMalloc(&c.mem, total) != cudaSuccess) return nullptr;
-    char* p = (char*)c.mem;
-    auto put = [&](const void* src, size_t bytes) {
-        void* dst = p;
-        if (bytes) cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
-        p += up(bytes);
-        return dst;
-    };
-    c.R.stage = (const int*)put(H.stage.data(), b_stage);
-    c.R.nstage = (int)H.stage.size() / 3;
-    c.R.meta = (const int*)put(H.meta.data(), b_meta);
-    c.R.ent = (const int4*)put(H.ent.data(), b_ent);
-    c.R.kterm = (const int4*)put(H.kterm.data(), b_kt);
-    c.R.bterm = (const int4*)put(H.bterm.data(), b_bt);
-    c.R.kstart = (const int*)put(H.kstart.data(), b_ks);
-    c.R.bstart = (const int*)put(H.bstart.data(), b_bs);
+    c.G = h->G;
+    if (cudaMalloc(&c.mem, h->bytes) != cudaSuccess) return nullptr;
+    if (gen_place(*h, c.mem, 0, &c.R) != 0 || cudaStreamSynchronize(0) != cudaSuccess) {
+        cudaFree(c.mem);
+        return nullptr;
+    }
     c.dev = dev;
     return &(cache[key] = c);
 }
 
-int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm, int fp32_list,
-                         cudaStream_t st)
+size_t generic_program_bytes(int la, int lb, int lc, int ld) { return gen_host(la, lb, lc, ld, false)->bytes; }
+
+// Shared-memory bytes, opt-in attribute and grid of one generic launch.
+static int generic_launch_shape(const GenLayout& G, int nq, int nsm, int* nt_out, size_t* bytes_out, int* grid_out)
 {
-    if (nq <= 0) return 0;
-    const GenCached* gc = gen_cached(la, lb, lc, ld);
-    if (!gc) return -1;
-    const size_t bytes = (size_t)gc->G.total * sizeof(double);
+    const size_t bytes = (size_t)G.total * sizeof(double);
     int dev = 0, maxsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -629,7 +661,39 @@ int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockPara
     }();
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fock_generic_kernel, nt, bytes);
-    const int grid = std::max(1, std::min(nq, nsm * std::max(per_sm, 1)));
+    *nt_out = nt;
+    *bytes_out = bytes;
+    *grid_out = std::max(1, std::min(nq, nsm * std::max(per_sm, 1)));
+    return 0;
+}
+
+// launch_generic_class with the class program copied into caller memory
+// (mem, 256-byte aligned, at least generic_program_bytes of the class) on
+// the launch stream instead of memory of its own: allocates nothing.
+int launch_generic_class_placed(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm,
+                                void* mem, size_t cap, cudaStream_t st)
+{
+    if (nq <= 0) return 0;
+    const GenHost* h = gen_host(la, lb, lc, ld, false);
+    if (h->bytes > cap) return -2;
+    int nt = 0, grid = 0;
+    size_t bytes = 0;
+    if (generic_launch_shape(h->G, nq, nsm, &nt, &bytes, &grid)) return -1;
+    GenProgram R;
+    if (gen_place(*h, mem, st, &R)) return -3;
+    QB_LAUNCH(fock_generic_kernel, grid, nt, bytes, st, P, cls, h->G, R, 0);
+    return nt;
+}
+
+int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm, int fp32_list,
+                         cudaStream_t st)
+{
+    if (nq <= 0) return 0;
+    const GenCached* gc = gen_cached(la, lb, lc, ld);
+    if (!gc) return -1;
+    int nt = 0, grid = 0;
+    size_t bytes = 0;
+    if (generic_launch_shape(gc->G, nq, nsm, &nt, &bytes, &grid)) return -1;
     QB_LAUNCH(fock_generic_kernel, grid, nt, bytes, st, P, cls, gc->G, gc->R, fp32_list);
     return nt;
 }

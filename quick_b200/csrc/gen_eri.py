@@ -692,6 +692,9 @@ def main(outdir, lmax=2, lmax_all=3):
              "static const int kNumPairTypes = %d;" % len(pair_types(lmax_all)),
              "static const int kPairTypeL[%d][2] = {%s};" % (len(pair_types(lmax_all)), ", ".join("{%d,%d}" % p for p in pair_types(lmax_all))),
              "static const int kGeneratedLmax = %d;   // classes above run the generic kernel" % lmax,
+             "// 1: the class has no straight-line kernel and runs the generic one (eri_generic.cu)",
+             "static const int kClassGeneric[%d] = {%s};" % (
+                 len(cls_all), ", ".join("0" if c in set(cls) else "1" for c in cls_all)),
              "}"]
     with open(os.path.join(outdir, "eri_classes.h"), "w") as fh:
         fh.write("\n".join(lines) + "\n")

@@ -6,17 +6,20 @@
 // between its set-up and its timed region.
 //
 // The working memory (per-class counters and offsets, the cons-scaled
-// density, the Fock accumulator and the quartet lists) lives in
+// density, the Fock accumulator, the device programs of the f-shell classes
+// that run the generic kernel, and the quartet lists) lives in
 // g_fock_scratch below: kFockScratchBytes on every GPU that loads the
 // library, held until the process exits.  Host code cannot use the array's
 // name as a device address (on the host it names a stand-in), so the device
-// address is fetched once per device with cudaGetSymbolAddress, with that
-// device current, on the first call made on it.  That first call should
-// therefore come before any stream capture.
+// address is fetched once per device with cudaGetSymbolAddress, with the
+// session's device current, on the first call made on it.
 //
 // Every call shares the one array and it keeps the last call's contents;
 // each call clears what must start at zero.  Calls that overlap on the GPU
 // (other host threads, other streams) race on it and must not be made.
+// Every quartet runs in FP64 here (the mixed split of qb_set_mixed_precision
+// is not applied), and each call waits for its stream twice (for the class
+// counts), so a call cannot be recorded into a CUDA graph.
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
@@ -56,12 +59,19 @@ static int fail(int code, const char* fmt, ...)
 
 using namespace qb;
 
+void qb::noalloc_reset()
+{
+    for (auto& p : g_scratch_addr) p = nullptr;
+}
+
 extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in, double* d_o_out)
 {
     SessionView v;
     if (int rc = session_view(&v)) return rc;
     int dev = 0;
     CKS(cudaGetDevice(&dev));
+    if (dev != v.dev_id)
+        return fail(1, "qb_fock_device_static: device %d is current but the session runs on device %d", dev, v.dev_id);
     if (dev < 0 || dev >= kMaxDevices) return fail(1, "qb_fock_device_static: device %d out of range", dev);
     if (!g_scratch_addr[dev]) {
         void* p = nullptr;
@@ -88,8 +98,6 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
     if (off > kFockScratchBytes)
         return fail(4, "qb_fock_device_static: %d basis functions need %zu bytes of working memory before any "
                        "quartet; the fixed array holds %zu bytes (use qb_fock_device)", n, off, kFockScratchBytes);
-    auto* quartets = (int2*)(base + off);
-    const long long qcap = (long long)((kFockScratchBytes - off) / sizeof(int2));
     cudaStream_t st = v.stream;
 
     // Schwarz-only count per class: an upper bound for any density
@@ -100,12 +108,32 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
     CKS(cudaMemsetAsync(counts32, 0, ncls * sizeof(unsigned long long), st));
     FockParams P = v.P;
     P.mixed_cut = 0.0;   // every quartet in FP64 here
-    ScreenParams S{d_cls, counts, quartets, counts32};
+    ScreenParams S{d_cls, counts, nullptr, counts32};
     launch_screen(S, P, ncls, 1, v.nsm, st);
     CKS(cudaGetLastError());
     std::vector<unsigned long long> cnt(ncls);
     CKS(cudaMemcpyAsync(cnt.data(), counts, ncls * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CKS(cudaStreamSynchronize(st));
+
+    // the kernel each class runs, chosen as fock_build chooses it, and the
+    // device programs of the classes that run the generic kernel
+    std::vector<int> generic(ncls, 0);
+    std::vector<unsigned char*> prog(ncls, nullptr);
+    std::vector<size_t> prog_bytes(ncls, 0);
+    for (int k = 0; k < ncls; k++) {
+        const int* L = kClassL[k];
+        generic[k] = kClassGeneric[k] || L[0] + L[1] + L[2] + L[3] >= v.generic_min_l;
+        if (!generic[k] || cnt[k] == 0) continue;
+        prog_bytes[k] = generic_program_bytes(L[0], L[1], L[2], L[3]);
+        prog[k] = take(prog_bytes[k]);
+    }
+    if (off > kFockScratchBytes)
+        return fail(4, "qb_fock_device_static: %d basis functions and the f-shell class programs need %zu bytes "
+                       "before any quartet; the fixed array holds %zu bytes (use qb_fock_device)", n, off,
+                    kFockScratchBytes);
+    auto* quartets = (int2*)(base + off);
+    const long long qcap = (long long)((kFockScratchBytes - off) / sizeof(int2));
+
     std::vector<long long> offs(ncls);
     long long total = 0;
     for (int k = 0; k < ncls; k++) {
@@ -133,6 +161,7 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
     P.class_end = nullptr;   // read only by the FP32 class kernels, which are not launched here
     P.dense = dense;
     P.fock = fock;
+    S.out = quartets;
     launch_screen(S, P, ncls, 0, v.nsm, st);
     launch_finish_counts(S, class_count, class_count32, overflow, ncls, st);
     CKS(cudaGetLastError());
@@ -144,7 +173,14 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
     if (ovf) return fail(3, "qb_fock_device_static: quartet list overflow (internal sizing error)");
     for (int k = 0; k < ncls; k++) {
         if (ccount[k] == 0) continue;
-        launch_class(k, P, v.group.empty() ? 1 : v.group[k], ccount[k], v.nsm, st);
+        const int* L = kClassL[k];
+        const int rc = generic[k]
+                           ? launch_generic_class_placed(k, L[0], L[1], L[2], L[3], P, ccount[k], v.nsm, prog[k],
+                                                         prog_bytes[k], st)
+                           : launch_class(k, P, v.group.empty() ? 1 : v.group[k], ccount[k], v.nsm, st);
+        if (rc < 0)
+            return fail(5, "qb_fock_device_static: class (%d%d|%d%d) could not be launched (%d)", L[0], L[1], L[2],
+                        L[3], rc);
     }
     CKS(cudaGetLastError());
     launch_fock_finish(fock, v.cons, d_o_in, d_o_out, n, st);

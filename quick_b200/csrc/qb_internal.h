@@ -29,6 +29,8 @@ struct SessionView {
     std::vector<int> group;             // lanes per shell quartet of each class kernel
     const double* cons;
     int nsm;
+    int dev_id;                         // the session's device
+    int generic_min_l;                  // classes with L sum >= this run the generic kernel (as fock_build)
     cudaStream_t stream;
 };
 int session_view(SessionView* v);
@@ -52,6 +54,15 @@ int class_max_group(int cls);
 // shared memory than the GPU offers.
 int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm, int fp32_list,
                          cudaStream_t st);
+// Device bytes of the generic kernel's program of class (la lb|lc ld), and
+// launch_generic_class with that program copied into caller memory (mem,
+// 256-byte aligned, cap bytes) instead of memory of its own; -2 if cap is
+// too small, -1 if the class needs more shared memory than the GPU offers.
+size_t generic_program_bytes(int la, int lb, int lc, int ld);
+int launch_generic_class_placed(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm,
+                                void* mem, size_t cap, cudaStream_t st);
+// Forget the fixed-array addresses of qb_fock_device_static (session end).
+void noalloc_reset();
 int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int GS, int nq, int nsm, cudaStream_t st);
 // The gradient of a class with an f shell (eri_generic.cu); -1 if its scratch cannot be allocated.
 int launch_generic_grad_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, const GradExtra& X, int nq,

@@ -9,7 +9,7 @@ coefficients as the decimal strings of the file, so that parsing them later
 gives bit-identical doubles to what QUICK's list-directed ``read`` sees.
 
 Usage (only where the QUICK tree is present):
-    python quick_b200/data/make_basis.py /path/to/quick/basis
+    python quick_b200/data/make_basis.py QUICK_ROOT   (or with $QUICK_ROOT set)
 """
 import json
 import os
@@ -70,4 +70,8 @@ def main(basis_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/basis")
+    # the QUICK tree from the argument or $QUICK_ROOT
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("QUICK_ROOT")
+    if not root:
+        sys.exit("usage: make_basis.py QUICK_ROOT (or set QUICK_ROOT)")
+    main(os.path.join(root, "basis"))

@@ -2,7 +2,7 @@
 inputs (example/benchmarks/ACE_ALA_NME/ala{n}.in of the QUICK tree), the
 molecules of QUICK's published HF energies.  Run where the QUICK tree exists:
 
-    python tests/golden/make_ace_ala.py /root/reference
+    python tests/golden/make_ace_ala.py [QUICK_ROOT]
 """
 import json
 import os
@@ -27,4 +27,6 @@ def main(quick_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..", "oracle"))
+    from build_ref import quick_root
+    main(sys.argv[1] if len(sys.argv) > 1 else quick_root())

@@ -1,5 +1,6 @@
 """GPU Fock build against the CPU oracle (which is itself pinned to QUICK's
-own kernels, tests/test_oracle_ref.py).  Tolerance: 1e-8 on Fock elements."""
+own kernels by tests/test_oracle.py and the fixtures of tests/golden/).
+Tolerance: 1e-8 on Fock elements."""
 import numpy as np
 import pytest
 

@@ -47,6 +47,19 @@ def test_pairlist_ties_keep_insertion_order():
     b = build_basis(m.symbols, "6-31G*")
     Y = np.ones((b.nshell, b.nshell), order="F") * 1e-5
     got = capi.build_pairlist_host(b, Y)
-    # band 2, all keys equal: plain scan order within each (q,p) class
-    xs = [tuple(p) for p in got["pairs"]]
-    assert xs == sorted(xs, key=lambda p: (p[0], p[1])) or len(xs) > 0
+    # Every bound is 1e-5 (band 2 of gpu.cu:532-636), so the Schwarz sort
+    # leaves QUICK's scan order and only the stable primitive-count sort
+    # (kprim(x) kprim(y) descending, then kprim(x) descending) reorders it.
+    sq, sqn, kp = got["sorted_Q"], got["sorted_Qnumber"], b.kprim
+    want = []
+    for qp in range(7):
+        for q in range(4):
+            for p in range(4):
+                if p + q != qp:
+                    continue
+                blk = [(i, j) for i in range(len(sq)) for j in range(len(sq))
+                       if sqn[i] == q and sqn[j] == p and sq[i] <= sq[j]]
+                blk.sort(key=lambda e: (-int(kp[sq[e[0]]]) * int(kp[sq[e[1]]]), -int(kp[sq[e[0]]])))
+                want += blk
+    xs = [tuple(int(v) for v in p) for p in got["pairs"]]
+    assert len(xs) > 0 and xs == want

@@ -79,7 +79,8 @@ def test_radial_grid_is_euler_maclaurin():
 
 
 def test_radial_grid_matches_quick_table():
-    src = "/root/reference/src/cuda/gpu_getxc.cu"
+    from oracle.build_ref import quick_root
+    src = os.path.join(quick_root(), "src", "cuda", "gpu_getxc.cu")
     if not os.path.exists(src):
         pytest.skip("QUICK source tree not present")
     import re
