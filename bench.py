@@ -35,37 +35,15 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# pure-Python input builders (no library load): QUICK's basis arrays, the
+# seeded molecules, the model density and QUICK's density screen
+from quick_b200.molecule import model_density  # noqa: E402
+from quick_b200.scf import shell_cut_matrix  # noqa: E402
+
 WORKLOAD = dict(name="(H2O)32 6-31G** RHF Fock build", grid=(4, 4, 2), basis="6-31G**", seed=0,
                 integral_cutoff=1e-10, prim_limit=1e-20)
-SAMPLE = dict(name="(H2O)16 6-31G** RHF Fock build", grid=(4, 2, 2), basis="6-31G**", seed=0)
 # mixed-precision split: shell quartets whose Y_ab Y_cd DNMax bound is below this run in FP32
 MIXED_CUT = 1e-3
-
-
-def model_density(mol, basis, seed=0):
-    """A symmetric density with the magnitude structure of a real one:
-    |D_ij| ~ 0.5 exp(-R_ij / 1.5 bohr) between the centres of functions i and
-    j, random signs, unit diagonal.  Seeded; used where no SCF density exists."""
-    rng = np.random.default_rng(seed)
-    xyz = mol.xyz_bohr.T
-    c = xyz[basis.ncenter - 1]
-    R = np.linalg.norm(c[:, None, :] - c[None, :, :], axis=-1)
-    u = rng.uniform(-1.0, 1.0, R.shape)
-    u = 0.5 * (u + u.T)
-    D = 0.5 * np.exp(-R / 1.5) * u
-    np.fill_diagonal(D, 1.0)
-    return np.asfortranarray(D)
-
-
-def shell_cut_matrix(basis, D):
-    """QUICK's density screen cutMatrix(II,JJ) = max |D| over the shell-pair
-    block (src/schwarz.f90:550-599), vectorised."""
-    first = basis.Ksumtype[:-1] - 1
-    last = basis.Ksumtype[1:] - 1
-    A = np.abs(D)
-    rowmax = np.stack([A[f:l].max(axis=0) for f, l in zip(first, last)])   # (nshell, nbasis)
-    cm = np.stack([rowmax[:, f:l].max(axis=1) for f, l in zip(first, last)], axis=1)
-    return np.asfortranarray(np.maximum(cm, cm.T))
 
 
 class Clocks:
@@ -147,53 +125,80 @@ def batch_sizes(nmol, rank):
     return np.random.default_rng(1234 + rank).integers(1, 13, size=nmol)
 
 
-def unique_quartets(b, Y, cm, cutoff):
-    """Unique shell quartets of the metric's unit (see module docstring),
-    counted on the host from QUICK's pair list and QUICK's two screens."""
-    from quick_b200 import capi
-    pl = capi.build_pairlist_host(b, Y)
-    sq, sqn = pl["sorted_Q"], pl["sorted_Qnumber"]
-    keep = []
-    for x, y in pl["pairs"]:
-        if sq[x] == sq[y] and x != y and sqn[x] > sqn[y]:
-            continue
-        keep.append((sq[x], sq[y]))
-    keep = np.array(keep)
-    Yp = Y[keep[:, 0], keep[:, 1]]
-    n = len(keep)
-    tot = 0
-    for a in range(n):
-        yy = Yp[a:] * Yp[a]
-        i, j = keep[a]
-        k, l = keep[a:, 0], keep[a:, 1]
-        dn = np.maximum.reduce([np.full(n - a, 4 * cm[i, j]), 4 * cm[k, l], cm[i, l], cm[i, k], cm[j, k], cm[j, l]])
-        tot += int(np.count_nonzero((yy > cutoff) & (yy * dn > cutoff)))
-    return tot
+WARMUP_SAMPLE = dict(name="(H2O)4 6-31G* RHF Fock build", grid=(2, 2, 1), basis="6-31G*")
+
+
+def workload_config(nbasis, quartets):
+    """The config object of the Fock-build line, the same for both arms."""
+    return {"workload": WORKLOAD["name"], "nbasis": nbasis, "quartets_per_step": quartets,
+            "integral_cutoff": WORKLOAD["integral_cutoff"], "prim_limit": WORKLOAD["prim_limit"],
+            "method": "HF (full exchange)", "density": "model density, seed %d" % WORKLOAD["seed"],
+            "l2": "GPU arm: flushed (256 MB write) before every timed step; host arm: not applicable",
+            "parallelism": "replicas"}
 
 
 def cpu_reference(threads, steps=1, warmup=0):
     """QUICK's own two-electron kernel (src/cuda/gpu_get2e_subs.h, driven by
-    QUICK's src/cuda/gpu.cu bridge) compiled for the host cores, on a bounded
-    sample of the workload.  Returns (quartets/s, quartets per step, s/step)."""
+    QUICK's src/cuda/gpu.cu bridge) compiled for the host cores
+    (oracle/_ref/libquickref.so), timed on the workload itself: one step is
+    one full Fock build of (H2O)32 in 6-31G** through QUICK's gpu_upload_* /
+    gpu_get2e_ sequence.  Warm-up steps run the same kernel on (H2O)4 in
+    6-31G*.  The shell quartets per step are counted by QUICK's own walk
+    (oracle.ref_quartet_counts: once per unordered pair of shell pairs, the
+    count the GPU arm reports; tests/test_gpu_configs.py holds the two equal).
+    Nothing of this package's library is loaded.
+    Returns (quartets/s, quartets per step, s per step, raw iclass calls)."""
     import oracle
     from quick_b200.basis import build_basis
     from quick_b200.molecule import water_cluster
-    m = water_cluster(SAMPLE["grid"], seed=SAMPLE["seed"])
-    b = build_basis(m.symbols, SAMPLE["basis"])
-    Y, cp = oracle.schwarz(b, m.xyz_bohr)
-    D = model_density(m, b)
-    cm = shell_cut_matrix(b, D)
-    nq = unique_quartets(b, Y, cm, WORKLOAD["integral_cutoff"])
-    oracle.ref_upload_molecule(m, b, Y, cp, threads=threads)
-    Z = np.zeros_like(D)
-    for _ in range(warmup):
-        oracle.ref_get2e(Z, D, cm, WORKLOAD["integral_cutoff"], WORKLOAD["prim_limit"])
-    ts = []
+    cut, plim = WORKLOAD["integral_cutoff"], WORKLOAD["prim_limit"]
+
+    def setup(grid, basis):
+        m = water_cluster(grid, seed=WORKLOAD["seed"])
+        b = build_basis(m.symbols, basis)
+        Y, cp = oracle.schwarz(b, m.xyz_bohr)
+        keep = oracle.ref_upload_molecule(m, b, Y, cp, threads=threads)
+        D = model_density(m, b, seed=WORKLOAD["seed"])
+        return b, keep, D, shell_cut_matrix(b, D)
+
+    if warmup:
+        b, keep, D, cm = setup(WARMUP_SAMPLE["grid"], WARMUP_SAMPLE["basis"])
+        for _ in range(warmup):
+            oracle.ref_get2e(np.zeros_like(D), D, cm, cut, plim)
+    b, keep, D, cm = setup(WORKLOAD["grid"], WORKLOAD["basis"])
+    ts, counts = [], set()
     for _ in range(steps):
         t0 = time.perf_counter()
-        oracle.ref_get2e(Z, D, cm, WORKLOAD["integral_cutoff"], WORKLOAD["prim_limit"])
+        oracle.ref_get2e(np.zeros_like(D), D, cm, cut, plim)
         ts.append(time.perf_counter() - t0)
-    return nq / np.mean(ts), nq, float(np.mean(ts))
+        counts.add(oracle.ref_quartet_counts())
+    assert len(counts) == 1, counts
+    raw, nq = counts.pop()
+    return nq / np.mean(ts), nq, float(np.mean(ts)), raw
+
+
+def quick_parity(G, quartets, n):
+    """max |G - G_QUICK| over the fixture's 20000 sampled elements and the
+    diagonal, the largest projection error, and whether the shell-quartet
+    count equals QUICK's (tests/golden/config1_water32_631gss.npz: QUICK's
+    kernel compiled for the host on this workload and density).  G is
+    row-major here; it is symmetric."""
+    path = os.path.join(ROOT, "tests", "golden", "config1_water32_631gss.npz")
+    if not os.path.exists(path) or WORKLOAD["grid"] != (4, 4, 2):
+        return None
+    z = np.load(path)
+    if int(z["nbasis"]) != n:
+        return None
+    rng = np.random.default_rng(123)           # the fixture's probes (make_config_golden.probes)
+    R = rng.standard_normal((n, 8))
+    idx = rng.integers(0, n, size=(20000, 2))
+    return {"max_abs_dF_sampled": float(max(np.abs(G[idx[:, 0], idx[:, 1]] - z["sample"]).max(),
+                                            np.abs(np.diag(G) - z["diag"]).max())),
+            "max_abs_dGR": float(np.abs(G @ R - z["GR"]).max()),
+            "quartets_equal_quick": int(z["unique_quartets"]) == int(quartets),
+            "quick_unique_quartets": int(z["unique_quartets"]),
+            "reference": "QUICK's get2e kernel compiled for the host, same inputs (20000 sampled elements, "
+                         "the diagonal and 8 projections of the 800 x 800 matrix)"}
 
 
 def run_ours(args, ws, rank, local):
@@ -274,6 +279,10 @@ def run_ours(args, ws, rank, local):
     step_ms = [a.elapsed_time(b_) for a, b_ in zip(e0, e1)]
     ms = max_over_ranks(float(np.mean(step_ms)), ws)
     clk = clocks.stop() if clocks else None
+
+    # the timed step's result against QUICK's own kernel on the same inputs
+    # (fixture of tests/golden/make_config_golden.py), outside the timed region
+    parity = quick_parity(dOut.double().cpu().numpy(), quartets, n)
 
     # end to end through QUICK's C ABI with pinned host buffers: upload D, O and
     # cutMatrix, Fock build, download O, every step
@@ -380,10 +389,9 @@ def run_ours(args, ws, rank, local):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic: seeded (H2O)32 geometry, model density",
-        "config": {"workload": WORKLOAD["name"], "nbasis": n, "quartets_per_step": quartets,
-                   "integral_cutoff": cutoff, "prim_limit": plim, "method": "HF (full exchange)",
-                   "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas",
-                   "lane_groups": "autotuned per class (qb_autotune_classes)"},
+        "config": workload_config(n, quartets),
+        "lane_groups": "autotuned per class (qb_autotune_classes)",
+        "parity_vs_quick": parity,
         "e2e": {"value": quartets * ws / (e2e_ms * 1e-3), "unit": "quartets/s",
                 "h2d_bytes_per_step": int(2 * n * n * 8 + b.nshell ** 2 * 8),
                 "d2h_bytes_per_step": int(n * n * 8), "ms_per_step": e2e_ms},
@@ -650,26 +658,27 @@ def main():
                     help="fock: the Fock build line only; xc: the XC quadrature line only; "
                          "scf: the SCF+gradient line only; batch: the many-small-molecules line only")
     args = ap.parse_args()
-    ws, rank, local = dist_setup()
     threads = os.cpu_count() or 1
     if args.impl == "reference":
-        if rank == 0:
-            qps, nq, sec = cpu_reference(threads, steps=args.steps, warmup=args.warmup)
-            sample = ("%s, %d quartets per step; QUICK's gpu_get2e_subs.h kernel and gpu.cu bridge "
-                      "compiled for the host cores" % (SAMPLE["name"], nq))
+        # QUICK's own kernel on the host cores; under torchrun rank 0 alone
+        # runs it and the other ranks exit without work (no process group)
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        if int(os.environ.get("RANK", "0")) == 0:
+            qps, nq, sec, raw = cpu_reference(threads, steps=args.steps, warmup=args.warmup)
+            sample = ("%d full Fock builds of %s (%d unique shell quartets, %d iclass calls, per build); "
+                      "QUICK's gpu_get2e_subs.h kernel and gpu.cu bridge compiled for the host cores; warm-up "
+                      "builds on %s" % (args.steps, WORKLOAD["name"], nq, raw, WARMUP_SAMPLE["name"]))
             out = {"impl": "reference", "metric": "Fock-build shell quartets/s (FP64)", "value": qps,
                    "unit": "quartets/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
                    "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                   "dtype": "f64", "data": "synthetic: seeded water cluster, model density",
-                   "config": {"workload": WORKLOAD["name"], "sample": SAMPLE["name"]},
+                   "dtype": "f64", "data": "synthetic: seeded (H2O)32 geometry, model density",
+                   "config": workload_config(800, nq),
                    "cpu_baseline": {"value": qps, "unit": "quartets/s", "cores": threads, "kind": "reference",
                                     "sample": sample},
                    "e2e": {"value": qps, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
             print(json.dumps(out))
-        if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
         return
+    ws, rank, local = dist_setup()
     if args.part in ("xc", "scf", "batch"):
         out = {"xc": run_xc, "scf": run_scf, "batch": run_batch}[args.part](args, ws, rank, local)
         if rank == 0:
@@ -684,11 +693,12 @@ def main():
         out["scf"] = run_scf(args, ws, rank, local)
         out["batch"] = run_batch(args, ws, rank, local)
     if rank == 0 and not args.no_cpu_baseline:
-        qps, nq, sec = cpu_reference(threads)
+        qps, nq, sec, raw = cpu_reference(threads)
         out["cpu_baseline"] = {"value": qps, "unit": "quartets/s", "cores": threads, "kind": "reference",
-                               "sample": "one Fock build of %s (%d quartets, %.2f s); QUICK's gpu_get2e_subs.h "
-                                         "kernel and gpu.cu bridge compiled for the host cores" % (
-                                             SAMPLE["name"], nq, sec)}
+                               "sample": "one full Fock build of %s (%d unique shell quartets, %.2f s); QUICK's "
+                                         "gpu_get2e_subs.h kernel and gpu.cu bridge compiled for the host cores"
+                                         % (WORKLOAD["name"], nq, sec),
+                               "quartets_equal_gpu_count": nq == out["config"]["quartets_per_step"]}
     if rank == 0:
         print(json.dumps(out))
     if ws > 1:

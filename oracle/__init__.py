@@ -338,10 +338,25 @@ def ref_pairlist():
                 sorted_Q=q[:nq].copy(), sorted_Qnumber=qn[:nq].copy())
 
 
+def ref_quartet_counts(spdf=False):
+    """Shell quartets of the last QUICK Fock builds since ref_get2e reset the
+    counter: (raw, unique).  raw counts QUICK's iclass calls
+    (gpu_get2e_subs.h:327-336: ordered pair-pairs with ii <= kk that pass both
+    Schwarz tests); unique counts the same walk once per unordered pair of
+    shell pairs, without the (p,s) copy of an sp shell's self-pair -- the
+    metric's unit."""
+    r = ref_lib(spdf)
+    raw, uniq = C.c_longlong(0), C.c_longlong(0)
+    r.qref_quartet_counts(C.byref(raw), C.byref(uniq))
+    return raw.value, uniq.value
+
+
 def ref_get2e(O, dense, cutMatrix, integral_cutoff, prim_limit, method=0, spdf=False):
     """One QUICK Fock build: upload_method/calculated/cutoff + gpu_get2e_
-    (src/hfoperator.f90:76-98).  Returns the new O."""
+    (src/hfoperator.f90:76-98).  Returns the new O; ref_quartet_counts()
+    then gives its shell-quartet counts."""
     r = ref_lib(spdf)
+    r.qref_reset_counts()
     n = O.shape[0]
     o = np.array(O, order="F", dtype=np.float64)
     co = np.zeros((n, n), order="F")

@@ -58,23 +58,28 @@ def build(quick_root, spdf=False, accurate_boys=False, jobs=8, opt="-O2"):
     assert n == 1, "expected one getxc_kernel launch"
     with open(os.path.join(OUT, "gpu_getxc_host.cu"), "w") as fh:
         fh.write(xc)
+    # build-directory copies: gpu_get2e.cu (so that its quoted includes look
+    # here first) and gpu_get2e_subs.h with a call of qref_count_quartet
+    # beside the spd walk's iclass call (the shell-quartet counter of the
+    # metric); with accurate_boys, QUICK's FmT renamed and an FmT that calls
+    # the accurate Boys function in its place
+    with open(os.path.join(src, "gpu_get2e.cu")) as fh:
+        g2 = fh.read()
+    with open(os.path.join(OUT, "gpu_get2e.cu"), "w") as fh:
+        fh.write(g2)
+    with open(os.path.join(src, "gpu_get2e_subs.h")) as fh:
+        sub = fh.read()
+    call = "iclass(iii, jjj, kkk, lll, ii, jj, kk, ll, DNMax);"
+    assert sub.count(call) == 1, "expected one spd iclass call"
+    sub = sub.replace(call, "qref_count_quartet(a, b, II, JJ, KK, LL, ii, kk); " + call)
     if accurate_boys:
-        # build-directory copies: gpu_get2e.cu (so that its quoted includes
-        # look here first) and gpu_get2e_subs.h with QUICK's FmT renamed and
-        # an FmT that calls the accurate Boys function in its place
-        with open(os.path.join(src, "gpu_get2e.cu")) as fh:
-            g2 = fh.read()
-        with open(os.path.join(OUT, "gpu_get2e.cu"), "w") as fh:
-            fh.write(g2)
-        with open(os.path.join(src, "gpu_get2e_subs.h")) as fh:
-            sub = fh.read()
         decl = "__device__ __forceinline__ void FmT(int MaxM, QUICKDouble X, QUICKDouble* YVerticalTemp)"
         assert sub.count(decl) == 1, "expected one FmT definition"
         sub = sub.replace(decl, "__device__ __forceinline__ void FmT(int MaxM, QUICKDouble X, QUICKDouble* YVerticalTemp)\n"
                                 "{ qref_boys_accurate(MaxM, X, YVerticalTemp); }\n"
                                 "__device__ __forceinline__ void FmT_quick(int MaxM, QUICKDouble X, QUICKDouble* YVerticalTemp)")
-        with open(os.path.join(OUT, "gpu_get2e_subs.h"), "w") as fh:
-            fh.write(sub)
+    with open(os.path.join(OUT, "gpu_get2e_subs.h"), "w") as fh:
+        fh.write(sub)
     flags = [opt, "-fPIC", "-std=c++17", "-w", "-include", os.path.join(SHIM, "qref_shim.h"),
              "-I" + SHIM, "-I" + os.path.join(OUT, "inc"), "-I" + OUT, "-I" + src, "-I" + CUDA_INC]
     units = ["ref_bridge", "ref_kernels", "ref_type", "ref_xc"]

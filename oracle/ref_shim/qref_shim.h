@@ -44,6 +44,12 @@ static inline unsigned int atomicAdd(unsigned int* a, unsigned int v)
    accurate-Boys checker build calls it in place of QUICK's FmT. */
 void qref_boys_accurate(int maxm, double x, double* out);
 
+/* Counts one iclass call of QUICK's spd walk (gpu_get2e_subs.h:327-336):
+   a and b index QUICK's pair list, II..LL its sorted Qshells, ii and kk the
+   first shells of the two pairs (defined in ref_kernels.cpp; the call is
+   added to a build-directory copy of gpu_get2e_subs.h by build_ref.py). */
+void qref_count_quartet(unsigned long long a, unsigned long long b, int II, int JJ, int KK, int LL, int ii, int kk);
+
 /* Runs the kernel named in a QUICK_SAFE_CALL launch expression on host
    threads (defined in ref_kernels.cpp). */
 void qref_launch(const char* launch_expression);

@@ -14,6 +14,37 @@
 
 thread_local qref_dim qref_blockIdx, qref_threadIdx, qref_blockDim, qref_gridDim;
 
+/* Shell-quartet counts of QUICK's own walk, kept per host thread and summed
+   when the launch's threads finish:
+     raw     every iclass call (ordered pair-pairs with ii <= kk that pass
+             both Schwarz tests, gpu_get2e_subs.h:311-336);
+     unique  the same walk counted once per unordered pair of pairs: for
+             ii == kk only a <= b, and without the (p,s) copy of an sp
+             shell's self-pair, whose integrals QUICK's basis-function
+             filter drops (gpu_get2e_subs.h:792-801). */
+static thread_local long long qref_raw_local = 0, qref_unique_local = 0;
+static long long qref_raw = 0, qref_unique = 0;
+
+static bool qref_sp_copy(int X, int Y)
+{
+    return devSim.sorted_Q[X] == devSim.sorted_Q[Y] && X != Y && devSim.sorted_Qnumber[X] > devSim.sorted_Qnumber[Y];
+}
+
+void qref_count_quartet(unsigned long long a, unsigned long long b, int II, int JJ, int KK, int LL, int ii, int kk)
+{
+    qref_raw_local++;
+    if (qref_sp_copy(II, JJ) || qref_sp_copy(KK, LL)) return;
+    if (ii < kk || a <= b) qref_unique_local++;
+}
+
+extern "C" void qref_quartet_counts(long long* raw, long long* unique)
+{
+    *raw = qref_raw;
+    *unique = qref_unique;
+}
+
+extern "C" void qref_reset_counts(void) { qref_raw = qref_unique = 0; }
+
 static int qref_nthreads = 1;
 static int qref_nvirtual = 0;   // 0: one virtual thread per host thread
 extern "C" void qref_set_threads(int n) { qref_nthreads = n > 0 ? n : 1; }
@@ -70,6 +101,9 @@ void qref_launch(const char* expr)
                 qref_gridDim = {(unsigned)nv, 1, 1};
                 fn();
             }
+            __atomic_fetch_add(&qref_raw, qref_raw_local, __ATOMIC_RELAXED);
+            __atomic_fetch_add(&qref_unique, qref_unique_local, __ATOMIC_RELAXED);
+            qref_raw_local = qref_unique_local = 0;
         });
     }
     for (auto& th : pool) th.join();

@@ -166,3 +166,18 @@ def parse_quick_input(text):
         elif started:
             break
     return Molecule(symbols, np.array(xyz))
+
+
+def model_density(mol, basis, seed=0):
+    """A symmetric density with the magnitude structure of a real one:
+    |D_ij| ~ 0.5 exp(-R_ij / 1.5 bohr) between the centres of functions i and
+    j, random signs, unit diagonal.  Seeded; used where no SCF density exists."""
+    rng = np.random.default_rng(seed)
+    xyz = mol.xyz_bohr.T
+    c = xyz[basis.ncenter - 1]
+    R = np.linalg.norm(c[:, None, :] - c[None, :, :], axis=-1)
+    u = rng.uniform(-1.0, 1.0, R.shape)
+    u = 0.5 * (u + u.T)
+    D = 0.5 * np.exp(-R / 1.5) * u
+    np.fill_diagonal(D, 1.0)
+    return np.asfortranarray(D)
