@@ -115,7 +115,7 @@ def build(lmax=2, jobs=None, verbose=False):
     with ThreadPoolExecutor(jobs) as ex:
         list(ex.map(cc, todo))
     if todo or not os.path.exists(LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lcublas", "-lpthread"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lpthread"]
         subprocess.run(cmd, check=True)
     return LIB
 

@@ -50,6 +50,9 @@ struct DevBuf {
     }
 };
 
+// side streams for concurrent class launches (QB_CLASS_STREAMS = total streams, default 4)
+constexpr int kSideStreams = 3;
+
 struct Context {
     int dev_id = -1;
     bool inited = false;
@@ -81,6 +84,9 @@ struct Context {
     std::vector<int> type_begin, type_end;
     // device tables
     DevBuf<double4> d_prim;
+    DevBuf<PrimRec32> d_prim32;          // FP32 records of the same primitive pairs
+    DevBuf<double4> d_pair_A;            // centre of each pair's first shell
+    DevBuf<float> d_boys32;              // FP32 Boys records
     DevBuf<double> d_pair_Y, d_boys, d_dense, d_dense_raw, d_cons, d_fock, d_cut_matrix, d_o_in, d_o_out, d_grad;
     DevBuf<int> d_shell_atom;
     DevBuf<int4> d_pair_bf, d_pair_sh;
@@ -96,6 +102,7 @@ struct Context {
     long long shell_first_version = -1;
     std::vector<ScreenClass> screen_cls;
     std::vector<int> class_group;        // lanes per shell quartet of each class kernel
+    std::vector<int> class_group32;      // the same for the FP32 class kernels of the mixed split
     int generic_min_l = 99;              // classes with L sum >= this run the generic kernel (QB_GENERIC_MIN_L)
     // per-iteration
     std::vector<double> o_host;          // O as uploaded (one-electron part)
@@ -115,6 +122,11 @@ struct Context {
     XcResult last_xc;
     double last_ms_eri = 0, last_ms_screen = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // side streams of the class launches (fock_build); nside < 0: not created yet
+    int nside = -1;
+    cudaStream_t side[kSideStreams] = {};
+    cudaEvent_t side_ev[kSideStreams] = {};
+    cudaEvent_t fork_ev = nullptr;
 };
 
 unsigned long long g_launches = 0;   // kernels launched by this library
@@ -350,6 +362,8 @@ static int build_tables(Context& c)
     std::vector<double> pY(c.npair);
     std::vector<double4> pAB(c.npair);
     std::vector<double4> prim;
+    std::vector<PrimRec32> prim32;
+    std::vector<double4> pA(c.npair);
     for (int i = 0; i < c.npair; i++) {
         const Rec& e = recs[i];
         const double *A = center(c, e.shA), *B = center(c, e.shB);
@@ -375,11 +389,18 @@ static int build_tables(Context& c)
                 prim.push_back(make_double4(p, K, P[0], P[1]));
                 prim.push_back(make_double4(P[2], PA[0], PA[1], PA[2]));
                 prim.push_back(make_double4(0.5 / p, a, cp, 0.0));
+                PrimRec32 r32;
+                r32.p = (float)p; r32.K = (float)K;
+                r32.PAx = (float)PA[0]; r32.PAy = (float)PA[1]; r32.PAz = (float)PA[2];
+                r32.o2p = (float)(0.5 / p);
+                r32.cp = cp;
+                prim32.push_back(r32);
             }
         pbf[i] = make_int4(bf_first(c, e.shA, e.LA), bf_first(c, e.shB, e.LB), off, (int)prim.size() / 3 - off);
         psh[i] = make_int4(e.shA, e.shB, e.key, e.ref);
         pY[i] = e.Y;
         pAB[i] = make_double4(A[0] - B[0], A[1] - B[1], A[2] - B[2], e.w);
+        pA[i] = make_double4(A[0], A[1], A[2], 0.0);
     }
     CK(c.d_prim.alloc(prim.size()));
     CK(c.d_pair_bf.alloc(c.npair));
@@ -387,6 +408,11 @@ static int build_tables(Context& c)
     CK(c.d_pair_Y.alloc(c.npair));
     CK(c.d_pair_AB.alloc(c.npair));
     CK(cudaMemcpy(c.d_prim.p, prim.data(), prim.size() * sizeof(double4), cudaMemcpyHostToDevice));
+    CK(c.d_prim32.alloc(std::max<size_t>(prim32.size(), 1)));
+    CK(c.d_pair_A.alloc(std::max<size_t>(pA.size(), 1)));
+    if (!prim32.empty())
+        CK(cudaMemcpy(c.d_prim32.p, prim32.data(), prim32.size() * sizeof(PrimRec32), cudaMemcpyHostToDevice));
+    if (!pA.empty()) CK(cudaMemcpy(c.d_pair_A.p, pA.data(), pA.size() * sizeof(double4), cudaMemcpyHostToDevice));
     std::vector<int> satom(c.nshell);
     for (int s = 0; s < c.nshell; s++) satom[s] = c.katom[s] - 1;
     CK(c.d_shell_atom.alloc(c.nshell));
@@ -432,9 +458,10 @@ static int build_tables(Context& c)
                      type_prims[pair_type_index(kClassL[k][2], kClassL[k][3])] / div;
         int g = 1;
         while (g * 2 <= est && g < 32) g *= 2;
-        if (gf && atoi(gf) > 0) g = atoi(gf);
+        if (gf && atoi(gf) > 0) g = atoi(gf);   // QB_FOCK_G forces one value
         c.class_group[k] = std::min(g, class_max_group(k));
     }
+    c.class_group32 = c.class_group;
     return 0;
 }
 
@@ -462,6 +489,9 @@ static FockParams fock_params(Context& c)
     P.class_count32 = c.d_class_count32.p;
     P.class_end = c.d_class_end.p;
     P.ket_segs = c.d_ket_segs.p;
+    P.prim32 = c.d_prim32.p;
+    P.pair_A = c.d_pair_A.p;
+    P.boys32 = c.d_boys32.p;
     return P;
 }
 
@@ -533,6 +563,44 @@ static int screen_quartets(Context& c, std::vector<int>& cnt)
     return 0;
 }
 
+// The classes are independent: their kernels are dealt round-robin to the
+// library stream and up to kSideStreams side streams, forked from and joined
+// back into the library stream with events (so a CUDA graph capture keeps
+// the order), which fills the tail of one class's launch with the next.
+// QB_CLASS_STREAMS sets the total number of streams (default 4).
+static int fork_side_streams(Context& c)
+{
+    if (c.nside < 0) {
+        const char* ns = getenv("QB_CLASS_STREAMS");
+        c.nside = std::max(0, std::min(ns ? atoi(ns) - 1 : kSideStreams, kSideStreams));
+        for (int i = 0; i < c.nside; i++) {
+            CK(cudaStreamCreateWithFlags(&c.side[i], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&c.side_ev[i], cudaEventDisableTiming));
+        }
+        CK(cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming));
+    }
+    if (c.nside > 0) {
+        CK(cudaEventRecord(c.fork_ev, c.stream));
+        for (int i = 0; i < c.nside; i++) CK(cudaStreamWaitEvent(c.side[i], c.fork_ev, 0));
+    }
+    return 0;
+}
+
+static cudaStream_t side_stream(Context& c, int turn)
+{
+    const int t = turn % (c.nside + 1);
+    return t == 0 ? c.stream : c.side[t - 1];
+}
+
+static int join_side_streams(Context& c)
+{
+    for (int i = 0; i < c.nside; i++) {
+        CK(cudaEventRecord(c.side_ev[i], c.side[i]));
+        CK(cudaStreamWaitEvent(c.stream, c.side_ev[i], 0));
+    }
+    return 0;
+}
+
 // Two-electron gradient into d_grad (3 natom), same quartet lists.
 static int grad_build(Context& c)
 {
@@ -548,16 +616,20 @@ static int grad_build(Context& c)
     CK(cudaEventRecord(c.ev[2], c.stream));
     long long total = 0;
     for (int k = 0; k < kNumClasses; k++) total += cnt[k];
+    if (int rc = fork_side_streams(c)) return rc;
+    int turn = 0;
     for (int k = 0; k < kNumClasses; k++) {
         if (cnt[k] == 0) continue;
         const int GS = std::min(c.class_group.empty() ? 1 : std::max(c.class_group[k], 1), grad_max_group(k));
-        if (launch_grad_class(k, P, G, GS, cnt[k], c.nsm, c.stream) < 0) {
+        if (launch_grad_class(k, P, G, GS, cnt[k], c.nsm, side_stream(c, turn++)) < 0) {
+            // the generic kernels share one scratch array: all on the library stream, in order
             const int* Lk = kClassL[k];
             if (launch_generic_grad_class(k, Lk[0], Lk[1], Lk[2], Lk[3], P, G, cnt[k], c.nsm, c.stream) < 0)
                 return set_error(2, "gpu_grad_: cannot allocate the scratch of class (%d%d|%d%d)", Lk[0], Lk[1],
                                  Lk[2], Lk[3]), 2;
         }
     }
+    if (int rc = join_side_streams(c)) return rc;
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[3], c.stream));
     CK(cudaStreamSynchronize(c.stream));
@@ -598,22 +670,27 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
     // bound), so nothing between screening and digestion waits for the host
     // and the whole build can be captured in a CUDA graph.
     CK(cudaEventRecord(c.ev[2], c.stream));
+    if (int rc = fork_side_streams(c)) return rc;
+    int turn = 0;
     for (int k = 0; k < kNumClasses; k++) {
         const long long cap = c.screen_cls[k].capacity;
         if (cap == 0) continue;
         const int nq = (int)std::min<long long>(cap, 1LL << 30);
         for (int f32 = 0; f32 < (c.mixed_cut > 0.0 ? 2 : 1); f32++) {
-            const int G = c.class_group.empty() ? 1 : c.class_group[k];
+            const int G = f32 ? (c.class_group32.empty() ? 1 : c.class_group32[k])
+                              : (c.class_group.empty() ? 1 : c.class_group[k]);
             const int* Lk = kClassL[k];
             const bool gen = Lk[0] + Lk[1] + Lk[2] + Lk[3] >= c.generic_min_l;
-            const int rc = gen ? launch_generic_class(k, Lk[0], Lk[1], Lk[2], Lk[3], P, nq, c.nsm, f32, c.stream)
-                               : (f32 ? launch_class32(k, P, G, nq, c.nsm, c.stream)
-                                      : launch_class(k, P, G, nq, c.nsm, c.stream));
+            cudaStream_t st = side_stream(c, turn++);
+            const int rc = gen ? launch_generic_class(k, Lk[0], Lk[1], Lk[2], Lk[3], P, nq, c.nsm, f32, st)
+                               : (f32 ? launch_class32(k, P, G, nq, c.nsm, st)
+                                      : launch_class(k, P, G, nq, c.nsm, st));
             if (rc < 0)
                 return set_error(5, "class (%d%d|%d%d) needs more shared memory than this GPU offers",
                                  kClassL[k][0], kClassL[k][1], kClassL[k][2], kClassL[k][3]), 5;
         }
     }
+    if (int rc = join_side_streams(c)) return rc;
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[3], c.stream));
     launch_fock_finish(c.d_fock.p, c.d_cons.p, d_o_in, d_o_out, n, c.stream);
@@ -705,8 +782,18 @@ void gpu_init_(void)
     if (!c.stream) c.stream = c.own_stream;
     std::vector<double> tab;
     boys_table(tab);
+    // FP32 records: F_L .. F_{L+4}, e^-T_k, two pad floats
+    std::vector<float> tab32(kBoys32Size, 0.0f);
+    for (int L = 0; L <= kBoysLMax; L++)
+        for (int k = 0; k < kBoysPoints; k++) {
+            float* r = tab32.data() + ((size_t)L * kBoysPoints + k) * 8;
+            for (int j = 0; j < 5; j++) r[j] = (float)tab[(size_t)k * kBoysCols + L + j];
+            r[5] = (float)tab[(size_t)k * kBoysCols + kBoysExpCol];
+        }
     if (c.d_boys.alloc(tab.size()) != cudaSuccess ||
-        cudaMemcpy(c.d_boys.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpy(c.d_boys.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        c.d_boys32.alloc(tab32.size()) != cudaSuccess ||
+        cudaMemcpy(c.d_boys32.p, tab32.data(), tab32.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
         set_error(2, "cannot upload the Boys table");
         return;
     }
@@ -728,6 +815,9 @@ void gpu_shutdown_(void)
     c.d_shell_atom.release();
     for (auto* b : dbl) b->release();
     c.d_prim.release();
+    c.d_prim32.release();
+    c.d_pair_A.release();
+    c.d_boys32.release();
     c.d_pair_bf.release();
     c.d_pair_sh.release();
     c.d_pair_AB.release();
@@ -743,6 +833,11 @@ void gpu_shutdown_(void)
     c.d_ket_segs.release();
     for (auto& e : c.ev)
         if (e) cudaEventDestroy(e), e = nullptr;
+    for (int i = 0; i < c.nside; i++) {
+        cudaStreamDestroy(c.side[i]);
+        cudaEventDestroy(c.side_ev[i]);
+    }
+    if (c.fork_ev) cudaEventDestroy(c.fork_ev);
     xc_release();
     oneint_release();
     generic_release();
@@ -978,36 +1073,48 @@ int qb_autotune_classes(int* groups, int cap)
     CK(cudaMemsetAsync(scratch.p, 0, (size_t)n * n * sizeof(double), c.stream));
     FockParams P = fock_params(c);
     P.fock = scratch.p;
+    const bool verbose = getenv("QB_AUTOTUNE_VERBOSE") && atoi(getenv("QB_AUTOTUNE_VERBOSE")) > 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
+    // the last build's lists: its FP64 kernels are tuned after an all-FP64
+    // build, its FP32 kernels after a build with the mixed split
+    std::vector<int> cnt32(kNumClasses);
+    CK(cudaMemcpy(cnt32.data(), c.d_class_count32.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost));
+    const bool f32 = c.mixed_cut > 0.0;
+    std::vector<int>& groups_k = f32 ? c.class_group32 : c.class_group;
     for (int k = 0; k < kNumClasses; k++) {
         const long long capk = c.screen_cls[k].capacity;
         const int* Lk = kClassL[k];
-        if (capk == 0 || Lk[0] + Lk[1] + Lk[2] + Lk[3] >= c.generic_min_l || class_max_group(k) <= 1) continue;
+        if (capk == 0 || Lk[0] + Lk[1] + Lk[2] + Lk[3] >= c.generic_min_l || kClassGeneric[k]) continue;
+        if (f32 && cnt32[k] == 0) continue;
         const int nq = (int)std::min<long long>(capk, 1LL << 30);
-        int best_g = c.class_group[k];
+        int best_g = groups_k[k];
         float best_t = 1e30f;
         for (int g = 1; g <= class_max_group(k); g *= 2) {
             float tmin = 1e30f;
             for (int rep = 0; rep < 2; rep++) {
                 CK(cudaEventRecord(e0, c.stream));
-                launch_class(k, P, g, nq, c.nsm, c.stream);
+                if (f32) launch_class32(k, P, g, nq, c.nsm, c.stream);
+                else launch_class(k, P, g, nq, c.nsm, c.stream);
                 CK(cudaEventRecord(e1, c.stream));
                 CK(cudaEventSynchronize(e1));
                 float ms = 0.f;
                 CK(cudaEventElapsedTime(&ms, e0, e1));
                 tmin = std::min(tmin, ms);
             }
+            if (verbose)
+                fprintf(stderr, "autotune %s (%d%d|%d%d) G=%d %.4f ms\n", f32 ? "fp32" : "fp64", Lk[0], Lk[1], Lk[2],
+                        Lk[3], g, tmin);
             if (tmin < best_t) best_t = tmin, best_g = g;
         }
-        c.class_group[k] = best_g;
+        groups_k[k] = best_g;
     }
     CK(cudaGetLastError());
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     scratch.release();
-    for (int k = 0; k < std::min(cap, kNumClasses); k++) groups[k] = c.class_group[k];
+    for (int k = 0; k < std::min(cap, kNumClasses); k++) groups[k] = groups_k[k];
     return 0;
 }
 

@@ -235,21 +235,28 @@ def gen_class(la, lb, lc, ld, prec="double"):
         w("    %s c_%s_%s = 0.0%s;" % (R, nm(e), nm(f), sfx))
     body = []
     b = body.append
-    b("const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
-    b("if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
-    b("const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
     if f32:
+        # one 32-byte record per primitive pair, FP32 Boys records
+        b("const PrimRec32 pk = load_prim32(P.prim32, q.ket_off + ik);")
+        b("if (!prim_survives(q, pb.cp, pk.cp, P.prim_limit)) continue;")
         b("PrimQuartet32 s;")
         b("float Fm[L + 1];")
-        b("prim_quartet32<L>(pb, pk, P, s, Fm);")
-        b("const float PAx = (float)pb.PAx, PAy = (float)pb.PAy, PAz = (float)pb.PAz;")
-        b("const float QCx = (float)pk.PAx, QCy = (float)pk.PAy, QCz = (float)pk.PAz;")
+        b("prim_quartet32r<L>(pb, pk, q, P.boys32, s, Fm);")
+        b("const float PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
+        b("const float QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
+        bra_load = ["const PrimRec32 pb = load_prim32(P.prim32, q.bra_off + ib);"]
     else:
+        # the ket's three vectors are requested together, ahead of the screen
+        b("const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
+        b("const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
+        b("if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
         b("PrimQuartet s;")
         b("double Fm[L + 1];")
         b("prim_quartet<L>(pb, pk, P, s, Fm);")
         b("const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
         b("const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
+        bra_load = ["const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);",
+                    "const PrimPair pb = load_prim(P, q.bra_off + ib, xb);"]
     b("const %s WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;" % R)
     b("const %s o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;" % R)
     b("(void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;")
@@ -262,8 +269,8 @@ def gen_class(la, lb, lc, ld, prec="double"):
     # G == 1: one lane walks the bra x ket primitive double loop
     w("    if constexpr (G == 1) {")
     w("    for (int ib = 0; ib < q.nbra; ib++) {")
-    w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
-    w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
+    for ln in bra_load:
+        w("        " + ln)
     w("        for (int ik = 0; ik < q.nket; ik++) {")
     for ln in body:
         w("            " + ln)
@@ -274,11 +281,11 @@ def gen_class(la, lb, lc, ld, prec="double"):
     w("    const int nk = q.nket, npq = q.nbra * nk;")
     w("    for (int t = sub; t < npq; t += G) {")
     w("        const int ib = t / nk, ik = t - ib * nk;")
-    w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
-    w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
+    for ln in bra_load:
+        w("        " + ln)
     w("        {")
     for ln in body:
-        w("            " + ln.replace("continue;", "continue;"))
+        w("            " + ln)
     w("        }")
     w("    }")
     for e, f, _ in targets:
@@ -302,15 +309,19 @@ def gen_class(la, lb, lc, ld, prec="double"):
     w("    const int n = P.nbasis;")
     w("    const int a0 = q.bfA, b0 = q.bfB, c0 = q.bfC, d0 = q.bfD;")
 
+    DT = "float" if f32 else "double"
+
     def dl(x, y):
+        if f32:
+            return "(float)__ldg(Dm + (size_t)(%s) * n + (%s))" % (x, y)
         return "__ldg(Dm + (size_t)(%s) * n + (%s))" % (x, y)
     # density loads
     for ic in range(nc):
         for id_ in range(nd):
-            w("    const double Dcd_%d_%d = %s;" % (ic, id_, dl("c0+%d" % ic, "d0+%d" % id_)))
+            w("    const %s Dcd_%d_%d = %s;" % (DT, ic, id_, dl("c0+%d" % ic, "d0+%d" % id_)))
     for ia in range(na):
         for ib in range(nb):
-            w("    const double Dab_%d_%d = %s;" % (ia, ib, dl("a0+%d" % ia, "b0+%d" % ib)))
+            w("    const %s Dab_%d_%d = %s;" % (DT, ia, ib, dl("a0+%d" % ia, "b0+%d" % ib)))
     w("    if (P.hybrid != 0.0) {")
     # exchange needs D_bd, D_bc, D_ad, D_ac
     Kspec = [("ac", "bd", na, nc, nb, nd), ("ad", "bc", na, nd, nb, nc), ("bc", "ad", nb, nc, na, nd), ("bd", "ac", nb, nd, na, nc)]
@@ -322,7 +333,7 @@ def gen_class(la, lb, lc, ld, prec="double"):
         x, y = blk
         for i in range(sizes[x]):
             for j in range(sizes[y]):
-                w("        const double D%s_%d_%d = %s;" % (blk, i, j, dl("%s+%d" % (bases[x], i), "%s+%d" % (bases[y], j))))
+                w("        const %s D%s_%d_%d = %s;" % (DT, blk, i, j, dl("%s+%d" % (bases[x], i), "%s+%d" % (bases[y], j))))
     for out_blk, d_blk, n1, n2, m1, m2 in Kspec:
         x, y = out_blk
         u, v = d_blk
@@ -334,7 +345,7 @@ def gen_class(la, lb, lc, ld, prec="double"):
                         idx = {x: i, y: j, u: k, v: l}
                         key = (idx["a"], idx["b"], idx["c"], idx["d"])
                         terms.append("D%s_%d_%d*%s" % (d_blk, k, l, vals[key]))
-                w("        const double K%s_%d_%d = %s;" % (out_blk, i, j, " + ".join(terms)))
+                w("        const %s K%s_%d_%d = %s;" % (DT, out_blk, i, j, " + ".join(terms)))
     for out_blk, _, n1, n2, _, _ in Kspec:
         x, y = out_blk
         for i in range(n1):
@@ -345,11 +356,11 @@ def gen_class(la, lb, lc, ld, prec="double"):
     for ia in range(na):
         for ib in range(nb):
             terms = ["Dcd_%d_%d*%s" % (ic, id_, vals[(ia, ib, ic, id_)]) for ic in range(nc) for id_ in range(nd)]
-            w("    const double Jab_%d_%d = %s;" % (ia, ib, " + ".join(terms)))
+            w("    const %s Jab_%d_%d = %s;" % (DT, ia, ib, " + ".join(terms)))
     for ic in range(nc):
         for id_ in range(nd):
             terms = ["Dab_%d_%d*%s" % (ia, ib, vals[(ia, ib, ic, id_)]) for ia in range(na) for ib in range(nb)]
-            w("    const double Jcd_%d_%d = %s;" % (ic, id_, " + ".join(terms)))
+            w("    const %s Jcd_%d_%d = %s;" % (DT, ic, id_, " + ".join(terms)))
     w("    const bool bra_uniform = warp_bra_uniform(qa);")
     for ia in range(na):
         for ib in range(nb):
@@ -440,6 +451,54 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     w('#include "grad_common.cuh"')
     w("namespace qb {")
     w("template <> struct GradEval<%d, %d, %d, %d, %d> {" % (la, lb, lc, ld, part))
+    # the primitive-quartet body of run<GS>
+    inner = ["PrimQuartet s;", "double Fm[L + 1];", "prim_quartet<L>(pb, pk, P, s, Fm);",
+             "const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;",
+             "const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;",
+             "const double WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;",
+             "const double o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;",
+             "(void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;",
+             "(void)WQx; (void)WQy; (void)WQz; (void)o2p; (void)o2q; (void)o2pq; (void)rp; (void)rq;"]
+    inner += ["const double F%d = Fm[%d];" % (m, m) for m in range(L + 1)]
+    inner += list(vrr.lines)
+    wt = {"s0": "", "sa": "a2*", "sb": "b2*", "sc": "c2*"}
+    for k, lst in acc.items():
+        for e, f, v in lst:
+            inner.append("%s_%s_%s += %s%s;" % (k, nm(e), nm(f), wt[k], v))
+    # after the contraction: horizontal recurrence, density products, digestion
+    tail = []
+    t_ = tail.append
+    t_("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
+    t_("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
+    for h in hrrs.values():
+        for ln in h.lines:
+            t_("    " + ln)
+    t_("    const double* __restrict__ Dm = P.dense;")
+    t_("    const int n = P.nbasis;")
+    t_("    const int a0 = q.bfA, b0 = q.bfB, c0 = q.bfC, d0 = q.bfD;")
+    t_("    const double hx = P.hybrid;")
+
+    def dl(x, y):
+        return "__ldg(Dm + (size_t)(%s) * n + (%s))" % (x, y)
+    bases = {"a": "a0", "b": "b0", "c": "c0", "d": "d0"}
+    sizes = {"a": na, "b": nb, "c": nc, "d": nd}
+    for blk in ("ab", "cd", "ac", "bd", "ad", "bc"):
+        x, y = blk
+        for i in range(sizes[x]):
+            for j in range(sizes[y]):
+                t_("    const double D%s_%d_%d = %s;" % (blk, i, j, dl("%s+%d" % (bases[x], i), "%s+%d" % (bases[y], j))))
+    t_("    double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};")
+    for ia in range(na):
+        for ib in range(nb):
+            for ic in range(nc):
+                for id_ in range(nd):
+                    t_("    {")
+                    t_("        const double g = 4.0*Dab_%d_%d*Dcd_%d_%d - hx*(Dac_%d_%d*Dbd_%d_%d + Dad_%d_%d*Dbc_%d_%d);" % (
+                        ia, ib, ic, id_, ia, ic, ib, id_, ia, id_, ib, ic))
+                    for i in range(3):
+                        da, db, dc = deriv[(ia, ib, ic, id_, i)]
+                        t_("        gA[%d] += g*(%s); gB[%d] += g*(%s); gC[%d] += g*(%s);" % (i, da, i, db, i, dc))
+                    t_("    }")
     w("template <int GS>")
     w("__device__ __forceinline__ static void run(const QuartetCtx& q, const FockParams& P, const GradExtra& G, int sub)")
     w("{")
@@ -460,23 +519,8 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     w("            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
     w("            const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
     w("            const double c2 = 2.0 * xk.y;")
-    w("            PrimQuartet s;")
-    w("            double Fm[L + 1];")
-    w("            prim_quartet<L>(pb, pk, P, s, Fm);")
-    w("            const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
-    w("            const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
-    w("            const double WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;")
-    w("            const double o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;")
-    w("            (void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;")
-    w("            (void)WQx; (void)WQy; (void)WQz; (void)o2p; (void)o2q; (void)o2pq; (void)rp; (void)rq;")
-    for m in range(L + 1):
-        w("            const double F%d = Fm[%d];" % (m, m))
-    for ln in vrr.lines:
+    for ln in inner:
         w("            " + ln)
-    wt = {"s0": "", "sa": "a2*", "sb": "b2*", "sc": "c2*"}
-    for k, lst in acc.items():
-        for e, f, v in lst:
-            w("            %s_%s_%s += %s%s;" % (k, nm(e), nm(f), wt[k], v))
     w("        }")
     w("    }")
     w("    if constexpr (GS > 1) {")
@@ -486,37 +530,8 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     w("    }")
     w("    QuartetCtx qa = q;")
     w("    qa.active = q.active && sub == 0;   // the group's first lane digests")
-    w("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
-    w("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
-    for h in hrrs.values():
-        for ln in h.lines:
-            w("    " + ln)
-    w("    const double* __restrict__ Dm = P.dense;")
-    w("    const int n = P.nbasis;")
-    w("    const int a0 = q.bfA, b0 = q.bfB, c0 = q.bfC, d0 = q.bfD;")
-    w("    const double hx = P.hybrid;")
-
-    def dl(x, y):
-        return "__ldg(Dm + (size_t)(%s) * n + (%s))" % (x, y)
-    bases = {"a": "a0", "b": "b0", "c": "c0", "d": "d0"}
-    sizes = {"a": na, "b": nb, "c": nc, "d": nd}
-    for blk in ("ab", "cd", "ac", "bd", "ad", "bc"):
-        x, y = blk
-        for i in range(sizes[x]):
-            for j in range(sizes[y]):
-                w("    const double D%s_%d_%d = %s;" % (blk, i, j, dl("%s+%d" % (bases[x], i), "%s+%d" % (bases[y], j))))
-    w("    double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};")
-    for ia in range(na):
-        for ib in range(nb):
-            for ic in range(nc):
-                for id_ in range(nd):
-                    w("    {")
-                    w("        const double g = 4.0*Dab_%d_%d*Dcd_%d_%d - hx*(Dac_%d_%d*Dbd_%d_%d + Dad_%d_%d*Dbc_%d_%d);" % (
-                        ia, ib, ic, id_, ia, ic, ib, id_, ia, id_, ib, ic))
-                    for i in range(3):
-                        da, db, dc = deriv[(ia, ib, ic, id_, i)]
-                        w("        gA[%d] += g*(%s); gB[%d] += g*(%s); gC[%d] += g*(%s);" % (i, da, i, db, i, dc))
-                    w("    }")
+    for ln in tail:
+        w(ln)
     w("    grad_digest<%d>(qa, G, gA, gB, gC);" % part)
     w("}")
     w("};")

@@ -30,7 +30,6 @@
 // weight and its alpha density exceed cut (:163, :170); the operator loop
 // skips row i unless |phi_i + sum dphi_i| > cut (:241).  cut is QUICK's GPU
 // DMCutoff, 1e-9 (src/cuda/gpu.cu:370).
-#include <cublas_v2.h>
 
 #include <cstdarg>
 
@@ -47,6 +46,7 @@
 #include "qb_internal.h"
 #include "xc/xc_api.h"
 #include "xc/xc_functional.cuh"
+#include "xc/xc_gemm.cuh"
 
 namespace qb {
 
@@ -327,15 +327,29 @@ __global__ void xc_point_kernel(XcPointParams q)
     }
 }
 
-// V(f_b, f_a) += M(a, b) for a <= b (lower triangle, column-major).
-__global__ void xc_scatter_kernel(const double* __restrict__ M, int nb, const int* __restrict__ funcs, int n,
-                                  double* __restrict__ V)
+// V(f_b, f_a) += sum_s M_s(a, b) for a <= b (lower triangle, column-major),
+// over the nslice partial products of the split-K GEMM.
+__global__ void xc_scatter_kernel(const double* __restrict__ M, int nb, int nslice, const int* __restrict__ funcs,
+                                  int n, double* __restrict__ V)
 {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= nb * nb) return;
     const int a = idx % nb, b = idx / nb;
     if (a > b) return;
-    V[funcs[b] + (size_t)funcs[a] * n] += M[idx];
+    double m = 0.0;
+    for (int s = 0; s < nslice; s++) m += M[(size_t)s * nb * nb + idx];
+    V[funcs[b] + (size_t)funcs[a] * n] += m;
+}
+
+// K slices of the nb x nb operator GEMM: about two blocks per SM over all
+// slices, at most kXcMaxSlices, each slice at least 256 deep.
+constexpr int kXcMaxSlices = 32;
+static int xc_ksplit(int nb, int K, int nsm)
+{
+    const int tiles = ((nb + 63) / 64) * ((nb + 63) / 64);
+    int s = (2 * nsm + tiles - 1) / tiles;
+    s = std::min(s, std::max(1, K / 256));
+    return std::max(1, std::min(s, kXcMaxSlices));
 }
 
 // Fixed-order sum of two arrays by one block (deterministic).
@@ -414,6 +428,7 @@ struct XcState {
     long long npts = 0;
     std::vector<XcChunk> chunks;
     int maxP = 0, maxNb = 0;
+    int nsm = 148, max_slices = 1;      // SMs of the device; most K slices of any chunk's operator GEMM
     double alg_bytes = 0.0, alg_flops = 0.0, gemm_flops = 0.0;
     XcBuf<double4> d_pts, d_center;
     XcBuf<int4> d_itype;
@@ -421,8 +436,6 @@ struct XcState {
     XcBuf<int> d_funcs;
     // work
     XcBuf<double> d_B, d_Psi, d_T0, d_S, d_L, d_U, d_M, d_e, d_n, d_sum;
-    cublasHandle_t blas = nullptr;
-    XcBuf<unsigned char> d_blas_ws;   // cuBLAS workspace (no allocation inside a capture)
     cudaGraphExec_t graph_exec = nullptr;
     const double* graph_dense = nullptr;
     double* graph_v = nullptr;
@@ -454,11 +467,6 @@ static int xc_fail(int code, const char* fmt, ...)
     do {                                                                                            \
         cudaError_t e_ = (call);                                                                    \
         if (e_ != cudaSuccess) return xc_fail(2, "%s failed: %s", #call, cudaGetErrorString(e_));  \
-    } while (0)
-#define XBL(call)                                                                 \
-    do {                                                                          \
-        cublasStatus_t s_ = (call);                                               \
-        if (s_ != CUBLAS_STATUS_SUCCESS) return xc_fail(2, "%s failed: %d", #call, (int)s_); \
     } while (0)
 
 // Points of one Lebedev-Laikov orbit (octahedral generator codes 1-6).
@@ -724,7 +732,14 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
     XCK(S.d_S.alloc(P * N));
     XCK(S.d_L.alloc(2 * P * N));
     XCK(S.d_U.alloc(N * N));
-    XCK(S.d_M.alloc(N * N));
+    {
+        int dev = 0;
+        XCK(cudaGetDevice(&dev));
+        XCK(cudaDeviceGetAttribute(&S.nsm, cudaDevAttrMultiProcessorCount, dev));
+        S.max_slices = 1;
+        for (const XcChunk& ch : S.chunks) S.max_slices = std::max(S.max_slices, xc_ksplit(ch.nb, 2 * ch.P, S.nsm));
+    }
+    XCK(S.d_M.alloc((size_t)S.max_slices * N * N));
     XCK(S.d_e.alloc(np));
     XCK(S.d_n.alloc(np));
     XCK(S.d_sum.alloc(2));
@@ -744,7 +759,6 @@ static int xc_enqueue(XcState& S, const XcInputs& in, const double* d_dense, dou
     XCK(cudaMemsetAsync(S.d_e.p, 0, std::max<long long>(S.npts, 1) * sizeof(double), st));
     XCK(cudaMemsetAsync(S.d_n.p, 0, std::max<long long>(S.npts, 1) * sizeof(double), st));
     XcBasisParams bp{S.d_center.p, S.d_itype.p, S.d_aexp.p, S.d_dcoeff.p, in.maxcontract};
-    const double one = 1.0, zero = 0.0;
     for (const XcChunk& ch : S.chunks) {
         const int P = ch.P, nb = ch.nb;
         const int* funcs = S.d_funcs.p + ch.f0;
@@ -755,19 +769,24 @@ static int xc_enqueue(XcState& S, const XcInputs& in, const double* d_dense, dou
                                                                         S.d_Psi.p);
         xc_usub_kernel<<<(nb * nb + 255) / 256, 256, 0, st>>>(d_dense, n, funcs, nb, S.d_U.p);
         g_launches += 2;
-        // T0 = U phi, S = U^T psi   (nb x P; U upper triangular: half a GEMM each)
-        XBL(cublasDtrmm(S.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, P,
-                        &one, S.d_U.p, nb, S.d_B.p + blk, nb, S.d_T0.p, nb));
-        XBL(cublasDtrmm(S.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, nb, P,
-                        &one, S.d_U.p, nb, S.d_Psi.p, nb, S.d_S.p, nb));
+        // T0 = U phi, S = U^T psi   (nb x P; U upper triangular: the zero tiles are skipped)
+        xcg::dmma_gemm({S.d_U.p, S.d_B.p + blk, S.d_T0.p, 1, nb, 1, nb, 1, nb, nb, P, nb, 1, 0, 0}, false, true, st);
+        xcg::dmma_gemm({S.d_U.p, S.d_Psi.p, S.d_S.p, nb, 1, 1, nb, 1, nb, nb, P, nb, 2, 0, 0}, true, true, st);
+        g_launches += 2;
         XcPointParams q{pts, P, nb, funcs, d_dense, n, S.d_B.p, S.d_T0.p, S.d_S.p, S.d_L.p, S.d_e.p + ch.p0,
                         S.d_n.p + ch.p0, in.method};
         xc_point_kernel<<<(unsigned)((P * 32 + 127) / 128), 128, 0, st>>>(q);
         ++g_launches;
-        // M = [phi' | chi'] [chi | phi]^T   (nb x nb, k = 2P)
-        XBL(cublasDgemm(S.blas, CUBLAS_OP_N, CUBLAS_OP_T, nb, nb, 2 * P, &one, S.d_L.p, nb, S.d_B.p, nb, &zero,
-                        S.d_M.p, nb));
-        xc_scatter_kernel<<<(nb * nb + 255) / 256, 256, 0, st>>>(S.d_M.p, nb, funcs, n, d_v);
+        // M = [phi' | chi'] [chi | phi]^T   (nb x nb, k = 2P), K split into
+        // slices so the few nb x nb tiles still fill the GPU; the scatter
+        // adds the slices' partial products in a fixed order
+        const int nslice = xc_ksplit(nb, 2 * P, S.nsm);
+        const int kchunk = ((2 * P + nslice - 1) / nslice + xcg::BK - 1) / xcg::BK * xcg::BK;
+        const int used = (2 * P + kchunk - 1) / kchunk;
+        xcg::dmma_gemm({S.d_L.p, S.d_B.p, S.d_M.p, 1, nb, nb, 1, 1, nb, nb, nb, 2 * P, 0, kchunk, (long long)nb * nb},
+                       false, false, st);
+        ++g_launches;
+        xc_scatter_kernel<<<(nb * nb + 255) / 256, 256, 0, st>>>(S.d_M.p, nb, used, funcs, n, d_v);
         ++g_launches;
     }
     xc_reduce_kernel<<<1, 1024, 0, st>>>(S.d_e.p, S.d_n.p, S.npts, S.d_sum.p);
@@ -784,12 +803,6 @@ int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResu
         return xc_fail(1, "gpu_getxc_: method %d has no XC functional (1 = B3LYP, 2 = BLYP)", in.method);
     if (!S.ev[0])
         for (auto& e : S.ev) XCK(cudaEventCreate(&e));
-    if (!S.blas) {
-        XBL(cublasCreate(&S.blas));
-        XCK(S.d_blas_ws.alloc((size_t)32 << 20));
-        XBL(cublasSetWorkspace(S.blas, S.d_blas_ws.p, (size_t)32 << 20));
-    }
-    XBL(cublasSetStream(S.blas, st));
     out->ms_grid = 0.0;
     bool same = S.valid && S.geom_version == in.geom_version && S.nbasis == in.nbasis &&
                 std::equal(S.sigrad2.begin(), S.sigrad2.end(), in.sigrad2);
