@@ -331,6 +331,10 @@ def run_ours(args, ws, rank, local):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    sess.autotune()          # lanes per quartet of the FP32 class kernels, on this build's FP32 lists
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
     barrier(ws)
     m0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     m1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -367,10 +371,24 @@ def run_ours(args, ws, rank, local):
         gr_e2e.append(1e3 * (time.perf_counter() - t0))
         gr_ms.append(sess.grad_stats()["ms"])
     gq = sess.grad_stats()["quartets"]
+    g64 = sess.grad(g_in, D, cm, cutoff, plim)
+    # the same gradient with the mixed split
+    lib.qb_set_mixed_precision(capi.C.c_double(MIXED_CUT))
+    for _ in range(args.warmup):
+        sess.grad(g_in, D, cm, cutoff, plim)
+    grm_ms = []
+    for _ in range(args.steps):
+        gmx = sess.grad(g_in, D, cm, cutoff, plim)
+        grm_ms.append(sess.grad_stats()["ms"])
+    lib.qb_set_mixed_precision(capi.C.c_double(0.0))
+    grm = max_over_ranks(float(np.mean(grm_ms)), ws)
     grad_line = {"metric": "two-electron gradient shell quartets/s (FP64)", "quartets_per_call": gq,
                  "kernel_ms": max_over_ranks(float(np.mean(gr_ms)), ws),
                  "value": gq * ws / (max_over_ranks(float(np.mean(gr_ms)), ws) * 1e-3), "unit": "quartets/s",
                  "e2e_ms_per_call": max_over_ranks(float(np.mean(gr_e2e)), ws),
+                 "mixed": {"kernel_ms": grm, "value": gq * ws / (grm * 1e-3), "cut": MIXED_CUT,
+                           "speedup_vs_fp64": max_over_ranks(float(np.mean(gr_ms)), ws) / grm,
+                           "max_abs_dgrad_vs_fp64": float(np.abs(gmx - g64).max())},
                  "note": "gpu_upload_calculated_/cutoff_/grad_ + gpu_grad_ per call; e2e by host clock"}
 
     mean_eri = float(np.mean(eri_ms))
@@ -432,17 +450,27 @@ def run_scf(args, ws, rank, local):
     import torch
     from quick_b200 import scf
     from quick_b200.molecule import water_cluster
+    from quick_b200 import capi
     torch.cuda.set_device(local)
     m = water_cluster(WORKLOAD["grid"], seed=WORKLOAD["seed"])
     nmol = max(1, min(args.steps, 3))
-    scf.run_rhf_device(m, WORKLOAD["basis"], 1e-10, 1e-20, conv=1e-8, device=local)   # warm-up
+    # one session for every molecule (the library's tables and buffers are
+    # reused); warm-up molecules, all-FP64 and mixed, each followed by the
+    # lane-group autotuner (FP64 class kernels, then FP32 ones)
+    sess = capi.Session(local)
+    scf.run_rhf_device(m, WORKLOAD["basis"], 1e-10, 1e-20, conv=1e-8, device=local, session=sess)
+    sess.autotune()
+    scf.run_rhf_device(m, WORKLOAD["basis"], 1e-10, 1e-20, conv=1e-8, device=local, session=sess,
+                       mixed_cut=MIXED_CUT)
+    sess.autotune()
     res = {}
     for tag, kw in (("fp64", {}), ("mixed", dict(mixed_cut=MIXED_CUT)), ("fp64_delta_d", dict(incremental=True)),
                     ("mixed_delta_d", dict(mixed_cut=MIXED_CUT, incremental=True))):
         secs, runs = [], []
         for _ in range(nmol):
             barrier(ws)
-            r, g = scf.run_rhf_device(m, WORKLOAD["basis"], 1e-10, 1e-20, conv=1e-8, device=local, **kw)
+            r, g = scf.run_rhf_device(m, WORKLOAD["basis"], 1e-10, 1e-20, conv=1e-8, device=local, session=sess,
+                                      **kw)
             secs.append(r.seconds)
             runs.append((r, g))
         r, g = runs[-1]
@@ -464,7 +492,8 @@ def run_scf(args, ws, rank, local):
     ks = []
     for _ in range(2):
         barrier(ws)
-        r, _ = scf.run_rhf_device(alk, "6-31G**", 1e-10, 1e-20, conv=1e-7, device=local, method=1, gradient=False)
+        r, _ = scf.run_rhf_device(alk, "6-31G**", 1e-10, 1e-20, conv=1e-7, device=local, method=1, gradient=False,
+                                  session=sess)
         ks.append(r)
     r = ks[-1]
     kohn_sham = {"workload": "C40H82 6-31G** (1010 basis functions), B3LYP, SG1 grid, seeded torsions",
@@ -478,7 +507,7 @@ def run_scf(args, ws, rank, local):
     for tag, kw in (("fp64_energy", dict(gradient=False)),
                     ("mixed_delta_d", dict(gradient=True, mixed_cut=MIXED_CUT, incremental=True))):
         barrier(ws)
-        r, g = scf.run_rhf_device(m, "cc-pVTZ", 1e-10, 1e-20, conv=1e-7, device=local, **kw)
+        r, g = scf.run_rhf_device(m, "cc-pVTZ", 1e-10, 1e-20, conv=1e-7, device=local, session=sess, **kw)
         tz[tag] = {"seconds_per_molecule": max_over_ranks(r.seconds, ws), "energy": r.energy,
                    "iterations": r.iterations, "converged": bool(r.converged),
                    "phases_s": {k: round(v, 3) for k, v in r.timings.items()}}
@@ -488,6 +517,7 @@ def run_scf(args, ws, rank, local):
     tz["mixed_delta_d"]["abs_dE_vs_fp64_Eh"] = abs(tz["mixed_delta_d"]["energy"] - tz["fp64_energy"]["energy"])
     cc_pvtz = {"workload": "(H2O)32 cc-pVTZ (2080 basis functions), RHF, density RMS 1e-7",
                "variants": tz, "note": "SCF+grad s/mol with f shells (mixed_delta_d); all-FP64 energy for |dE|"}
+    sess.close()
     return {"metric": "SCF+grad s/mol (RHF energy + analytic gradient)", "unit": "s/mol",
             "higher_is_better": False, "value": res[best]["seconds_per_molecule"], "best": best,
             "workload": "(H2O)32 6-31G** (800 basis functions), seeded 4x4x2 cluster",

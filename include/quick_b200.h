@@ -137,11 +137,12 @@ int qb_last_fock_stats(long long* quartets, double* ms_eri, double* ms_screen);
    gradient class kernels in ms. */
 int qb_last_grad_stats(long long* quartets, double* ms);
 
-/* Mixed precision for the following Fock builds (no counterpart in QUICK, which is FP64
-   throughout): shell quartets whose bound Y_ab Y_cd DNMax (QUICK's own screening product,
-   gpu_get2e_subs.h:323-328) is below cut run their Boys function, recurrences and contraction
-   in FP32; the others, and all accumulation into the Fock matrix, stay FP64.  cut = 0 (the
-   default) keeps every quartet in FP64.  Gradients always run in FP64. */
+/* Mixed precision for the following Fock builds and gradients (no counterpart in QUICK, which
+   is FP64 throughout): shell quartets whose bound Y_ab Y_cd DNMax (QUICK's own screening
+   product, gpu_get2e_subs.h:323-328) is below cut run their Boys function, recurrences,
+   contraction and density products in FP32; the others, and all accumulation into the Fock
+   matrix or the gradient, stay FP64.  Classes with an f shell and L sum >= 7 run their FP32
+   list in FP64.  cut = 0 (the default) keeps every quartet in FP64. */
 int qb_set_mixed_precision(double cut);
 
 /* The last Fock build's shell quartets by precision. */
@@ -174,11 +175,13 @@ long long qb_xc_grid(double* xyzw, long long cap);
 int qb_xc_functional(int method, int n, const double* rho, const double* sigma, double* out);
 
 /* No counterpart in QUICK.  Autotunes the lanes per shell quartet of each straight-line Fock
-   class: after a Fock build (gpu_get2e_ or qb_fock_device), times every compiled lane-group
-   size of every class on that build's quartet lists (into a scratch matrix; the Fock matrix
-   is untouched) and keeps the fastest for the following builds of the same molecule (a new
-   gpu_upload_cutoff_matrix_ restores the default choice).  Writes the chosen sizes, one per
-   class, to groups (cap entries at most).  Synchronises the library stream. */
+   class: after a Fock build (gpu_get2e_ or qb_fock_device) or a gradient, times every compiled
+   lane-group size of every class on that call's quartet lists (into a scratch matrix; the Fock
+   matrix is untouched) and keeps the fastest for the following builds.  After an all-FP64 call
+   it tunes the FP64 class kernels, after a call with the mixed split (qb_set_mixed_precision)
+   the FP32 ones on the FP32 lists.  The choice stays for the rest of the session, later
+   molecules included (gpu_shutdown_ forgets it).  Writes the chosen sizes, one per class, to
+   groups (cap entries at most).  Synchronises the library stream. */
 int qb_autotune_classes(int* groups, int cap);
 
 /* Device form of gpu_upload_cutoff_: the integral and primitive cutoffs, and QUICK's density

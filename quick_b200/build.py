@@ -33,7 +33,7 @@ def _extra_flags(src):
     10.5 KB stack frame); -O1 keeps 255 registers and spills about a third as
     much (measured with -Xptxas -v for every class)."""
     b = os.path.basename(src)
-    for pre, lim in (("eri_", 6), ("eri32_", 6), ("grad_", 4)):
+    for pre, lim in (("eri_", 6), ("eri32_", 6), ("grad_", 4), ("grad32_", 4)):
         if b.startswith(pre) and b[len(pre):len(pre) + 4].isdigit():
             if sum(int(ch) for ch in b[len(pre):len(pre) + 4]) >= lim:
                 return ["-Xptxas", "-O1"]

@@ -103,6 +103,7 @@ struct Context {
     std::vector<ScreenClass> screen_cls;
     std::vector<int> class_group;        // lanes per shell quartet of each class kernel
     std::vector<int> class_group32;      // the same for the FP32 class kernels of the mixed split
+    bool tuned64 = false, tuned32 = false;   // set by qb_autotune_classes
     int generic_min_l = 99;              // classes with L sum >= this run the generic kernel (QB_GENERIC_MIN_L)
     // per-iteration
     std::vector<double> o_host;          // O as uploaded (one-electron part)
@@ -392,7 +393,7 @@ static int build_tables(Context& c)
                 PrimRec32 r32;
                 r32.p = (float)p; r32.K = (float)K;
                 r32.PAx = (float)PA[0]; r32.PAy = (float)PA[1]; r32.PAz = (float)PA[2];
-                r32.o2p = (float)(0.5 / p);
+                r32.alpha = (float)a;
                 r32.cp = cp;
                 prim32.push_back(r32);
             }
@@ -452,6 +453,10 @@ static int build_tables(Context& c)
     const double div = gd && atof(gd) > 0 ? atof(gd) : 2.0;
     const char* gm = getenv("QB_GENERIC_MIN_L");
     c.generic_min_l = gm && atoi(gm) > 0 ? atoi(gm) : 99;
+    // lane groups chosen by qb_autotune_classes stay for the following
+    // molecules of the session
+    if (c.tuned64 && c.tuned32) return 0;
+    std::vector<int> keep64 = c.class_group, keep32 = c.class_group32;
     c.class_group.assign(kNumClasses, 1);
     for (int k = 0; k < kNumClasses; k++) {
         double est = type_prims[pair_type_index(kClassL[k][0], kClassL[k][1])] *
@@ -462,6 +467,8 @@ static int build_tables(Context& c)
         c.class_group[k] = std::min(g, class_max_group(k));
     }
     c.class_group32 = c.class_group;
+    if (c.tuned64) c.class_group = keep64;
+    if (c.tuned32) c.class_group32 = keep32;
     return 0;
 }
 
@@ -536,7 +543,7 @@ static int size_quartet_lists(Context& c)
 
 // Screening into the per-class quartet lists for the current density; the
 // class counts come back to the host to size the class launches.
-static int screen_quartets(Context& c, std::vector<int>& cnt)
+static int screen_quartets(Context& c, std::vector<int>& cnt, std::vector<int>& cnt32)
 {
     if (require(c.have_pairs, "gpu_upload_cutoff_matrix_ must precede the two-electron kernels")) return 1;
     if (require(c.have_cutoff, "gpu_upload_cutoff_ must precede the two-electron kernels")) return 1;
@@ -548,15 +555,17 @@ static int screen_quartets(Context& c, std::vector<int>& cnt)
     CK(cudaMemsetAsync(c.d_overflow.p, 0, sizeof(int), c.stream));
     CK(c.d_dense.alloc((size_t)n * n));
     launch_scale_density(c.d_dense_raw.p, c.d_cons.p, c.d_dense.p, n, c.stream);
-    FockParams P = fock_params(c);
-    P.mixed_cut = 0.0;   // the gradient kernels run every quartet in FP64
+    FockParams P = fock_params(c);   // with the mixed split: the FP32 list from the back of each class region
     ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p, c.d_counts32.p};
     launch_screen(S, P, kNumClasses, 0, c.nsm, c.stream);
     launch_finish_counts(S, c.d_class_count.p, c.d_class_count32.p, c.d_overflow.p, kNumClasses, c.stream);
     CK(cudaGetLastError());
     cnt.assign(kNumClasses, 0);
+    cnt32.assign(kNumClasses, 0);
     int ovf = 0;
     CK(cudaMemcpyAsync(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(cnt32.data(), c.d_class_count32.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost,
+                       c.stream));
     CK(cudaMemcpyAsync(&ovf, c.d_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     if (ovf) return set_error(3, "quartet list overflow (internal sizing error)"), 3;
@@ -604,8 +613,8 @@ static int join_side_streams(Context& c)
 // Two-electron gradient into d_grad (3 natom), same quartet lists.
 static int grad_build(Context& c)
 {
-    std::vector<int> cnt;
-    if (int rc = screen_quartets(c, cnt)) return rc;
+    std::vector<int> cnt, cnt32;
+    if (int rc = screen_quartets(c, cnt, cnt32)) return rc;
     CK(c.d_grad.alloc(3 * (size_t)c.natom));
     CK(cudaMemsetAsync(c.d_grad.p, 0, 3 * (size_t)c.natom * sizeof(double), c.stream));
     FockParams P = fock_params(c);
@@ -615,20 +624,25 @@ static int grad_build(Context& c)
         if (!c.ev[k]) CK(cudaEventCreate(&c.ev[k]));
     CK(cudaEventRecord(c.ev[2], c.stream));
     long long total = 0;
-    for (int k = 0; k < kNumClasses; k++) total += cnt[k];
+    for (int k = 0; k < kNumClasses; k++) total += cnt[k] + cnt32[k];
     if (int rc = fork_side_streams(c)) return rc;
     int turn = 0;
-    for (int k = 0; k < kNumClasses; k++) {
-        if (cnt[k] == 0) continue;
-        const int GS = std::min(c.class_group.empty() ? 1 : std::max(c.class_group[k], 1), grad_max_group(k));
-        if (launch_grad_class(k, P, G, GS, cnt[k], c.nsm, side_stream(c, turn++)) < 0) {
-            // the generic kernels share one scratch array: all on the library stream, in order
-            const int* Lk = kClassL[k];
-            if (launch_generic_grad_class(k, Lk[0], Lk[1], Lk[2], Lk[3], P, G, cnt[k], c.nsm, c.stream) < 0)
-                return set_error(2, "gpu_grad_: cannot allocate the scratch of class (%d%d|%d%d)", Lk[0], Lk[1],
-                                 Lk[2], Lk[3]), 2;
+    for (int k = 0; k < kNumClasses; k++)
+        for (int f32 = 0; f32 < 2; f32++) {
+            const int nq = f32 ? cnt32[k] : cnt[k];
+            if (nq == 0) continue;
+            const int GS = std::min(c.class_group.empty() ? 1 : std::max(c.class_group[k], 1), grad_max_group(k));
+            cudaStream_t st = side_stream(c, turn++);
+            const int rc = f32 ? launch_grad_class32(k, P, G, GS, nq, c.nsm, st) : launch_grad_class(k, P, G, GS, nq, c.nsm, st);
+            if (rc < 0) {
+                // the generic kernels (FP64, either list) share one scratch
+                // array: all on the library stream, in order
+                const int* Lk = kClassL[k];
+                if (launch_generic_grad_class(k, Lk[0], Lk[1], Lk[2], Lk[3], P, G, nq, c.nsm, f32, c.stream) < 0)
+                    return set_error(2, "gpu_grad_: cannot allocate the scratch of class (%d%d|%d%d)", Lk[0], Lk[1],
+                                     Lk[2], Lk[3]), 2;
+            }
         }
-    }
     if (int rc = join_side_streams(c)) return rc;
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[3], c.stream));
@@ -1110,6 +1124,7 @@ int qb_autotune_classes(int* groups, int cap)
         }
         groups_k[k] = best_g;
     }
+    (f32 ? c.tuned32 : c.tuned64) = true;
     CK(cudaGetLastError());
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

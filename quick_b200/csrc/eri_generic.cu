@@ -758,6 +758,7 @@ struct GenGradInfo {
     int ne, nf;             // extents of the sums (rows |e| in [elo, LA+LB+1], columns |f| in [flo, LC+LD+1])
     long long per_block;    // scratch doubles per block
     long long x_off[5];     // ket-transformed sums: 2a (c,d), 1 (c,d), 2b (c,d), 2g (c+1,d), 1 (c-1,d)
+    int fp32_list;          // walk the class's FP32 list of the mixed split (evaluated in FP64 here)
 };
 
 __device__ __forceinline__ int gen_gidx(int x, int y, int z, int lo)
@@ -827,8 +828,8 @@ __global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, c
     double* Ec = Eb + nacc;
     __shared__ double red[9][4];
     const int na = g_ncart(I.la), nb = g_ncart(I.lb), nc = g_ncart(I.lc), nd = g_ncart(I.ld);
-    const int n = P.class_count[cls];
-    const int2* list = P.quartets + P.class_offset[cls];
+    const int n = I.fp32_list ? P.class_count32[cls] : P.class_count[cls];
+    const int2* list = I.fp32_list ? P.quartets + (P.class_end[cls] - n) : P.quartets + P.class_offset[cls];
     for (int qi = blockIdx.x; qi < n; qi += gridDim.x) {
         QuartetCtx q;
         load_quartet(P, list[qi], true, q);
@@ -1012,13 +1013,13 @@ void generic_release()
 }
 
 int launch_generic_grad_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, const GradExtra& X, int nq,
-                              int nsm, cudaStream_t st)
+                              int nsm, int fp32_list, cudaStream_t st)
 {
     if (nq <= 0) return 0;
     const int elo = la > 0 ? la - 1 : 0, flo = lc > 0 ? lc - 1 : 0;
     const GenCached* gc = gen_cached(elo, la + lb + 1 - elo, flo, lc + ld + 1 - flo, true);
     if (!gc) return -1;
-    GenGradInfo I{la, lb, lc, ld, elo, flo, gc->G.ne, gc->G.nf, 0, {0, 0, 0, 0, 0}};
+    GenGradInfo I{la, lb, lc, ld, elo, flo, gc->G.ne, gc->G.nf, 0, {0, 0, 0, 0, 0}, fp32_list};
     const long long nacc = (long long)I.ne * I.nf, ndd = g_ncart(ld);
     const long long cols[5] = {g_ncart(lc) * ndd, g_ncart(lc) * ndd, g_ncart(lc) * ndd, g_ncart(lc + 1) * ndd,
                                g_ncart(lc - 1) * ndd};

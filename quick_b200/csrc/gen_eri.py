@@ -392,7 +392,7 @@ def gen_class(la, lb, lc, ld, prec="double"):
     return "\n".join(o) + "\n", stats
 
 
-def gen_grad_class(la, lb, lc, ld, part=0):
+def gen_grad_class(la, lb, lc, ld, part=0, prec="double"):
     """Nuclear gradient of the two-electron energy for one class: derivative
     integrals from exponent-weighted contractions,
       d/dA (ab|cd) = (a+1 b|cd)_{2 alpha} - a_i (a-1 b|cd),
@@ -400,8 +400,14 @@ def gen_grad_class(la, lb, lc, ld, part=0):
       d/dC (ab|cd) = (ab|c+1 d)_{2 gamma} - c_i (ab|c-1 d),   d/dD = -(A+B+C)
     (QUICK: gpu_get2e_subs_grad.h:143-512, storeAA/BB/CC), contracted with
     Gamma = w [4 D_ab D_cd - h (D_ac D_bd + D_ad D_bc)], the sum of the
-    energy's density factors over the eight index permutations."""
+    energy's density factors over the eight index permutations.
+    prec = "float": the FP32 kernel of the mixed split (FP32 primitive and
+    Boys records, recurrences, transfer and density products in FP32; the
+    twelve numbers of a quartet are added to the gradient in FP64)."""
     L = la + lb + lc + ld + 1
+    f32 = prec == "float"
+    R = prec
+    sfx = "f" if f32 else ""
     tag = "%d%d%d%d" % (la, lb, lc, ld) + ("" if part == 0 else "_" + "abc"[part - 1])
     rng = lambda lo, hi: [e for n in range(max(lo, 0), hi + 1) for e in carts(n)]
     want = {"s0": True, "sa": part in (0, 1), "sb": part in (0, 2), "sc": part in (0, 3)}
@@ -409,12 +415,12 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     SAe, SAf = rng(la + 1, la + lb + 1), rng(lc, lc + ld)
     SBe, SBf = rng(la, la + lb + 1), rng(lc, lc + ld)
     SCe, SCf = rng(la, la + lb), rng(lc + 1, lc + ld + 1)
-    vrr = VRR()
+    vrr = VRR(prec)
     acc = {}
     for nmz, es, fs in (("s0", S0e, S0f), ("sa", SAe, SAf), ("sb", SBe, SBf), ("sc", SCe, SCf)):
         if want[nmz]:
             acc[nmz] = [(e, f, None) for e in es for f in fs]
-    hrrs = {k: HRRX(k) for k in acc}
+    hrrs = {k: HRRX(k, prec) for k in acc}
     A, B, Cc, D = QUICK_ORDER[la], QUICK_ORDER[lb], QUICK_ORDER[lc], QUICK_ORDER[ld]
     na, nb, nc, nd = len(A), len(B), len(Cc), len(D)
     deriv = {}
@@ -423,19 +429,19 @@ def gen_grad_class(la, lb, lc, ld, part=0):
             for ic, c in enumerate(Cc):
                 for id_, d in enumerate(D):
                     for i in range(3):
-                        ta = tb = tc = ["0.0"]
+                        ta = tb = tc = ["0.0" + sfx]
                         if want["sa"]:
                             ta = [hrrs["sa"].get(add(a, i), b, c, d)]
                             if a[i] > 0:
-                                ta.append("-%d.0*%s" % (a[i], hrrs["s0"].get(sub(a, i), b, c, d)))
+                                ta.append("-%d.0%s*%s" % (a[i], sfx, hrrs["s0"].get(sub(a, i), b, c, d)))
                         if want["sb"]:
                             tb = [hrrs["sb"].get(a, add(b, i), c, d)]
                             if b[i] > 0:
-                                tb.append("-%d.0*%s" % (b[i], hrrs["s0"].get(a, sub(b, i), c, d)))
+                                tb.append("-%d.0%s*%s" % (b[i], sfx, hrrs["s0"].get(a, sub(b, i), c, d)))
                         if want["sc"]:
                             tc = [hrrs["sc"].get(a, b, add(c, i), d)]
                             if c[i] > 0:
-                                tc.append("-%d.0*%s" % (c[i], hrrs["s0"].get(a, b, sub(c, i), d)))
+                                tc.append("-%d.0%s*%s" % (c[i], sfx, hrrs["s0"].get(a, b, sub(c, i), d)))
                         deriv[(ia, ib, ic, id_, i)] = (" + ".join(ta), " + ".join(tb), " + ".join(tc))
     # only the accumulators the horizontal recurrence reads, and only their
     # vertical-recurrence targets
@@ -450,16 +456,19 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     w('#include "eri_common.cuh"')
     w('#include "grad_common.cuh"')
     w("namespace qb {")
-    w("template <> struct GradEval<%d, %d, %d, %d, %d> {" % (la, lb, lc, ld, part))
+    w("template <> struct %s<%d, %d, %d, %d, %d> {" % ("GradEval32" if f32 else "GradEval", la, lb, lc, ld, part))
     # the primitive-quartet body of run<GS>
-    inner = ["PrimQuartet s;", "double Fm[L + 1];", "prim_quartet<L>(pb, pk, P, s, Fm);",
-             "const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;",
-             "const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;",
-             "const double WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;",
-             "const double o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;",
+    if f32:
+        inner = ["PrimQuartet32 s;", "float Fm[L + 1];", "prim_quartet32r<L>(pb, pk, q, P.boys32, s, Fm);"]
+    else:
+        inner = ["PrimQuartet s;", "double Fm[L + 1];", "prim_quartet<L>(pb, pk, P, s, Fm);"]
+    inner += ["const %s PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;" % R,
+             "const %s QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;" % R,
+             "const %s WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;" % R,
+             "const %s o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;" % R,
              "(void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;",
              "(void)WQx; (void)WQy; (void)WQz; (void)o2p; (void)o2q; (void)o2pq; (void)rp; (void)rq;"]
-    inner += ["const double F%d = Fm[%d];" % (m, m) for m in range(L + 1)]
+    inner += ["const %s F%d = Fm[%d];" % (R, m, m) for m in range(L + 1)]
     inner += list(vrr.lines)
     wt = {"s0": "", "sa": "a2*", "sb": "b2*", "sc": "c2*"}
     for k, lst in acc.items():
@@ -468,7 +477,10 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     # after the contraction: horizontal recurrence, density products, digestion
     tail = []
     t_ = tail.append
-    t_("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
+    if f32:
+        t_("    const float ABx = (float)q.ABx, ABy = (float)q.ABy, ABz = (float)q.ABz, CDx = (float)q.CDx, CDy = (float)q.CDy, CDz = (float)q.CDz;")
+    else:
+        t_("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
     t_("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
     for h in hrrs.values():
         for ln in h.lines:
@@ -476,9 +488,11 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     t_("    const double* __restrict__ Dm = P.dense;")
     t_("    const int n = P.nbasis;")
     t_("    const int a0 = q.bfA, b0 = q.bfB, c0 = q.bfC, d0 = q.bfD;")
-    t_("    const double hx = P.hybrid;")
+    t_("    const %s hx = (%s)P.hybrid;" % (R, R))
 
     def dl(x, y):
+        if f32:
+            return "(float)__ldg(Dm + (size_t)(%s) * n + (%s))" % (x, y)
         return "__ldg(Dm + (size_t)(%s) * n + (%s))" % (x, y)
     bases = {"a": "a0", "b": "b0", "c": "c0", "d": "d0"}
     sizes = {"a": na, "b": nb, "c": nc, "d": nd}
@@ -486,15 +500,15 @@ def gen_grad_class(la, lb, lc, ld, part=0):
         x, y = blk
         for i in range(sizes[x]):
             for j in range(sizes[y]):
-                t_("    const double D%s_%d_%d = %s;" % (blk, i, j, dl("%s+%d" % (bases[x], i), "%s+%d" % (bases[y], j))))
-    t_("    double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0}, gC[3] = {0.0, 0.0, 0.0};")
+                t_("    const %s D%s_%d_%d = %s;" % (R, blk, i, j, dl("%s+%d" % (bases[x], i), "%s+%d" % (bases[y], j))))
+    t_("    %s gA[3] = {0.0%s, 0.0%s, 0.0%s}, gB[3] = {0.0%s, 0.0%s, 0.0%s}, gC[3] = {0.0%s, 0.0%s, 0.0%s};" % ((R,) + (sfx,) * 9))
     for ia in range(na):
         for ib in range(nb):
             for ic in range(nc):
                 for id_ in range(nd):
                     t_("    {")
-                    t_("        const double g = 4.0*Dab_%d_%d*Dcd_%d_%d - hx*(Dac_%d_%d*Dbd_%d_%d + Dad_%d_%d*Dbc_%d_%d);" % (
-                        ia, ib, ic, id_, ia, ic, ib, id_, ia, id_, ib, ic))
+                    t_("        const %s g = 4.0%s*Dab_%d_%d*Dcd_%d_%d - hx*(Dac_%d_%d*Dbd_%d_%d + Dad_%d_%d*Dbc_%d_%d);" % (
+                        R, sfx, ia, ib, ic, id_, ia, ic, ib, id_, ia, id_, ib, ic))
                     for i in range(3):
                         da, db, dc = deriv[(ia, ib, ic, id_, i)]
                         t_("        gA[%d] += g*(%s); gB[%d] += g*(%s); gC[%d] += g*(%s);" % (i, da, i, db, i, dc))
@@ -505,20 +519,29 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     w("    constexpr int L = %d;" % L)
     for k, lst in acc.items():
         for e, f, _ in lst:
-            w("    double %s_%s_%s = 0.0;" % (k, nm(e), nm(f)))
+            w("    %s %s_%s_%s = 0.0%s;" % (R, k, nm(e), nm(f), sfx))
     # GS lanes per quartet stride over the flattened primitive quartets
     w("    const int nk = q.nket, npq = q.nbra * nk;")
     w("    for (int t = (GS == 1 ? 0 : sub); t < npq; t += GS) {")
     w("        const int ib = t / nk, ik = t - ib * nk;")
-    w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
-    w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
-    w("        const double a2 = 2.0 * xb.y;")
-    w("        const double b2 = 2.0 * pb.p - a2;")
-    w("        {")
-    w("            const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
-    w("            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
-    w("            const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
-    w("            const double c2 = 2.0 * xk.y;")
+    if f32:
+        w("        const PrimRec32 pb = load_prim32(P.prim32, q.bra_off + ib);")
+        w("        const float a2 = 2.0f * pb.alpha;")
+        w("        const float b2 = 2.0f * pb.p - a2;")
+        w("        {")
+        w("            const PrimRec32 pk = load_prim32(P.prim32, q.ket_off + ik);")
+        w("            if (!prim_survives(q, pb.cp, pk.cp, P.prim_limit)) continue;")
+        w("            const float c2 = 2.0f * pk.alpha;")
+    else:
+        w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
+        w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
+        w("        const double a2 = 2.0 * xb.y;")
+        w("        const double b2 = 2.0 * pb.p - a2;")
+        w("        {")
+        w("            const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
+        w("            const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
+        w("            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
+        w("            const double c2 = 2.0 * xk.y;")
     for ln in inner:
         w("            " + ln)
     w("        }")
@@ -532,19 +555,24 @@ def gen_grad_class(la, lb, lc, ld, part=0):
     w("    qa.active = q.active && sub == 0;   // the group's first lane digests")
     for ln in tail:
         w(ln)
-    w("    grad_digest<%d>(qa, G, gA, gB, gC);" % part)
+    if f32:
+        w("    const double dA[3] = {gA[0], gA[1], gA[2]}, dB[3] = {gB[0], gB[1], gB[2]}, dC[3] = {gC[0], gC[1], gC[2]};")
+        w("    grad_digest<%d>(qa, G, dA, dB, dC);" % part)
+    else:
+        w("    grad_digest<%d>(qa, G, gA, gB, gC);" % part)
     w("}")
     w("};")
     gs = grad_group_sizes(la, lb, lc, ld)
     w("// lanes per shell quartet compiled for this class: %s" % ", ".join(str(x) for x in gs))
-    w("int launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int GS, int nq, int nsm, cudaStream_t st)" % tag)
+    kname = "grad_class_kernel32" if f32 else "grad_class_kernel"
+    w("int launch_grad%s_%s(const FockParams& P, const GradExtra& G, int cls, int GS, int nq, int nsm, cudaStream_t st)" % ("32" if f32 else "", tag))
     w("{")
     w("    switch (GS) {")
     for x in gs:
-        w("    case %d: { auto kern = grad_class_kernel<%d, %d, %d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, %d, nsm), 128, grad_smem(G), st, P, G, cls); return %d; }"
-          % (x, la, lb, lc, ld, part, x, x, x))
-    w("    default: { auto kern = grad_class_kernel<%d, %d, %d, %d, %d, 1>; QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, grad_smem(G), st, P, G, cls); return 1; }"
-      % (la, lb, lc, ld, part))
+        w("    case %d: { auto kern = %s<%d, %d, %d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, %d, nsm), 128, grad_smem(G), st, P, G, cls); return %d; }"
+          % (x, kname, la, lb, lc, ld, part, x, x, x))
+    w("    default: { auto kern = %s<%d, %d, %d, %d, %d, 1>; QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, grad_smem(G), st, P, G, cls); return 1; }"
+      % (kname, la, lb, lc, ld, part))
     w("    }")
     w("}")
     w("}  // namespace qb")
@@ -555,8 +583,8 @@ def gen_grad_class(la, lb, lc, ld, part=0):
 class HRRX(HRR):
     """HRR over one named accumulator set (prefix_<e>_<f> leaves)."""
 
-    def __init__(self, prefix):
-        HRR.__init__(self)
+    def __init__(self, prefix, prec="double"):
+        HRR.__init__(self, prec)
         self.prefix = prefix
         self.leaves = set()
 
@@ -581,7 +609,7 @@ class HRRX(HRR):
             return name
         self.nflops += 2
         name = "%s_h%s_%s_%s_%s" % (self.prefix, nm(a), nm(b), nm(c), nm(d))
-        self.lines.append("const double %s = %s;" % (name, expr))
+        self.lines.append("const %s %s = %s;" % (self.prec, name, expr))
         self.memo[key] = name
         return name
 
@@ -770,7 +798,10 @@ def main(outdir, lmax=2, lmax_all=3):
             tg = "%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1])
             gstats[tg] = st_
             write_if_changed(os.path.join(outdir, "grad_%s.cu" % tg), src)
+            src32, _ = gen_grad_class(*c, part=pt, prec="float")
+            write_if_changed(os.path.join(outdir, "grad32_%s.cu" % tg), src32)
             gl.append("int launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int GS, int nq, int nsm, cudaStream_t st);" % tg)
+            gl.append("int launch_grad32_%s(const FockParams& P, const GradExtra& G, int cls, int GS, int nq, int nsm, cudaStream_t st);" % tg)
     gl += ["// returns 0, or -1 for a class without a gradient kernel (f shells)",
            "int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int GS, int nq, int nsm, cudaStream_t st)",
            "{", "    switch (cls) {"]
@@ -778,6 +809,16 @@ def main(outdir, lmax=2, lmax_all=3):
         if c not in parts:
             continue
         calls = " ".join("launch_grad_%s(P, G, %d, GS, nq, nsm, st);" % ("%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1]), k)
+                         for pt in parts[c])
+        gl.append("    case %d: %s return 0;" % (k, calls))
+    gl += ["    default: return -1;", "    }", "}"]
+    gl += ["// the FP32 kernels of the mixed split, on the class's FP32 list; -1 as above",
+           "int launch_grad_class32(int cls, const FockParams& P, const GradExtra& G, int GS, int nq, int nsm, cudaStream_t st)",
+           "{", "    switch (cls) {"]
+    for k, c in enumerate(cls_all):
+        if c not in parts:
+            continue
+        calls = " ".join("launch_grad32_%s(P, G, %d, GS, nq, nsm, st);" % ("%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1]), k)
                          for pt in parts[c])
         gl.append("    case %d: %s return 0;" % (k, calls))
     gl += ["    default: return -1;", "    }", "}"]
@@ -790,8 +831,9 @@ def main(outdir, lmax=2, lmax_all=3):
     write_if_changed(os.path.join(outdir, "grad_flops.json"), json.dumps(gstats, indent=1))
     # per-centre files left over from a build with another split threshold
     for f in os.listdir(outdir):
-        if f.startswith("grad_") and f.endswith(".cu") and f != "grad_launch.cu" and f[5:-3] not in gstats:
-            os.remove(os.path.join(outdir, f))
+        for pre in ("grad_", "grad32_"):
+            if f.startswith(pre) and f.endswith(".cu") and f != "grad_launch.cu" and f[len(pre):-3] not in gstats:
+                os.remove(os.path.join(outdir, f))
     # Schwarz kernels, one per pair type
     st = ['#include "eri_common.cuh"', '#include "schwarz.cuh"', '#include "eri_classes.h"', "namespace qb {"]
     for t in pair_types(lmax):

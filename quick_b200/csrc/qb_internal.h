@@ -64,9 +64,12 @@ int launch_generic_class_placed(int cls, int la, int lb, int lc, int ld, const F
 // Forget the fixed-array addresses of qb_fock_device_static (session end).
 void noalloc_reset();
 int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int GS, int nq, int nsm, cudaStream_t st);
+// The FP32 gradient kernels of the mixed split, on the class's FP32 list; -1
+// for a class without a straight-line gradient kernel.
+int launch_grad_class32(int cls, const FockParams& P, const GradExtra& G, int GS, int nq, int nsm, cudaStream_t st);
 // The gradient of a class with an f shell (eri_generic.cu); -1 if its scratch cannot be allocated.
 int launch_generic_grad_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, const GradExtra& X, int nq,
-                              int nsm, cudaStream_t st);
+                              int nsm, int fp32_list, cudaStream_t st);
 void generic_release();
 int grad_max_group(int cls);
 int fma_probe(int fp64, int nsm, double* gflops, cudaStream_t st);

@@ -1,8 +1,9 @@
-"""Mixed-precision Fock builds (qb_set_mixed_precision): quartets whose
-Y_ab Y_cd DNMax bound is below the cut run in FP32.  Checked against the FP64
-oracle: Fock elements within 1e-7 and the two-electron energy
-E2 = 1/2 sum D G within 1e-6 Eh (the 1 micro-Hartree target) at cut 1e-3;
-gradients stay FP64 whatever the setting."""
+"""Mixed-precision Fock builds and gradients (qb_set_mixed_precision):
+quartets whose Y_ab Y_cd DNMax bound is below the cut run in FP32.  Checked
+against the FP64 oracle: Fock elements within 1e-7 and the two-electron
+energy E2 = 1/2 sum D G within 1e-6 Eh (the 1 micro-Hartree target) at cut
+1e-3; the two-electron gradient within 1e-5 Eh/bohr (the gradient target) at
+cut 1e-3, with both lists non-empty; cut 0 gives the FP64 gradient exactly."""
 import numpy as np
 import pytest
 
@@ -39,16 +40,23 @@ def test_mixed_fock_within_tolerance(session, oracle_lib, name):
     assert abs(0.5 * np.sum(D * (got - ref))) < 1e-6
 
 
-def test_mixed_setting_leaves_gradient_fp64(session, oracle_lib):
-    m, b = case("water3_631gss")
+@pytest.mark.parametrize("name", ["water3_631gss", "propane_631gss"])
+def test_mixed_gradient_within_tolerance(session, oracle_lib, name):
+    m, b = case(name)
     Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
     session.upload_molecule(m, b, Y, cp)
     D = random_density(b.nbasis, seed=5, scale=0.05)
     cm = oracle_lib.cutmatrix(b, D)
+    ref = oracle_lib.grad2e(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
     g0 = session.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
     try:
-        session.set_mixed_precision(1e-2)
+        session.set_mixed_precision(1e-3)
         g1 = session.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
+        session.set_mixed_precision(0.0)
+        g2 = session.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
     finally:
         session.set_mixed_precision(0.0)
-    assert np.abs(g1 - g0).max() < 1e-12
+    assert np.abs(g0 - ref).max() < 1e-8
+    assert np.abs(g1 - ref).max() < 1e-5
+    assert np.abs(g1 - g0).max() > 0.0          # the FP32 list was used
+    assert np.abs(g2 - g0).max() < 1e-12        # cut 0: every quartet in FP64 again
