@@ -195,6 +195,14 @@ int qb_upload_cutoff_device(const double* d_dense, double integralCutoff, double
    when the gradient kernels have finished (their quartet counts are read back). */
 int qb_grad_device(const double* d_dense, double* d_grad);
 
+/* Pulay DIIS coefficients on the device, for an SCF iteration that never waits for the host
+   (replaces the host solve of QUICK's electdiis, src/scf.f90:249-523).  d_B: m x m overlaps of
+   the stored error vectors (row-major); d_w: m flags, slot i used when d_w[i] != 0 (unused slots
+   get c_i = 0); d_newest: the slot of the newest Fock matrix (int64), whose coefficient is 1 if
+   the system is singular.  Writes the m coefficients (summing to 1) to d_c.  1 <= m <= 32.
+   Asynchronous on the library stream; can be captured into a CUDA graph. */
+int qb_diis_solve_device(const double* d_B, const double* d_w, int m, const long long* d_newest, double* d_c);
+
 /* One-electron integrals.  QUICK forms these on the host in Fortran; these entry points follow
    the gpu_* conventions (arguments by pointer, Fortran column-major nbasis^2 matrices) and use
    the uploaded basis, coordinates and charges (gpu_upload_xyz_, gpu_upload_atom_and_chg_,

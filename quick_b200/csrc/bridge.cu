@@ -1667,6 +1667,14 @@ int session_view(SessionView* v)
     return 0;
 }
 
+int library_stream(cudaStream_t* st)
+{
+    Context& c = ctx();
+    if (require(c.inited, "gpu_init_ must come first")) return 1;
+    *st = c.stream;
+    return 0;
+}
+
 int report_error(int code, const char* msg)
 {
     set_error(code, "%s", msg);

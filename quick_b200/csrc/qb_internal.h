@@ -34,6 +34,8 @@ struct SessionView {
     cudaStream_t stream;
 };
 int session_view(SessionView* v);
+// The library stream of an initialised session (qb_set_stream or its own).
+int library_stream(cudaStream_t* st);
 int report_error(int code, const char* msg);
 
 void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int count_only, int nsm, cudaStream_t st);

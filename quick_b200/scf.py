@@ -357,9 +357,143 @@ class DeviceRHF:
         self.nfock += 1
         return F
 
-    def run(self, nocc, D0, conv=1e-8, max_iter=100, diis_size=10, incremental=False, rebuild_every=8):
+    def fock_into(self, Dd, Oin, Out):
+        """Out = Oin + G(Dd) with the density screen from Dd (Out may be Oin)."""
+        C = self.C
+        self._rc(self.lib.qb_upload_cutoff_device(self._p(Dd), C.c_double(self.cut), C.c_double(self.plim)))
+        self._rc(self.lib.qb_fock_device(self._p(Dd), self._p(Oin), self._p(Out)))
+        self.nfock += 1
+
+    def run(self, nocc, D0, conv=1e-8, max_iter=100, diis_size=10, incremental=False, rebuild_every=8,
+            graph=False, sp2_iters=48):
+        """graph=True: every iteration after the first is one CUDA-graph replay
+        (Hartree-Fock only; see _run_graph)."""
         with self.torch.cuda.stream(self.stream):
+            if graph:
+                if self.method:
+                    raise ValueError("the graph-captured SCF is Hartree-Fock only (the XC quadrature captures "
+                                     "its own graph)")
+                return self._run_graph(nocc, D0, conv, max_iter, min(diis_size, 32), incremental, rebuild_every,
+                                       sp2_iters)
             return self._run(nocc, D0, conv, max_iter, diis_size, incremental, rebuild_every)
+
+    def _sp2(self, Fo, nocc, iters):
+        """Projector onto the nocc lowest eigenvectors of the symmetric Fo by
+        Niklasson's second-order spectral projection (SP2, Phys. Rev. B 66,
+        155115 (2002)): X0 = (e_max - Fo)/(e_max - e_min) with Gershgorin
+        bounds, then X <- X^2 when tr X > nocc, else X <- 2X - X^2.  Matrix
+        products and a device-side choice only, so it can be captured."""
+        torch = self.torch
+        d = Fo.diagonal()
+        r = Fo.abs().sum(1) - d.abs()
+        emin, emax = (d - r).min(), (d + r).max()
+        eye = torch.eye(Fo.shape[0], **self.opts)
+        X = (emax * eye - Fo) / (emax - emin)
+        for _ in range(iters):
+            X2 = X @ X
+            X = torch.where(X.diagonal().sum() > nocc, X2, 2.0 * X - X2)
+        return X
+
+    def _run_graph(self, nocc, D0, conv, max_iter, M, incremental, rebuild_every, sp2_iters):
+        """The SCF with each iteration captured as a CUDA graph and replayed:
+        density screen and Fock build (full, or incremental F + G(D - D_built)
+        with a full rebuild every rebuild_every iterations: one graph each),
+        the DIIS error X^T (F D S - S D F) X into a ring of M slots, the
+        overlaps of all slots by one GEMM, the Pulay coefficients on the device
+        (qb_diis_solve_device), the extrapolated Fock matrix, and the new
+        density from SP2 purification (_sp2) in place of a diagonalisation.
+        The host reads three scalars per iteration (energy, RMS and largest
+        density change) for QUICK's convergence test; the eigenvectors are
+        formed once, after convergence."""
+        torch = self.torch
+        t_start = time.perf_counter()
+        S, H = self.S, self.H
+        s, U = torch.linalg.eigh(S)
+        keep = s > 1e-4
+        X = U[:, keep] * s[keep].rsqrt()
+        if bool(keep.all()):
+            X = X @ U.T
+        Xt = X.T.contiguous()
+        n = S.shape[0]
+        m = X.shape[1]
+        opts = self.opts
+        D = torch.as_tensor(np.ascontiguousarray(D0), **opts).clone()
+        D_built = torch.zeros_like(D)
+        dIn = torch.zeros_like(D)
+        F2 = torch.zeros_like(D)
+        focks = torch.zeros((M, n, n), **opts)
+        errs = torch.zeros((M, m, m), **opts)
+        it_dev = torch.zeros((), dtype=torch.int64, device=D.device)
+        slot = torch.zeros((), dtype=torch.int64, device=D.device)
+        cvec = torch.zeros(M, **opts)
+        ar = torch.arange(M, device=D.device)
+        stats = torch.zeros(3, **opts)
+        enuc = self.mol.nuclear_repulsion()
+        lib, C = self.lib, self.C
+
+        def step(incr):
+            if incr:
+                torch.sub(D, D_built, out=dIn)
+                self.fock_into(dIn, F2, F2)
+            else:
+                self.fock_into(D, H, F2)
+            D_built.copy_(D)
+            e = 0.5 * (D * (H + F2)).sum()
+            FDS = F2 @ D @ S
+            err = Xt @ (FDS - FDS.T) @ X
+            torch.remainder(it_dev, M, out=slot)
+            focks.index_copy_(0, slot.view(1), F2.unsqueeze(0))
+            errs.index_copy_(0, slot.view(1), err.unsqueeze(0))
+            E = errs.view(M, -1)
+            B = (E @ E.T).contiguous()
+            w = (ar <= it_dev).to(torch.float64)
+            self._rc(lib.qb_diis_solve_device(self._p(B), self._p(w), C.c_int(M), self._p(slot), self._p(cvec)))
+            Fx = (cvec.view(M, 1, 1) * focks).sum(0)
+            P = self._sp2(Xt @ Fx @ X, nocc, sp2_iters)
+            Dn = 2.0 * (X @ P @ Xt)
+            dD = Dn - D
+            stats.copy_(torch.stack([e, dD.square().mean().sqrt(), dD.abs().max()]))
+            D.copy_(Dn)
+            it_dev.add_(1)
+
+        history = []
+        converged = False
+        it = 1
+        # iteration 1 eagerly (it also warms up the library, cuBLAS and the allocator)
+        t0 = time.perf_counter()
+        step(False)
+        vals = stats.cpu().numpy()
+        history.append((float(vals[0]) + enuc, float(vals[1]), time.perf_counter() - t0))
+        if vals[1] < conv and vals[2] < 100.0 * conv:
+            converged = True
+        graphs = {}
+        if not converged:
+            torch.cuda.synchronize()
+            for incr in ((False, True) if incremental else (False,)):
+                g = torch.cuda.CUDAGraph()
+                pool = graphs[False].pool() if graphs else None
+                with torch.cuda.graph(g, stream=self.stream, pool=pool):
+                    step(incr)
+                self.nfock -= 1          # captured, not built
+                graphs[incr] = g
+            for it in range(2, max_iter + 1):
+                t0 = time.perf_counter()
+                graphs[incremental and (it - 1) % rebuild_every != 0].replay()
+                self.nfock += 1
+                vals = stats.cpu().numpy()
+                history.append((float(vals[0]) + enuc, float(vals[1]), time.perf_counter() - t0))
+                if vals[1] < conv and vals[2] < 100.0 * conv:
+                    converged = True
+                    break
+        e_elec = float(vals[0])
+        eps, Cp = torch.linalg.eigh(Xt @ F2 @ X)
+        Cm = X @ Cp
+        self.D_dev, self.C_dev, self.eps_dev = D_built.clone(), Cm, eps
+        torch.cuda.synchronize()
+        graphs.clear()
+        return SCFResult(energy=e_elec + enuc, e_elec=e_elec, e_nuc=enuc, converged=converged, iterations=it,
+                         D=D_built.cpu().numpy(), C=Cm.cpu().numpy(), eps=eps.cpu().numpy(), nocc=nocc,
+                         history=history, seconds=time.perf_counter() - t_start)
 
     def _run(self, nocc, D0, conv, max_iter, diis_size, incremental, rebuild_every):
         torch = self.torch
@@ -460,13 +594,14 @@ _ATOM_DENSITY = {}
 
 
 def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1e-8, gradient=True,
-                   mixed_cut=0.0, incremental=False, device=0, max_iter=100, method=0, session=None):
+                   mixed_cut=0.0, incremental=False, device=0, max_iter=100, method=0, session=None, graph=False):
     """Energy and gradient with the device-resident SCF (DeviceRHF) from the
     SAD guess; atomic densities are cached per (element, basis).  Returns
     (SCFResult, gradient or None); SCFResult.seconds covers guess, set-up,
     SCF and gradient (timings holds each, and the session close apart).  ``session``: an open capi.Session to upload into and keep
     open (molecule after molecule without re-initialising the library); by
-    default a session is opened and closed around the call."""
+    default a session is opened and closed around the call.  graph=True: each
+    SCF iteration after the first is one CUDA-graph replay (DeviceRHF.run)."""
     from .basis import build_basis
     from .capi import Session
     t0 = time.perf_counter()
@@ -484,11 +619,12 @@ def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
     s = Session(device) if own else session
     try:
         s.upload_molecule(mol, b)
+        t_up = time.perf_counter()
         s.set_mixed_precision(mixed_cut)
         eng = DeviceRHF(s, mol, b, integral_cutoff, prim_limit, method=method)
         eng.torch.cuda.synchronize()
         t2 = time.perf_counter()
-        r = eng.run(mol.n_electrons // 2, D0, conv=conv, incremental=incremental, max_iter=max_iter)
+        r = eng.run(mol.n_electrons // 2, D0, conv=conv, incremental=incremental, max_iter=max_iter, graph=graph)
         t3 = time.perf_counter()
         # no exchange-correlation gradient exists on QUICK's GPU path: DFT returns no gradient
         g = eng.gradient() if gradient and not method else None
@@ -505,5 +641,6 @@ def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
     # the work of one molecule; closing the session (freeing the library's
     # device memory, which a long-lived session does once) is reported apart
     r.seconds = t4 - t0
-    r.timings = dict(guess=t1 - t0, setup=t2 - t1, scf=t3 - t2, gradient=t4 - t3, close=time.perf_counter() - t5)
+    r.timings = dict(guess=t1 - t0, setup=t2 - t1, scf=t3 - t2, gradient=t4 - t3, close=time.perf_counter() - t5,
+                     setup_upload=t_up - t1)
     return r, g
