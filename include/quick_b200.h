@@ -70,7 +70,9 @@ void gpu_grad_(double* grad);
 /* src/cuda/gpu.cu:1866-1975: XC quadrature on QUICK's SG1 grid for the method of the last
    gpu_upload_method_ (1 = B3LYP, 2 = BLYP).  Eelxc, aelec and belec are accumulated into; o is
    overwritten with the symmetrised lower triangle of (O as uploaded by gpu_upload_calculated_ +
-   V_xc).  Only isg = 1 (SG1) is accepted: QUICK's GPU path generates no SG0 points. */
+   V_xc).  isg = 1 is QUICK's SG1 grid; isg = 2 (no counterpart in QUICK's GPU path) is a
+   75-radial (Euler-Maclaurin) x 302-point (Lebedev-Laikov) grid per atom with Becke's fuzzy-cell
+   partition.  isg = 0 is rejected: QUICK's GPU path generates no SG0 points. */
 void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double* belec, double* o);
 /* src/cuda/gpu.cu:1446-1479 */
 void gpu_cleanup_(void);
@@ -153,6 +155,19 @@ int qb_last_fock_split(long long* quartets_fp64, long long* quartets_fp32);
    j >= i; not zeroed here) for the density d_dense, and returns the grid sums of the energy
    density and of the alpha density.  sigrad2 is a host array (nbasis), as for gpu_getxc_. */
 int qb_xc_device(const double* d_dense, const double* sigrad2, double* d_vxc, double* exc, double* nalpha);
+
+/* Grid of the following qb_xc_device / qb_xc_grad_device calls: 1 = SG1 (default), 2 = the
+   75 x 302 Becke grid (gpu_getxc_'s isg = 2).  No counterpart in QUICK. */
+int qb_set_xc_grid(int grid);
+
+/* The exchange-correlation term of the nuclear gradient (no counterpart in QUICK: its DFT
+   gradient is commented out, src/optimize.f90:175): adds dE_xc/dR (3 natom, Eh/bohr) to d_grad
+   for the density d_dense (device, column-major nbasis^2, total density), the functional of the
+   last gpu_upload_method_ and the grid of qb_set_xc_grid.  The grid moves with the atoms: the
+   basis-centre terms, the terms of the points moving with their atom and the derivatives of the
+   partition weights (SSW or Becke) are all included, so the result is the derivative of the
+   energy qb_xc_device integrates.  Synchronises the library stream. */
+int qb_xc_grad_device(const double* d_dense, const double* sigrad2, double* d_grad);
 
 /* Statistics of the last XC quadrature: grid points kept (weight above 1e-9), point chunks
    with at least one significant basis function, device time of the per-call phase in ms, and

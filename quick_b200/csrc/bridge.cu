@@ -120,6 +120,8 @@ struct Context {
     double last_ms_grad = 0.0;
     bool stats_pending = false;          // the last Fock build's counts are still on the device
     double mixed_cut = 0.0;      // Fock builds: quartets with Y Y DNMax below this run in FP32 (0: all FP64)
+    int xc_grid = 1;             // grid of qb_xc_device: 1 SG1, 2 the 75 x 302 Becke grid
+    double last_ms_xc_grad = 0.0;
     XcResult last_xc;
     double last_ms_eri = 0, last_ms_screen = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -1168,6 +1170,41 @@ int qb_grad_device(const double* d_dense, double* d_grad)
     return 0;
 }
 
+int qb_xc_grad_device(const double* d_dense, const double* sigrad2, double* d_grad)
+{
+    Context& c = ctx();
+    if (require(c.have_basis && !c.xyz.empty(), "basis and coordinates must be uploaded before qb_xc_grad_device"))
+        return 1;
+    XcInputs in;
+    in.natom = c.natom;
+    in.nbasis = c.nbasis;
+    in.maxcontract = c.maxcontract;
+    in.method = c.method;
+    in.xyz = c.xyz.data();
+    in.iattype = c.iattype.data();
+    in.ncenter = c.ncenter.data();
+    in.itype = c.itype.data();
+    in.ncontract = c.ncontract.data();
+    in.aexp = c.aexp.data();
+    in.dcoeff = c.dcoeff.data();
+    in.sigrad2 = sigrad2;
+    in.geom_version = c.geom_version;
+    in.grid = c.xc_grid;
+    in.stream = c.stream;
+    double ms = 0.0;
+    if (int rc = xc_gradient(in, d_dense, d_grad, &ms)) return rc;
+    c.last_ms_xc_grad = ms;
+    return 0;
+}
+
+int qb_set_xc_grid(int grid)
+{
+    Context& c = ctx();
+    if (grid != 1 && grid != 2) return set_error(1, "qb_set_xc_grid: grid must be 1 (SG1) or 2 (75 x 302 Becke)"), 1;
+    c.xc_grid = grid;
+    return 0;
+}
+
 int qb_xc_device(const double* d_dense, const double* sigrad2, double* d_vxc, double* exc, double* nalpha)
 {
     Context& c = ctx();
@@ -1186,6 +1223,7 @@ int qb_xc_device(const double* d_dense, const double* sigrad2, double* d_vxc, do
     in.dcoeff = c.dcoeff.data();
     in.sigrad2 = sigrad2;
     in.geom_version = c.geom_version;
+    in.grid = c.xc_grid;
     in.stream = c.stream;
     XcResult r;
     if (int rc = xc_quadrature(in, d_dense, d_vxc, &r)) return rc;
@@ -1425,10 +1463,10 @@ void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double*
     Context& c = ctx();
     if (require(c.have_calc, "gpu_upload_calculated_ must precede gpu_getxc_")) return;
     if (require(c.have_basis && !c.xyz.empty(), "basis and coordinates must be uploaded before gpu_getxc_")) return;
-    if (*isg != 1) {
+    if (*isg != 1 && *isg != 2) {
         // QUICK's GPU path builds no grid points for SG0 (gridFormSG0 is
         // commented out, gpu_getxc.cu:117-121) and silently returns zeros.
-        set_error(1, "gpu_getxc_: only the SG1 grid (isg = 1) is implemented, got isg = %d", *isg);
+        set_error(1, "gpu_getxc_: isg must be 1 (SG1) or 2 (75 x 302 Becke grid), got isg = %d", *isg);
         return;
     }
     const size_t nn = (size_t)c.nbasis * c.nbasis;
@@ -1455,6 +1493,7 @@ void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double*
     in.dcoeff = c.dcoeff.data();
     in.sigrad2 = sigrad2;
     in.geom_version = c.geom_version;
+    in.grid = *isg;
     in.stream = c.stream;
     XcResult r;
     if (xc_quadrature(in, c.d_dense_raw.p, c.d_o_out.p, &r)) return;

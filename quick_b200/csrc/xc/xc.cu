@@ -77,12 +77,16 @@ struct XcGridParams {
     const XcShell* shells;
     int nshell;
     int npts;
-    const double4* leb_pts;   // x, y, z, 4 pi w of the four spheres, concatenated
+    const double4* leb_pts;   // x, y, z, 4 pi w of the spheres, concatenated
     const int* leb_off;
     const double4* atoms;     // x, y, z, distance to the nearest other atom
     const double* atom_rad;   // SG-1 radius of each atom
     int natom;
     double4* out;             // x, y, z, weight
+    const double* rgrid;      // radial points and weights in units of the atomic radius
+    const double* rweight;
+    const double* inv_rij;    // natom x natom inverse interatomic distances (Becke partition)
+    int becke;                // 0: Stratmann-Scuseria-Frisch partition (SG1), 1: Becke's
 };
 
 struct XcBasisParams {
@@ -145,6 +149,41 @@ __device__ double ssw_weight(double gx, double gy, double gz, int parent, const 
     return wp / total;
 }
 
+// Becke's fuzzy-cell function (J. Chem. Phys. 88, 2547 (1988)):
+// s(mu) = (1 - p(p(p(mu))))/2 with p(x) = 3x/2 - x^3/2, and its derivative.
+__device__ __forceinline__ double becke_cell(double mu, double* ds = nullptr)
+{
+    const double p1 = 1.5 * mu - 0.5 * mu * mu * mu;
+    const double p2 = 1.5 * p1 - 0.5 * p1 * p1 * p1;
+    const double p3 = 1.5 * p2 - 0.5 * p2 * p2 * p2;
+    if (ds) *ds = -0.5 * (1.5 - 1.5 * p2 * p2) * (1.5 - 1.5 * p1 * p1) * (1.5 - 1.5 * mu * mu);
+    return 0.5 * (1.0 - p3);
+}
+
+// Becke weight of a point owned by atom `parent`: P_parent / sum_C P_C with
+// P_C = prod_{D != C} s(mu_CD), mu_CD = (|r - R_C| - |r - R_D|) / |R_C - R_D|
+// (no atomic-size adjustment).
+__device__ double becke_weight(double gx, double gy, double gz, int parent, const double4* atoms,
+                               const double* inv_rij, int natom)
+{
+    if (natom == 1) return 1.0;
+    double Z = 0.0, Pp = 0.0;
+    for (int i = 0; i < natom; i++) {
+        const double4 I = atoms[i];
+        const double ri = dist3(gx, gy, gz, I.x, I.y, I.z);
+        double Pi = 1.0;
+        for (int j = 0; j < natom && Pi != 0.0; j++) {
+            if (j == i) continue;
+            const double4 J = atoms[j];
+            const double rj = dist3(gx, gy, gz, J.x, J.y, J.z);
+            Pi *= becke_cell((ri - rj) * inv_rij[(size_t)i * natom + j]);
+        }
+        Z += Pi;
+        if (i == parent) Pp = Pi;
+    }
+    return Z > 0.0 ? Pp / Z : 0.0;
+}
+
 __global__ void xc_grid_kernel(XcGridParams p)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -158,9 +197,11 @@ __global__ void xc_grid_kernel(XcGridParams p)
     const double4 ang = p.leb_pts[p.leb_off[s.leb] + (i - s.begin)];
     const double4 A = p.atoms[s.atom];
     const double R = p.atom_rad[s.atom];
-    const double rr = R * c_xc_rgrid[s.rad];
+    const double rr = R * p.rgrid[s.rad];
     const double gx = A.x + rr * ang.x, gy = A.y + rr * ang.y, gz = A.z + rr * ang.z;
-    const double w = ssw_weight(gx, gy, gz, s.atom, p.atoms, p.natom) * ang.w * (R * R * R * c_xc_rweight[s.rad]);
+    const double part = p.becke ? becke_weight(gx, gy, gz, s.atom, p.atoms, p.inv_rij, p.natom)
+                                : ssw_weight(gx, gy, gz, s.atom, p.atoms, p.natom);
+    const double w = part * ang.w * (R * R * R * p.rweight[s.rad]);
     p.out[i] = make_double4(gx, gy, gz, w);
 }
 
@@ -423,6 +464,7 @@ struct XcChunk {
 struct XcState {
     bool valid = false;
     long long geom_version = -1;
+    int grid = 0;                       // grid type of the cached grid (XcInputs::grid)
     std::vector<double> sigrad2;
     int nbasis = 0;
     long long npts = 0;
@@ -431,6 +473,12 @@ struct XcState {
     int nsm = 148, max_slices = 1;      // SMs of the device; most K slices of any chunk's operator GEMM
     double alg_bytes = 0.0, alg_flops = 0.0, gemm_flops = 0.0;
     XcBuf<double4> d_pts, d_center;
+    XcBuf<int> d_parent;                // owning atom of each point
+    XcBuf<double> d_H, d_T4, d_Cb, d_Df, d_fpt;   // gradient work (xc_gradient)
+    XcBuf<int> d_fatom;
+    XcBuf<double4> d_atoms;             // atoms: x, y, z, nearest-neighbour distance
+    XcBuf<double> d_inv_rij;            // natom x natom inverse distances
+    bool becke = false;                 // partition of the cached grid
     XcBuf<int4> d_itype;
     XcBuf<double> d_aexp, d_dcoeff;
     XcBuf<int> d_funcs;
@@ -542,10 +590,11 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
         if (in.iattype[a] < 1 || in.iattype[a] > kXcMaxZ)
             return xc_fail(1, "gpu_getxc_: atom %d has atomic number %d; the SG1 grid covers H..Ar", a + 1,
                            in.iattype[a]);
+    const bool becke = in.grid == 2;
     // Lebedev spheres, weights times 4 pi
     std::vector<double4> leb;
-    std::vector<int> leb_off(4);
-    for (int k = 0; k < 4; k++) {
+    std::vector<int> leb_off(5);
+    for (int k = 0; k < 5; k++) {
         leb_off[k] = (int)leb.size();
         for (int o = 0; o < kXcLebNOrbits[k]; o++) leb_expand(kXcLebOrbits[k][o], leb);
         if ((int)leb.size() - leb_off[k] != kXcLebOrders[k])
@@ -566,26 +615,43 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
         atoms[a] = make_double4(in.xyz[3 * a], in.xyz[3 * a + 1], in.xyz[3 * a + 2], nn);
         arad[a] = kXcRadius[in.iattype[a] - 1];
     }
+    // SG1: 50 radial shells with SG-1's pruned spheres; the Becke grid: 75
+    // shells of 302 points each
     std::vector<XcShell> shells;
     long long total = 0;
+    const int nrad = becke ? kXcRadialBecke : kXcRadial;
     for (int a = 0; a < natom; a++)
-        for (int j = 0; j < kXcRadial; j++) {
-            int k = sg1_leb_index(in.iattype[a], kXcRGrid[j]);
+        for (int j = 0; j < nrad; j++) {
+            int k = becke ? 4 : sg1_leb_index(in.iattype[a], kXcRGrid[j]);
             shells.push_back({a, j, k, (int)total});
             total += kXcLebOrders[k];
         }
+    std::vector<double> rgrid(becke ? kXcRGridBecke : kXcRGrid, (becke ? kXcRGridBecke : kXcRGrid) + nrad);
+    std::vector<double> rweight(becke ? kXcRWeightBecke : kXcRWeight, (becke ? kXcRWeightBecke : kXcRWeight) + nrad);
+    std::vector<double> inv_rij((size_t)natom * natom, 0.0);
+    for (int a = 0; a < natom; a++)
+        for (int b = 0; b < natom; b++)
+            if (a != b) {
+                double dx = in.xyz[3 * a] - in.xyz[3 * b], dy = in.xyz[3 * a + 1] - in.xyz[3 * b + 1],
+                       dz = in.xyz[3 * a + 2] - in.xyz[3 * b + 2];
+                inv_rij[(size_t)a * natom + b] = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+            }
     if (total >= (1LL << 31)) return xc_fail(1, "gpu_getxc_: %lld grid points", total);
     XcBuf<double4> d_leb, d_atoms, d_all;
     XcBuf<int> d_leb_off;
     XcBuf<XcShell> d_shells;
-    XcBuf<double> d_arad;
+    XcBuf<double> d_arad, d_rgrid, d_rweight, d_inv_rij;
+    XCK(d_rgrid.upload(rgrid, st));
+    XCK(d_rweight.upload(rweight, st));
+    XCK(d_inv_rij.upload(inv_rij, st));
     XCK(d_leb.upload(leb, st));
     XCK(d_leb_off.upload(leb_off, st));
     XCK(d_atoms.upload(atoms, st));
     XCK(d_arad.upload(arad, st));
     XCK(d_shells.upload(shells, st));
     XCK(d_all.alloc(total));
-    XcGridParams gp{d_shells.p, (int)shells.size(), (int)total, d_leb.p, d_leb_off.p, d_atoms.p, d_arad.p, natom, d_all.p};
+    XcGridParams gp{d_shells.p, (int)shells.size(), (int)total, d_leb.p, d_leb_off.p, d_atoms.p, d_arad.p, natom, d_all.p,
+                    d_rgrid.p, d_rweight.p, d_inv_rij.p, becke ? 1 : 0};
     XCK(cudaEventRecord(S.ev[2], st));
     xc_grid_kernel<<<(unsigned)((total + 127) / 128), 128, 0, st>>>(gp);
     ++g_launches;
@@ -597,16 +663,27 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
     float ms = 0.f;
     cudaEventElapsedTime(&ms, S.ev[2], S.ev[3]);
     *ms_grid = ms;
-    d_leb.release(); d_leb_off.release(); d_atoms.release(); d_arad.release(); d_shells.release(); d_all.release();
+    d_leb.release(); d_leb_off.release(); d_arad.release(); d_shells.release(); d_all.release();
+    d_rgrid.release(); d_rweight.release();
+    // the atoms and partition tables stay for the weight derivatives of the XC gradient
+    std::swap(S.d_atoms, d_atoms);
+    std::swap(S.d_inv_rij, d_inv_rij);
+    d_atoms.release();
+    d_inv_rij.release();
+    S.becke = becke;
+    std::vector<int> parent_all(total);
+    for (const XcShell& sh : shells)
+        for (int k = 0; k < kXcLebOrders[sh.leb]; k++) parent_all[sh.begin + k] = sh.atom;
 
     const long long kXcChunkPoints = std::min<long long>((long long)env_or("QB_XC_POINTS", kXcChunkPointsDefault), 16384);
     const double kXcCell = env_or("QB_XC_CELL", kXcCellDefault);
     const double kXcChunkSpan = env_or("QB_XC_SPAN", kXcChunkSpanDefault);
     // keep points with weight above the cutoff, sort them into cells
     std::vector<double4> kept;
+    std::vector<int> kept_parent;
     kept.reserve(total);
-    for (auto& p : all)
-        if (p.w > kXcCut) kept.push_back(p);
+    for (long long i = 0; i < total; i++)
+        if (all[i].w > kXcCut) kept.push_back(all[i]), kept_parent.push_back(parent_all[i]);
     const long long np = (long long)kept.size();
     std::vector<unsigned long long> key(np);
     for (long long i = 0; i < np; i++) {
@@ -620,7 +697,8 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
     std::iota(order.begin(), order.end(), 0LL);
     std::stable_sort(order.begin(), order.end(), [&](long long a, long long b) { return key[a] < key[b]; });
     std::vector<double4> pts(np);
-    for (long long i = 0; i < np; i++) pts[i] = kept[order[i]];
+    std::vector<int> parent(np);
+    for (long long i = 0; i < np; i++) pts[i] = kept[order[i]], parent[i] = kept_parent[order[i]];
 
     // chunks: whole cells merged while small and compact, big cells split
     struct Box { double lo[3], hi[3]; };
@@ -720,6 +798,7 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
     std::vector<double> aexp(in.aexp, in.aexp + (size_t)in.maxcontract * nb);
     std::vector<double> dco(in.dcoeff, in.dcoeff + (size_t)in.maxcontract * nb);
     XCK(S.d_pts.upload(pts, st));
+    XCK(S.d_parent.upload(parent, st));
     XCK(S.d_center.upload(center, st));
     XCK(S.d_itype.upload(itp, st));
     XCK(S.d_aexp.upload(aexp, st));
@@ -747,6 +826,7 @@ static int xc_build_grid(XcState& S, const XcInputs& in, double* ms_grid)
     S.npts = np;
     S.nbasis = nb;
     S.geom_version = in.geom_version;
+    S.grid = in.grid;
     S.sigrad2.assign(in.sigrad2, in.sigrad2 + nb);
     S.valid = true;
     return 0;
@@ -795,6 +875,384 @@ static int xc_enqueue(XcState& S, const XcInputs& in, const double* d_dense, dou
     return 0;
 }
 
+// ---------------------------------------------------------------- gradient
+// Nuclear gradient of E_xc = sum_g w_g f(rho_g, sigma_g) (no counterpart in
+// QUICK's GPU path; its CPU DFTgrad is commented out, src/optimize.f90:175).
+// The grid moves with the atoms: point g = R_A(g) + fixed offset, weight
+// w_g = w_radial w_angular W_g with W_g the partition weight.  Then
+//   dE/dR_B = sum_g w_g [v_rho drho_g/dR_B + v_sigma dsigma_g/dR_B]
+//           + sum_g f_g w_radial w_angular dW_g/dR_B,
+// and drho_g/dR_B has a basis-centre part (functions on B, phi(r - R_mu))
+// and a point part (B = A(g)).  With T0 = D phi, T_i = D d_i phi (D the full
+// density block of the chunk) and
+//   c_mu,j(g) = w_g [v_rho d_j phi_mu T0_mu
+//                    + 2 v_sigma sum_i d_i rho (d_j d_i phi_mu T0_mu + d_j phi_mu T_i,mu)],
+// the centre part is -2 sum_g c_mu,j(g) on the atom of mu and the point part
+// +2 sum_mu c_mu,j(g) on A(g).  The partition derivatives are those of
+// Becke's or the Stratmann-Scuseria-Frisch cells (xc_wgrad_kernel).
+
+// phi, its gradient and its Hessian for one chunk (10 blocks, nb x P each):
+// [phi | d_x | d_y | d_z | d_xx | d_xy | d_xz | d_yy | d_yz | d_zz].
+__global__ void xc_basis2_kernel(XcBasisParams B, const double4* __restrict__ pts, int P, const int* __restrict__ funcs,
+                                 int nb, double* __restrict__ H)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)P * nb) return;
+    const int g = (int)(idx / nb), a = (int)(idx - (long long)g * nb);
+    const int f = funcs[a];
+    const double4 pt = pts[g];
+    const double4 c = B.center[f];
+    const int4 t = B.itype[f];
+    const double r[3] = {pt.x - c.x, pt.y - c.y, pt.z - c.z};
+    const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    double out[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (r2 <= c.w) {
+        const double* al = B.aexp + (size_t)f * B.maxcontract;
+        const double* dc = B.dcoeff + (size_t)f * B.maxcontract;
+        double S0 = 0.0, S1 = 0.0, S2 = 0.0;   // sum e, sum -2a e, sum 4a^2 e
+        for (int k = 0; k < t.w; k++) {
+            const double e = dc[k] * exp(-al[k] * r2);
+            S0 += e;
+            S1 -= 2.0 * al[k] * e;
+            S2 += 4.0 * al[k] * al[k] * e;
+        }
+        // x^n, its first and second derivatives, per axis
+        const int n[3] = {t.x, t.y, t.z};
+        double v[3], d1[3], d2[3];
+        for (int q = 0; q < 3; q++) {
+            double p = 1.0;
+            for (int k = 0; k < n[q] - 2; k++) p *= r[q];   // x^(n-2)
+            const double nn = n[q];
+            v[q] = n[q] >= 2 ? p * r[q] * r[q] : (n[q] == 1 ? r[q] : 1.0);
+            d1[q] = n[q] >= 2 ? nn * p * r[q] : (n[q] == 1 ? 1.0 : 0.0);
+            d2[q] = n[q] >= 2 ? nn * (nn - 1.0) * p : 0.0;
+        }
+        const double A = v[0] * v[1] * v[2];
+        out[0] = A * S0;
+        // first derivatives: d_i phi = (d1_i v_j v_k) S0 + A S1 r_i
+        double dA[3];
+        dA[0] = d1[0] * v[1] * v[2];
+        dA[1] = v[0] * d1[1] * v[2];
+        dA[2] = v[0] * v[1] * d1[2];
+        for (int i = 0; i < 3; i++) out[1 + i] = dA[i] * S0 + A * S1 * r[i];
+        // second derivatives: d_i d_j phi = (d_i d_j A) S0 + d_i A S1 r_j + d_j A S1 r_i
+        //                                   + A (S2 r_i r_j + delta_ij S1)
+        int o = 4;
+        for (int i = 0; i < 3; i++)
+            for (int j = i; j < 3; j++) {
+                double dij;
+                if (i == j) {
+                    dij = d2[i];
+                    for (int q = 0; q < 3; q++)
+                        if (q != i) dij *= v[q];
+                } else {
+                    const int k = 3 - i - j;
+                    dij = d1[i] * d1[j] * v[k];
+                }
+                out[o++] = dij * S0 + dA[i] * S1 * r[j] + dA[j] * S1 * r[i] + A * (S2 * r[i] * r[j] + (i == j ? S1 : 0.0));
+            }
+    }
+    const size_t blk = (size_t)nb * P, off = (size_t)g * nb + a;
+    for (int k = 0; k < 10; k++) H[k * blk + off] = out[k];
+}
+
+// Df(a, b) = D(f_a, f_b): the chunk's block of the full density.
+__global__ void xc_dfull_kernel(const double* __restrict__ dense, int n, const int* __restrict__ funcs, int nb,
+                                double* __restrict__ Df)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nb * nb) return;
+    const int a = idx % nb, b = idx / nb;
+    Df[idx] = dense[funcs[a] + (size_t)funcs[b] * n];
+}
+
+struct XcGradPointParams {
+    const double4* pts;
+    const int* parent;          // chunk's slice
+    int P, nb;
+    const double* H;            // 10 blocks (xc_basis2_kernel)
+    const double* T;            // 4 blocks: D phi, D d_x phi, D d_y phi, D d_z phi
+    double* Cb;                 // 3 blocks: c_mu,x, c_mu,y, c_mu,z
+    double* fpt;                // chunk's slice: f per point (0 where the point does not contribute)
+    double* grad;               // 3 natom
+    int method;
+};
+
+// One warp per point: rho, grad rho and the functional, c_mu,j into Cb, and
+// the point part +2 sum_mu c_mu,j onto the point's atom.
+__global__ void xc_gpoint_kernel(XcGradPointParams q)
+{
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (g >= q.P) return;
+    const int nb = q.nb;
+    const size_t blk = (size_t)nb * q.P, o = (size_t)g * nb;
+    const double* phi = q.H + o;
+    double rho = 0.0, gr[3] = {0.0, 0.0, 0.0};
+    for (int a = lane; a < nb; a += 32) {
+        const double t0 = q.T[o + a];
+        rho += phi[a] * t0;
+        for (int i = 0; i < 3; i++) gr[i] += 2.0 * q.H[(1 + i) * blk + o + a] * t0;
+    }
+    rho = warp_sum(rho);
+    for (int i = 0; i < 3; i++) gr[i] = warp_sum(gr[i]);
+    double frho = 0.0, fs4 = 0.0, f = 0.0;
+    // the energy's point test: alpha density above the cutoff
+    const bool ok = 0.5 * rho > kXcCut;
+    if (ok) f = xc_eval(q.method, rho, gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2], &frho, &fs4);
+    const double w = q.pts[g].w, vr = ok ? w * frho : 0.0, vs2 = ok ? 0.5 * w * fs4 : 0.0;   // w v_rho, 2 w v_sigma
+    if (lane == 0) q.fpt[g] = ok ? f : 0.0;
+    double cs[3] = {0.0, 0.0, 0.0};
+    for (int a = lane; a < nb; a += 32) {
+        const double t0 = q.T[o + a];
+        const double ti[3] = {q.T[blk + o + a], q.T[2 * blk + o + a], q.T[3 * blk + o + a]};
+        const double d[3] = {q.H[blk + o + a], q.H[2 * blk + o + a], q.H[3 * blk + o + a]};
+        // Hessian blocks xx, xy, xz, yy, yz, zz
+        const double hxx = q.H[4 * blk + o + a], hxy = q.H[5 * blk + o + a], hxz = q.H[6 * blk + o + a];
+        const double hyy = q.H[7 * blk + o + a], hyz = q.H[8 * blk + o + a], hzz = q.H[9 * blk + o + a];
+        const double h[3][3] = {{hxx, hxy, hxz}, {hxy, hyy, hyz}, {hxz, hyz, hzz}};
+        const double gt = gr[0] * ti[0] + gr[1] * ti[1] + gr[2] * ti[2];
+        for (int j = 0; j < 3; j++) {
+            const double gh = gr[0] * h[j][0] + gr[1] * h[j][1] + gr[2] * h[j][2];
+            const double cj = vr * d[j] * t0 + vs2 * (gh * t0 + d[j] * gt);
+            q.Cb[j * blk + o + a] = cj;
+            cs[j] += cj;
+        }
+    }
+    for (int j = 0; j < 3; j++) cs[j] = warp_sum(cs[j]);
+    if (lane == 0 && ok)
+        for (int j = 0; j < 3; j++) atomicAdd(q.grad + 3 * q.parent[g] + j, 2.0 * cs[j]);
+}
+
+// One thread per function: the centre part -2 sum_g c_mu,j(g) on its atom.
+__global__ void xc_gfunc_kernel(const double* __restrict__ Cb, int P, int nb, const int* __restrict__ funcs,
+                                const int* __restrict__ fatom, double* __restrict__ grad)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nb) return;
+    const size_t blk = (size_t)nb * P;
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int g = 0; g < P; g++)
+        for (int j = 0; j < 3; j++) s[j] += Cb[j * blk + (size_t)g * nb + a];
+    const int A = fatom[funcs[a]];
+    for (int j = 0; j < 3; j++) atomicAdd(grad + 3 * A + j, -2.0 * s[j]);
+}
+
+// Stratmann-Scuseria-Frisch cell function and its derivative (a = 0.64).
+__device__ __forceinline__ double ssf_cell_d(double mu, double* ds)
+{
+    if (mu >= 0.64 || mu <= -0.64) {
+        *ds = 0.0;
+        return mu >= 0.64 ? 0.0 : 1.0;
+    }
+    const double t = mu / 0.64, t2 = t * t;
+    const double g = t * (35.0 + t2 * (-35.0 + t2 * (21.0 - 5.0 * t2))) / 16.0;
+    const double dg = (35.0 + t2 * (-105.0 + t2 * (105.0 - 35.0 * t2))) / 16.0;
+    *ds = -0.5 * dg / 0.64;
+    return 0.5 * (1.0 - g);
+}
+
+__device__ __forceinline__ double cell_d(bool becke, double mu, double* ds)
+{
+    return becke ? becke_cell(mu, ds) : ssf_cell_d(mu, ds);
+}
+
+struct XcWgradParams {
+    const double4* pts;
+    const int* parent;
+    const double* fpt;          // f per point (xc_gpoint_kernel)
+    long long npts;
+    const double4* atoms;       // x, y, z, nearest-neighbour distance
+    const double* inv_rij;
+    int natom;
+    int becke;
+    double* grad;
+};
+
+// The partition part: f_g w_radial w_angular dW_g/dR_B for every atom B.
+// W = P_A / Z, Z = sum_C P_C, P_C = prod_{D != C} s(mu_CD); one warp per
+// point, the per-atom distances and unit vectors in shared memory, lanes over
+// the atoms B, each accumulating B's terms in registers:
+//   as C (= B): k_BX (-e_B - mu_BX e_BX),  as D (= B): k_XB (e_B + mu_BX e_BX),
+// k_CD = f w_ra (delta_CA - W)/Z P_C s'(mu_CD)/s(mu_CD) / R_CD, and the point's
+// atom A receives sum k_CD (e_C - e_D).  e_C = (r - R_C)/|r - R_C|,
+// e_BX = (R_B - R_X)/R_BX; s(-mu) = 1 - s(mu), s'(-mu) = s'(mu).
+__global__ void xc_wgrad_kernel(XcWgradParams p)
+{
+    extern __shared__ double wsm[];
+    const int natom = p.natom;
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    double* sgrad = wsm;                                   // 3 natom
+    double* my = wsm + 3 * natom + (size_t)wib * 5 * natom; // r, ex, ey, ez, P per atom
+    double* rA = my;
+    double* eX = my + natom;
+    double* eY = my + 2 * natom;
+    double* eZ = my + 3 * natom;
+    double* PC = my + 4 * natom;
+    for (int i = threadIdx.x; i < 3 * natom; i += blockDim.x) sgrad[i] = 0.0;
+    __syncthreads();
+    for (long long g = (long long)blockIdx.x * wpb + wib; g < p.npts; g += (long long)gridDim.x * wpb) {
+        const double f = p.fpt[g];
+        if (f == 0.0) continue;   // warp-uniform
+        const double4 pt = p.pts[g];
+        const int A = p.parent[g];
+        for (int x = lane; x < natom; x += 32) {
+            const double4 X = p.atoms[x];
+            const double dx = pt.x - X.x, dy = pt.y - X.y, dz = pt.z - X.z;
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            const double ir = r > 0.0 ? 1.0 / r : 0.0;
+            rA[x] = r; eX[x] = dx * ir; eY[x] = dy * ir; eZ[x] = dz * ir;
+        }
+        __syncwarp();
+        // QUICK's SSW shortcut: W = 1 within 0.18 of the nearest-neighbour distance
+        if (!p.becke && rA[A] < 0.18 * p.atoms[A].w) {
+            __syncwarp();
+            continue;
+        }
+        double zs = 0.0;
+        for (int c = lane; c < natom; c += 32) {
+            double P = 1.0;
+            for (int d = 0; d < natom && P != 0.0; d++) {
+                if (d == c) continue;
+                double ds;
+                P *= cell_d(p.becke, (rA[c] - rA[d]) * p.inv_rij[(size_t)c * natom + d], &ds);
+            }
+            PC[c] = P;
+            zs += P;
+        }
+        const double Z = warp_sum(zs);
+        __syncwarp();
+        if (!(Z > 0.0)) {
+            __syncwarp();
+            continue;
+        }
+        const double W = PC[A] / Z;
+        if (!(W > 0.0)) {
+            __syncwarp();
+            continue;
+        }
+        const double scale = f * (pt.w / W) / Z;   // f w_ra / Z
+        const double thr = 1e-15 * Z;
+        double aA[3] = {0.0, 0.0, 0.0};
+        for (int b = lane; b < natom; b += 32) {
+            double gB[3] = {0.0, 0.0, 0.0};
+            const double4 RB = p.atoms[b];
+            const double kb = scale * ((b == A ? 1.0 : 0.0) - W) * PC[b];
+            for (int x = 0; x < natom; x++) {
+                if (x == b) continue;
+                const double irx = p.inv_rij[(size_t)b * natom + x];
+                const double mu = (rA[b] - rA[x]) * irx;
+                double ds;
+                const double sv = cell_d(p.becke, mu, &ds);
+                if (ds == 0.0) continue;
+                const double4 RX = p.atoms[x];
+                const double ebx[3] = {(RB.x - RX.x) * irx, (RB.y - RX.y) * irx, (RB.z - RX.z) * irx};
+                const double eb[3] = {eX[b], eY[b], eZ[b]};
+                const double ex[3] = {eX[x], eY[x], eZ[x]};
+                // B as C, X as D
+                if (PC[b] > thr && sv > 0.0) {
+                    const double k = kb * ds / sv * irx;
+                    for (int j = 0; j < 3; j++) {
+                        gB[j] += k * (-eb[j] - mu * ebx[j]);
+                        aA[j] += k * (eb[j] - ex[j]);
+                    }
+                }
+                // X as C, B as D: mu_XB = -mu, s(mu_XB) = 1 - sv, s'(mu_XB) = ds
+                if (PC[x] > thr && 1.0 - sv > 0.0) {
+                    const double k = scale * ((x == A ? 1.0 : 0.0) - W) * PC[x] * ds / (1.0 - sv) * irx;
+                    for (int j = 0; j < 3; j++) gB[j] += k * (eb[j] + mu * ebx[j]);
+                }
+            }
+            for (int j = 0; j < 3; j++)
+                if (gB[j] != 0.0) atomicAdd(sgrad + 3 * b + j, gB[j]);
+        }
+        for (int j = 0; j < 3; j++) aA[j] = warp_sum(aA[j]);
+        if (lane == 0)
+            for (int j = 0; j < 3; j++) atomicAdd(sgrad + 3 * A + j, aA[j]);
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * natom; i += blockDim.x)
+        if (sgrad[i] != 0.0) atomicAdd(p.grad + i, sgrad[i]);
+}
+
+// (Re)builds the grid when the geometry, grid type or significance radii changed.
+static int xc_prepare(XcState& S, const XcInputs& in, double* ms_grid)
+{
+    bool same = S.valid && S.geom_version == in.geom_version && S.grid == in.grid && S.nbasis == in.nbasis &&
+                std::equal(S.sigrad2.begin(), S.sigrad2.end(), in.sigrad2);
+    if (!same) {
+        S.valid = false;
+        if (S.graph_exec) cudaGraphExecDestroy(S.graph_exec), S.graph_exec = nullptr;
+        if (int rc = xc_build_grid(S, in, ms_grid)) return rc;
+    }
+    return 0;
+}
+
+int xc_gradient(const XcInputs& in, const double* d_dense, double* d_grad, double* ms)
+{
+    XcState& S = xc_state();
+    cudaStream_t st = in.stream;
+    if (in.method != 1 && in.method != 2)
+        return xc_fail(1, "qb_xc_grad_device: method %d has no XC functional (1 = B3LYP, 2 = BLYP)", in.method);
+    if (!S.ev[0])
+        for (auto& e : S.ev) XCK(cudaEventCreate(&e));
+    double msg = 0.0;
+    if (int rc = xc_prepare(S, in, &msg)) return rc;
+    const int n = in.nbasis, natom = in.natom;
+    const size_t P = S.maxP, N = S.maxNb;
+    XCK(S.d_H.alloc(10 * P * N));
+    XCK(S.d_T4.alloc(4 * P * N));
+    XCK(S.d_Cb.alloc(3 * P * N));
+    XCK(S.d_Df.alloc(N * N));
+    XCK(S.d_fpt.alloc(std::max<long long>(S.npts, 1)));
+    std::vector<int> fatom(n);
+    for (int f = 0; f < n; f++) fatom[f] = in.ncenter[f] - 1;
+    XCK(S.d_fatom.upload(fatom, st));
+    XCK(cudaEventRecord(S.ev[0], st));
+    // points of chunks that no basis function reaches have rho = 0 and f = 0
+    XCK(cudaMemsetAsync(S.d_fpt.p, 0, std::max<long long>(S.npts, 1) * sizeof(double), st));
+    XcBasisParams bp{S.d_center.p, S.d_itype.p, S.d_aexp.p, S.d_dcoeff.p, in.maxcontract};
+    for (const XcChunk& ch : S.chunks) {
+        const int Pc = ch.P, nb = ch.nb;
+        const int* funcs = S.d_funcs.p + ch.f0;
+        const double4* pts = S.d_pts.p + ch.p0;
+        const long long work = (long long)Pc * nb;
+        xc_basis2_kernel<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(bp, pts, Pc, funcs, nb, S.d_H.p);
+        xc_dfull_kernel<<<(nb * nb + 255) / 256, 256, 0, st>>>(d_dense, n, funcs, nb, S.d_Df.p);
+        // [D phi | D d_x phi | D d_y phi | D d_z phi]   (nb x 4P)
+        xcg::dmma_gemm({S.d_Df.p, S.d_H.p, S.d_T4.p, 1, nb, 1, nb, 1, nb, nb, 4 * Pc, nb, 0, 0, 0}, false, true, st);
+        XcGradPointParams q{pts, S.d_parent.p + ch.p0, Pc, nb, S.d_H.p, S.d_T4.p, S.d_Cb.p, S.d_fpt.p + ch.p0, d_grad,
+                            in.method};
+        xc_gpoint_kernel<<<(unsigned)((Pc * 32 + 127) / 128), 128, 0, st>>>(q);
+        xc_gfunc_kernel<<<(nb + 127) / 128, 128, 0, st>>>(S.d_Cb.p, Pc, nb, funcs, S.d_fatom.p, d_grad);
+        g_launches += 5;
+    }
+    // the partition part, over all points
+    const size_t per_warp = 5 * (size_t)natom * sizeof(double), base = 3 * (size_t)natom * sizeof(double);
+    const size_t smem_cap = 200 * 1024;
+    int wpb = (int)std::min<size_t>(4, base + per_warp > smem_cap ? 0 : (smem_cap - base) / per_warp);
+    if (wpb < 1) return xc_fail(1, "qb_xc_grad_device: %d atoms exceed the partition-derivative kernel", natom);
+    const size_t smem = base + wpb * per_warp;
+    XCK(cudaFuncSetAttribute(xc_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, nsm = 148;
+    XCK(cudaGetDevice(&dev));
+    XCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    XcWgradParams wp{S.d_pts.p, S.d_parent.p, S.d_fpt.p, S.npts, S.d_atoms.p, S.d_inv_rij.p, natom, S.becke ? 1 : 0,
+                     d_grad};
+    const long long blocks = std::max<long long>(1, std::min<long long>((S.npts + wpb - 1) / wpb, (long long)nsm * 8));
+    xc_wgrad_kernel<<<(unsigned)blocks, 32 * wpb, smem, st>>>(wp);
+    ++g_launches;
+    XCK(cudaGetLastError());
+    XCK(cudaEventRecord(S.ev[1], st));
+    XCK(cudaStreamSynchronize(st));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, S.ev[0], S.ev[1]);
+    *ms = t;
+    return 0;
+}
+
 int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResult* out)
 {
     XcState& S = xc_state();
@@ -804,13 +1262,7 @@ int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResu
     if (!S.ev[0])
         for (auto& e : S.ev) XCK(cudaEventCreate(&e));
     out->ms_grid = 0.0;
-    bool same = S.valid && S.geom_version == in.geom_version && S.nbasis == in.nbasis &&
-                std::equal(S.sigrad2.begin(), S.sigrad2.end(), in.sigrad2);
-    if (!same) {
-        S.valid = false;
-        if (S.graph_exec) cudaGraphExecDestroy(S.graph_exec), S.graph_exec = nullptr;
-        if (int rc = xc_build_grid(S, in, &out->ms_grid)) return rc;
-    }
+    if (int rc = xc_prepare(S, in, &out->ms_grid)) return rc;
     XCK(cudaEventRecord(S.ev[0], st));
     // the per-call sequence (about 6 launches per chunk) replays from a CUDA
     // graph captured on the first call for these buffers; the legacy
@@ -884,7 +1336,8 @@ void xc_release()
 {
     if (!g_xc) return;
     XcState& S = *g_xc;
-    S.d_pts.release(); S.d_center.release(); S.d_itype.release(); S.d_aexp.release(); S.d_dcoeff.release();
+    S.d_H.release(); S.d_T4.release(); S.d_Cb.release(); S.d_Df.release(); S.d_fpt.release(); S.d_fatom.release();
+    S.d_pts.release(); S.d_parent.release(); S.d_atoms.release(); S.d_inv_rij.release(); S.d_center.release(); S.d_itype.release(); S.d_aexp.release(); S.d_dcoeff.release();
     S.d_funcs.release(); S.d_B.release(); S.d_Psi.release(); S.d_T0.release(); S.d_S.release(); S.d_L.release();
     S.d_U.release(); S.d_M.release();
     S.d_e.release(); S.d_n.release(); S.d_sum.release();

@@ -16,6 +16,7 @@ struct XcInputs {
     const double* dcoeff = nullptr;  // (maxcontract, nbasis), normalised
     const double* sigrad2 = nullptr; // (nbasis)
     long long geom_version = 0;      // changes whenever coordinates or basis change
+    int grid = 1;                    // 1: QUICK's SG1 grid; 2: 75 x 302 grid with Becke's partition
     cudaStream_t stream = nullptr;
 };
 
@@ -40,6 +41,11 @@ struct XcResult {
 // changed.  Returns 0 or a QUICK-bridge status code after reporting the
 // error.
 int xc_quadrature(const XcInputs& in, const double* d_dense, double* d_v, XcResult* out);
+
+// Adds the XC term of the nuclear gradient, dE_xc/dR (3 natom, the grid
+// moving with the atoms, partition derivatives included), to d_grad for the
+// density d_dense; ms: device time.  Synchronises the stream.
+int xc_gradient(const XcInputs& in, const double* d_dense, double* d_grad, double* ms);
 
 // Evaluates the functional (xc_functional.cuh) at n (rho, sigma) pairs on the
 // device: out[3k] = f, out[3k+1] = df/drho, out[3k+2] = 4 df/dsigma.

@@ -300,7 +300,8 @@ class DeviceRHF:
     tensors on the same stream.  Per iteration only the DIIS overlaps and the
     convergence scalars come back to the host."""
 
-    def __init__(self, session, mol, basis, integral_cutoff=1e-10, prim_limit=1e-20, grad_cutoff=None, method=0):
+    def __init__(self, session, mol, basis, integral_cutoff=1e-10, prim_limit=1e-20, grad_cutoff=None, method=0,
+                 xc_grid=1):
         import ctypes as C
 
         import torch
@@ -328,6 +329,8 @@ class DeviceRHF:
         if method:
             from .basis import sigrad2
             self.sg = np.ascontiguousarray(sigrad2(basis))
+            # 1: QUICK's SG1 grid, 2: 75 x 302 points per atom with Becke's partition
+            self._rc(self.lib.qb_set_xc_grid(C.c_int(xc_grid)))
 
     def xc(self, D):
         """(V_xc symmetrised, E_xc) for the device density D (qb_xc_device)."""
@@ -587,6 +590,9 @@ class DeviceRHF:
         self._rc(self.lib.qb_grad1e_device(self._p(D), self._p(W), self._p(g)))
         self._rc(self.lib.qb_upload_cutoff_device(self._p(D), C.c_double(self.grad_cut), C.c_double(self.plim)))
         self._rc(self.lib.qb_grad_device(self._p(D), self._p(g)))
+        if self.method:
+            # the exchange-correlation term (the two-electron one above carries the exchange fraction)
+            self._rc(self.lib.qb_xc_grad_device(self._p(D), self.sg.ctypes.data_as(C.c_void_p), self._p(g)))
         return g.cpu().numpy()
 
 
@@ -594,14 +600,17 @@ _ATOM_DENSITY = {}
 
 
 def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1e-8, gradient=True,
-                   mixed_cut=0.0, incremental=False, device=0, max_iter=100, method=0, session=None, graph=False):
+                   mixed_cut=0.0, incremental=False, device=0, max_iter=100, method=0, session=None, graph=False,
+                   xc_grid=1):
     """Energy and gradient with the device-resident SCF (DeviceRHF) from the
     SAD guess; atomic densities are cached per (element, basis).  Returns
     (SCFResult, gradient or None); SCFResult.seconds covers guess, set-up,
     SCF and gradient (timings holds each, and the session close apart).  ``session``: an open capi.Session to upload into and keep
     open (molecule after molecule without re-initialising the library); by
     default a session is opened and closed around the call.  graph=True: each
-    SCF iteration after the first is one CUDA-graph replay (DeviceRHF.run)."""
+    SCF iteration after the first is one CUDA-graph replay (DeviceRHF.run).
+    method 1 / 2 (B3LYP / BLYP): Kohn-Sham, with the XC term in the gradient;
+    xc_grid 1 = QUICK's SG1 grid, 2 = the 75 x 302 Becke grid."""
     from .basis import build_basis
     from .capi import Session
     t0 = time.perf_counter()
@@ -621,13 +630,12 @@ def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
         s.upload_molecule(mol, b)
         t_up = time.perf_counter()
         s.set_mixed_precision(mixed_cut)
-        eng = DeviceRHF(s, mol, b, integral_cutoff, prim_limit, method=method)
+        eng = DeviceRHF(s, mol, b, integral_cutoff, prim_limit, method=method, xc_grid=xc_grid)
         eng.torch.cuda.synchronize()
         t2 = time.perf_counter()
         r = eng.run(mol.n_electrons // 2, D0, conv=conv, incremental=incremental, max_iter=max_iter, graph=graph)
         t3 = time.perf_counter()
-        # no exchange-correlation gradient exists on QUICK's GPU path: DFT returns no gradient
-        g = eng.gradient() if gradient and not method else None
+        g = eng.gradient() if gradient else None
         t4 = time.perf_counter()
         r.fock_builds = eng.nfock
     finally:

@@ -215,9 +215,64 @@ def test_kohn_sham_scf(method, name):
     r_h, _ = scf.run_rhf_gpu(m, "6-31G*", 1e-11, 1e-20, conv=1e-8, method=method)
     r_d, g_d = scf.run_rhf_device(m, "6-31G*", 1e-11, 1e-20, conv=1e-8, method=method)
     assert r_h.converged and r_d.converged
-    assert g_d is None          # no exchange-correlation gradient on this path
+    assert g_d is not None and np.abs(g_d.reshape(-1, 3).sum(axis=0)).max() < 1e-6   # translational invariance
     assert abs(r_h.energy - gold) < 1e-7
     assert abs(r_d.energy - gold) < 1e-7
+
+
+@pytest.mark.parametrize("xc_grid", [1, 2])
+def test_kohn_sham_gradient_vs_finite_differences(xc_grid):
+    """The B3LYP nuclear gradient (one-electron, two-electron with the 0.2
+    exchange fraction, and the XC term with the grid moving with the atoms:
+    basis-centre, point-movement and partition-weight derivatives) against
+    central differences (h = 1e-3 bohr) of the converged Kohn-Sham energy, on
+    QUICK's SG1 grid (xc_grid 1) and the 75 x 302 Becke grid (2): 1e-5
+    Eh/bohr on six seeded coordinates of a water dimer in 6-31G*."""
+    m = water_cluster((2, 1, 1), seed=3)
+    kw = dict(conv=1e-10, method=1, xc_grid=xc_grid, max_iter=200)
+    r, g = scf.run_rhf_device(m, "6-31G*", 1e-12, 1e-25, **kw)
+    assert r.converged
+    h = 1e-3
+    rng = np.random.default_rng(11)
+    for atom, k in [(int(a), int(c)) for a, c in zip(rng.integers(0, m.natom, 6), rng.integers(0, 3, 6))]:
+        e = []
+        for sgn in (1, -1):
+            x = m.xyz_angstrom.copy()
+            x[atom, k] += sgn * h / A_TO_BOHRS
+            rr, _ = scf.run_rhf_device(Molecule(m.symbols, x), "6-31G*", 1e-12, 1e-25, gradient=False, **kw)
+            e.append(rr.energy)
+        fd = (e[0] - e[1]) / (2 * h)
+        assert abs(g[3 * atom + k] - fd) < 1e-5, (xc_grid, atom, k, g[3 * atom + k], fd)
+    assert np.abs(g.reshape(-1, 3).sum(axis=0)).max() < 1e-6
+
+
+def test_becke_grid_integrates_the_density():
+    """The 75 x 302 Becke grid: its weights integrate a sum of atom-centred
+    Gaussians exp(-|r - R_A|^2) to 1e-7 relative (SG1: 1e-4); the electron
+    count of a converged B3LYP density of a water trimer is 30 to 5e-4 on
+    both grids (QUICK's density cutoffs drop the far tails); the B3LYP energy
+    on the two grids agrees to 1e-3 Eh."""
+    m = water_cluster((3, 1, 1), seed=2)
+    rs, _ = scf.run_rhf_device(m, "6-31G*", 1e-11, 1e-20, conv=1e-8, method=1, xc_grid=1, gradient=False)
+    rb, _ = scf.run_rhf_device(m, "6-31G*", 1e-11, 1e-20, conv=1e-8, method=1, xc_grid=2, gradient=False)
+    assert rs.converged and rb.converged
+    assert abs(rs.energy - rb.energy) < 1e-3
+    b = build_basis(m.symbols, "6-31G*")
+    s = capi.Session(0)
+    try:
+        s.upload_molecule(m, b)
+        from quick_b200.basis import sigrad2
+        sg = np.ascontiguousarray(sigrad2(b))
+        for grid, tol_q in ((2, 1e-7), (1, 1e-4)):
+            _, _, na, nb_ = s.getxc(np.zeros((b.nbasis, b.nbasis), order="F"), rb.D, sg, method=1, isg=grid)
+            assert abs(na + nb_ - m.n_electrons) < 5e-4, (grid, na + nb_)
+            p = s.xc_grid()
+            d2 = ((p[:, None, :3] - m.xyz_bohr.T[None, :, :]) ** 2).sum(axis=2)
+            got = float((p[:, 3] * np.exp(-d2).sum(axis=1)).sum())
+            ref = m.natom * np.pi ** 1.5
+            assert abs(got - ref) < tol_q * ref, (grid, got, ref)
+    finally:
+        s.close()
 
 
 def test_fshell_full_gradient_vs_finite_differences():

@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "quick_b200", "csrc"))
 import gen_xc  # noqa: E402
 
-DEGREE = {6: 3, 38: 9, 86: 11, 194: 17}
+DEGREE = {6: 3, 38: 9, 86: 11, 194: 17, 302: 29}
 
 
 def expand(orbits):
@@ -51,7 +51,7 @@ def sphere_mean(a, b, c):
     return df(a - 1) * df(b - 1) * df(c - 1) / df(a + b + c + 1)
 
 
-@pytest.mark.parametrize("order", [6, 38, 86, 194])
+@pytest.mark.parametrize("order", [6, 38, 86, 194, 302])
 def test_lebedev_exact_to_its_degree(order):
     with open(os.path.join(ROOT, "quick_b200", "data", "lebedev.json")) as fh:
         leb = json.load(fh)
