@@ -210,6 +210,28 @@ int qb_upload_cutoff_device(const double* d_dense, double integralCutoff, double
    when the gradient kernels have finished (their quartet counts are read back). */
 int qb_grad_device(const double* d_dense, double* d_grad);
 
+/* Many molecules in one Fock build / gradient (no counterpart in QUICK, which runs one molecule
+   per process).  Upload each molecule through the bridge as usual (gpu_setup_ ..
+   gpu_upload_cutoff_matrix_), then call qb_batch_add to append its tables; qb_batch_finalize
+   sizes the batch's quartet lists for the given cutoffs.  A batched build is one screen launch
+   and one launch per angular class for all molecules; quartets pair only bras and kets of the
+   same molecule.  Matrices are packed: molecule i's n_i x n_i column-major block at offset
+   off_i = sum_{j<i} n_j^2 (qb_batch_layout returns n_i, natom_i and off_i, and the number of
+   molecules).  Exchange fraction, mixed split and lane groups are the session's settings at the
+   time of the call; the batch keeps its own copies of the tables, so later uploads of other
+   molecules do not change it.  qb_batch_reset frees it.  The batch's work matrices are block
+   diagonal over the total dimension N = sum n_i (2 N^2 doubles; refused above 120 GB). */
+int qb_batch_reset(void);
+int qb_batch_add(void);
+int qb_batch_finalize(double integralCutoff, double primLimit);
+int qb_batch_layout(int* nbasis, int* natom, long long* offsets, int cap);
+/* O_out = O_in + G(D) for every molecule (packed device arrays; the density screen is taken
+   from D).  Asynchronous on the library stream. */
+int qb_batch_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out);
+/* d_grad (3 x sum natom_i, molecule after molecule) += the two-electron gradient of every
+   molecule at the packed density D.  Asynchronous on the library stream. */
+int qb_batch_grad_device(const double* d_dense, double* d_grad);
+
 /* Pulay DIIS coefficients on the device, for an SCF iteration that never waits for the host
    (replaces the host solve of QUICK's electdiis, src/scf.f90:249-523).  d_B: m x m overlaps of
    the stored error vectors (row-major); d_w: m flags, slot i used when d_w[i] != 0 (unused slots

@@ -74,8 +74,10 @@ class Session:
         self._keep.append(x)
         return _ptr(x)
 
-    def upload_molecule(self, mol, basis, YCutoff=None, cutPrim=None):
-        """Start-up uploads; YCutoff / cutPrim default to the GPU Schwarz kernel."""
+    def upload_molecule(self, mol, basis, YCutoff=None, cutPrim=None, pairs=True):
+        """Start-up uploads; YCutoff / cutPrim default to the GPU Schwarz kernel.
+        pairs=False: coordinates, charges and basis only (enough for the
+        one-electron integrals and gradient), no Schwarz bounds or pair list."""
         r = lib()
         b = basis
         self.basis = b
@@ -98,6 +100,8 @@ class Session:
                             self._arr(b.Qsbasis, I32), self._arr(b.Qfbasis, I32), self._arr(b.gccoeff, F64),
                             self._arr(b.cons, F64), self._arr(b.gcexpo, F64), self._arr(b.KLMN, I32))
         check()
+        if not pairs:
+            return
         if YCutoff is None:
             YCutoff, cutPrim = self.schwarz()
         r.gpu_upload_cutoff_matrix_(self._arr(YCutoff, F64), self._arr(cutPrim, F64))

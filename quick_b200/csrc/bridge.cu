@@ -103,6 +103,7 @@ struct Context {
     std::vector<ScreenClass> screen_cls;
     std::vector<int> class_group;        // lanes per shell quartet of each class kernel
     std::vector<int> class_group32;      // the same for the FP32 class kernels of the mixed split
+    HostTables host;                     // host copies of the pair and primitive tables (build_tables)
     bool tuned64 = false, tuned32 = false;   // set by qb_autotune_classes
     int generic_min_l = 99;              // classes with L sum >= this run the generic kernel (QB_GENERIC_MIN_L)
     // per-iteration
@@ -437,9 +438,28 @@ static int build_tables(Context& c)
         s.seg_begin = tseg_begin[tk];
         s.seg_end = tseg_end[tk];
         s.same_type = tb == tk;
+        s.counter = k;
         s.out_offset = 0;
         s.capacity = 0;
     }
+    // host copies of the molecule's tables, for a many-molecule batch (batch.cu)
+    HostTables& h = c.host;
+    h.nbasis = c.nbasis;
+    h.nshell = c.nshell;
+    h.natom = c.natom;
+    h.pbf = pbf;
+    h.psh = psh;
+    h.pY = pY;
+    h.pAB = pAB;
+    h.pA = pA;
+    h.prim = prim;
+    h.prim32 = prim32;
+    h.segs = segs;
+    h.scls = c.screen_cls;
+    h.cons = c.cons;
+    h.shell_atom = satom;
+    h.shell_first.resize(c.nshell + 1);
+    for (int sh = 0; sh <= c.nshell; sh++) h.shell_first[sh] = c.Ksumtype[sh] - 1;
     // lanes per shell quartet: the class's mean primitive quartets before
     // screening (mean primitive pairs of the bra type x of the ket type) over
     // QB_FOCK_GDIV (default 2), rounded down to a power of two and clamped to
@@ -858,6 +878,7 @@ void gpu_shutdown_(void)
     oneint_release();
     generic_release();
     noalloc_reset();
+    batch_release();
     c.d_S1.release();
     c.d_H1.release();
     c.d_D1.release();
@@ -1703,6 +1724,22 @@ int session_view(SessionView* v)
     v->dev_id = c.dev_id;
     v->generic_min_l = c.generic_min_l;
     v->stream = c.stream;
+    return 0;
+}
+
+int session_tables(const HostTables** t, FockParams* P, std::vector<int>* group, std::vector<int>* group32,
+                   int* generic_min_l, int* nsm, int* method, double* mixed_cut)
+{
+    Context& c = ctx();
+    if (require(c.have_pairs && c.have_basis, "a molecule's basis and pair list must be uploaded first")) return 1;
+    *t = &c.host;
+    *P = fock_params(c);
+    *group = c.class_group;
+    *group32 = c.class_group32;
+    *generic_min_l = c.generic_min_l;
+    *nsm = c.nsm;
+    *method = c.method;
+    *mixed_cut = c.mixed_cut;
     return 0;
 }
 

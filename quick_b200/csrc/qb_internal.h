@@ -12,8 +12,24 @@ struct ScreenClass {
     int ket_begin, ket_end;     // ket pairs
     int same_type;              // bra and ket of the same pair type: kets b >= a only
     int seg_begin, seg_end;     // the ket type's constant primitive-count segments (FockParams::ket_segs)
+    int counter;                // angular class: its counters and list region (a batch has one entry
+                                // per molecule and class, all molecules' entries sharing the class's)
     long long out_offset;       // first slot of this class in the quartet buffer
     long long capacity;         // slots reserved for this class
+};
+
+// Host copies of one molecule's device tables (build_tables), for batches.
+struct HostTables {
+    int nbasis = 0, nshell = 0, natom = 0;
+    std::vector<int4> pbf, psh;         // pair tables (FockParams::pair_bf, pair_sh)
+    std::vector<double> pY;
+    std::vector<double4> pAB, pA, prim;
+    std::vector<PrimRec32> prim32;
+    std::vector<int2> segs;             // constant primitive-count segments of each pair type
+    std::vector<ScreenClass> scls;      // one per angular class
+    std::vector<double> cons;           // per basis function
+    std::vector<int> shell_atom;        // 0-based atom of each shell
+    std::vector<int> shell_first;       // first basis function of each shell, nshell + 1 entries
 };
 
 struct ScreenParams {
@@ -34,11 +50,16 @@ struct SessionView {
     cudaStream_t stream;
 };
 int session_view(SessionView* v);
+// The current molecule's host tables and the session settings a batch needs.
+int session_tables(const HostTables** t, FockParams* P, std::vector<int>* group, std::vector<int>* group32,
+                   int* generic_min_l, int* nsm, int* method, double* mixed_cut);
 // The library stream of an initialised session (qb_set_stream or its own).
 int library_stream(cudaStream_t* st);
 int report_error(int code, const char* msg);
 
-void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int count_only, int nsm, cudaStream_t st);
+// ncls screen entries (blockIdx.y); gx blocks per entry (0: 4 per SM)
+void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int count_only, int nsm, cudaStream_t st,
+                   int gx = 0);
 void launch_finish_counts(const ScreenParams& S, int* class_count, int* class_count32, int* overflow, int ncls,
                           cudaStream_t st);
 void launch_scale_density(const double* D, const double* cons, double* Ds, int n, cudaStream_t st);
@@ -65,6 +86,8 @@ int launch_generic_class_placed(int cls, int la, int lb, int lc, int ld, const F
                                 void* mem, size_t cap, cudaStream_t st);
 // Forget the fixed-array addresses of qb_fock_device_static (session end).
 void noalloc_reset();
+// Free a many-molecule batch (batch.cu; session end).
+void batch_release();
 int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int GS, int nq, int nsm, cudaStream_t st);
 // The FP32 gradient kernels of the mixed split, on the class's FP32 list; -1
 // for a class without a straight-line gradient kernel.

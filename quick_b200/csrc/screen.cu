@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const
                 if (tot + tot32 == 0) continue;
                 unsigned long long base = 0, base32 = 0;
                 if (lane == 0) {
-                    if (tot) base = atomicAdd(S.counts + cls, (unsigned long long)tot);
-                    if (tot32) base32 = atomicAdd(S.counts32 + cls, (unsigned long long)tot32);
+                    if (tot) base = atomicAdd(S.counts + c.counter, (unsigned long long)tot);
+                    if (tot32) base32 = atomicAdd(S.counts32 + c.counter, (unsigned long long)tot32);
                 }
                 if (count_only) continue;
                 base = __shfl_sync(FULL, base, 0);
@@ -145,9 +145,10 @@ __global__ void fock_finish_kernel(const double* __restrict__ G, const double* _
     }
 }
 
-void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int count_only, int nsm, cudaStream_t st)
+void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int count_only, int nsm, cudaStream_t st,
+                   int gx)
 {
-    dim3 grid(nsm * 4, ncls);
+    dim3 grid(gx > 0 ? gx : nsm * 4, ncls);
     QB_LAUNCH(screen_kernel, grid, 256, 0, st, S, P, count_only);
 }
 

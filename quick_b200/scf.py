@@ -652,3 +652,211 @@ def run_rhf_device(mol, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
     r.timings = dict(guess=t1 - t0, setup=t2 - t1, scf=t3 - t2, gradient=t4 - t3, close=time.perf_counter() - t5,
                      setup_upload=t_up - t1)
     return r, g
+
+
+def run_batch_rhf(mols, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, conv=1e-8, max_iter=100, diis_size=8,
+                  mixed_cut=0.0, incremental=True, rebuild_every=8, gradient=True, device=0, session=None,
+                  sp2_iters=48):
+    """Closed-shell SCF (and gradient) of many molecules advanced together:
+    every iteration is one batched Fock build for all of them
+    (qb_batch_fock_device: one screen launch and one launch per angular class)
+    and batched dense algebra on zero-padded blocks (torch bmm): DIIS per
+    molecule, and the new density by SP2 purification (DeviceRHF._sp2's
+    scheme, with each padding diagonal set to the block's upper spectral bound
+    so it stays unoccupied).  With incremental=True the builds take
+    D - D_built (full rebuild every rebuild_every iterations), so molecules
+    that have converged add no quartets.  The two-electron gradient is one
+    batched call (qb_batch_grad_device); the one-electron gradient runs per
+    molecule.  Returns (list of SCFResult, list of gradients or None, timings)."""
+    import ctypes as C
+
+    import torch
+
+    from .basis import build_basis
+    from .capi import QuickB200Error, Session, check, lib
+
+    L = lib()
+    t0 = time.perf_counter()
+    own = session is None
+    s = Session(device) if own else session
+    dev = torch.device("cuda", torch.cuda.current_device())
+    opts = dict(dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream()
+    L.qb_set_stream(C.c_void_p(stream.cuda_stream))
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+
+    def rc(v):
+        if v:
+            check()
+            raise QuickB200Error(v, "batched SCF call failed")
+
+    timings = {}
+    try:
+        with torch.cuda.stream(stream):
+            nmol = len(mols)
+            bases = [build_basis(m.symbols, basis_name) for m in mols]
+            ns = [b.nbasis for b in bases]
+            nmax = max(ns)
+            nocc = torch.tensor([m.n_electrons // 2 for m in mols], **opts)
+            S = torch.zeros((nmol, nmax, nmax), **opts)
+            H = torch.zeros((nmol, nmax, nmax), **opts)
+            D = torch.zeros((nmol, nmax, nmax), **opts)
+            rc(L.qb_batch_reset())
+
+            def atom(sym):
+                key = (sym, basis_name)
+                if key not in _ATOM_DENSITY:
+                    _ATOM_DENSITY[key] = gpu_atom_density(sym, basis_name, device, session=s)
+                return _ATOM_DENSITY[key]
+
+            for i, (m, b) in enumerate(zip(mols, bases)):
+                n = b.nbasis
+                s.upload_molecule(m, b)
+                rc(L.qb_batch_add())
+                Si = torch.empty((n, n), **opts)
+                Hi = torch.empty((n, n), **opts)
+                rc(L.qb_oneint_device(p(Si), p(Hi)))
+                S[i, :n, :n] = Si
+                H[i, :n, :n] = Hi
+                D[i, :n, :n] = torch.as_tensor(np.ascontiguousarray(sad_guess(m, b, atom)), **opts)
+            s.set_mixed_precision(mixed_cut)
+            rc(L.qb_batch_finalize(C.c_double(integral_cutoff), C.c_double(prim_limit)))
+            nb_ = np.zeros(nmol, dtype=np.int32)
+            na_ = np.zeros(nmol, dtype=np.int32)
+            off = np.zeros(nmol, dtype=np.int64)
+            L.qb_batch_layout(nb_.ctypes.data_as(C.c_void_p), na_.ctypes.data_as(C.c_void_p),
+                              off.ctypes.data_as(C.c_void_p), C.c_int(nmol))
+            # packed element e = a + b n_i of molecule i <-> padded [i, b, a] (symmetric blocks)
+            idx = np.concatenate([i * nmax * nmax + (np.arange(n)[None, :] * nmax + np.arange(n)[:, None]).T.ravel()
+                                  for i, n in enumerate(ns)])
+            pidx = torch.as_tensor(idx, device=dev)
+            ntot_pk = int(off[-1] + ns[-1] * ns[-1])
+
+            def pack(X):
+                return X.reshape(-1).index_select(0, pidx).contiguous()
+
+            def unpack(x):
+                X = torch.zeros((nmol, nmax, nmax), **opts)
+                X.view(-1).index_copy_(0, pidx, x)
+                return X
+
+            real = torch.zeros((nmol, nmax), dtype=torch.bool, device=dev)
+            for i, n in enumerate(ns):
+                real[i, :n] = True
+            pad = (~real).to(torch.float64)
+            # symmetric orthogonalisers, identity on the padding
+            Sid = S + torch.diag_embed(pad)
+            sv, U = torch.linalg.eigh(Sid)
+            if bool((sv < 1e-4).any()):
+                raise QuickB200Error(1, "run_batch_rhf: an overlap eigenvalue below 1e-4 (use run_rhf_device)")
+            X = U @ torch.diag_embed(sv.rsqrt()) @ U.transpose(1, 2)
+            Xt = X.transpose(1, 2)
+            Hp = pack(H)
+            enuc = torch.tensor([m.nuclear_repulsion() for m in mols], **opts)
+            nel = torch.tensor(ns, **opts) ** 2
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            timings["setup"] = t1 - t0
+            M = diis_size
+            focks = torch.zeros((M, nmol, nmax, nmax), **opts)
+            errs = torch.zeros((M, nmol, nmax, nmax), **opts)
+            F2p = torch.zeros(ntot_pk, **opts)
+            Dbuilt = torch.zeros(ntot_pk, **opts)
+            converged = torch.zeros(nmol, dtype=torch.bool, device=dev)
+            iters = torch.zeros(nmol, dtype=torch.int64, device=dev)
+            e_t = torch.zeros(nmol, **opts)
+            it = 0
+            for it in range(1, max_iter + 1):
+                Dp = pack(D)
+                if incremental and it > 1 and (it - 1) % rebuild_every != 0:
+                    dDp = Dp - Dbuilt
+                    rc(L.qb_batch_fock_device(p(dDp), p(F2p), p(F2p)))
+                else:
+                    rc(L.qb_batch_fock_device(p(Dp), p(Hp), p(F2p)))
+                Dbuilt = Dp
+                F = unpack(F2p)
+                e_t = 0.5 * (D * (H + F)).sum(dim=(1, 2))
+                FDS = F @ D @ S
+                err = Xt @ (FDS - FDS.transpose(1, 2)) @ X
+                slot = (it - 1) % M
+                focks[slot] = F
+                errs[slot] = err
+                m_ = min(it, M)
+                E = errs[:m_].permute(1, 0, 2, 3).reshape(nmol, m_, -1)
+                B = E @ E.transpose(1, 2)
+                A = -torch.ones((nmol, m_ + 1, m_ + 1), **opts)
+                A[:, m_, m_] = 0.0
+                A[:, :m_, :m_] = B
+                rhs = torch.zeros((nmol, m_ + 1), **opts)
+                rhs[:, m_] = -1.0
+                c, info = torch.linalg.solve_ex(A, rhs)
+                c = torch.where((info == 0)[:, None], c[:, :m_],
+                                torch.nn.functional.one_hot(torch.tensor(slot, device=dev), m_).to(torch.float64))
+                Fx = torch.einsum("nm,mnij->nij", c, focks[:m_])
+                Fo = Xt @ Fx @ X
+                # SP2 with the padding parked at the block's upper bound (projector value 0 there)
+                d = Fo.diagonal(dim1=1, dim2=2)
+                r = Fo.abs().sum(2) - d.abs()
+                emin = torch.where(real, d - r, torch.full_like(d, 1e300)).min(1).values
+                emax = torch.where(real, d + r, torch.full_like(d, -1e300)).max(1).values
+                Fo = Fo + torch.diag_embed(pad * emax[:, None])
+                eye = torch.eye(nmax, **opts).expand(nmol, nmax, nmax)
+                P = (emax[:, None, None] * eye - Fo) / (emax - emin)[:, None, None]
+                for _ in range(sp2_iters):
+                    P2 = P @ P
+                    tr = P.diagonal(dim1=1, dim2=2).sum(1)
+                    P = torch.where((tr > nocc)[:, None, None], P2, 2.0 * P - P2)
+                Dn = 2.0 * (X @ P @ Xt)
+                dD = Dn - D
+                drms = (dD.square().sum(dim=(1, 2)) / nel).sqrt()
+                dmax = dD.abs().amax(dim=(1, 2))
+                done = (drms < conv) & (dmax < 100.0 * conv)
+                iters = torch.where(converged, iters, torch.full_like(iters, it))
+                converged = converged | done
+                # a converged molecule keeps the density of its last build (its energy's)
+                D = torch.where(converged[:, None, None], D, Dn)
+                if bool(converged.all()):
+                    break
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            timings["scf"] = t2 - t1
+            energy = (e_t + enuc).cpu().numpy()
+            # D is the density of the last build for converged molecules
+            Dfin = unpack(Dbuilt)
+            grads = None
+            if gradient:
+                g2 = torch.zeros(3 * int(na_.sum()), **opts)
+                rc(L.qb_batch_grad_device(p(Dbuilt), p(g2)))
+                # W = 2 sum_occ e_k C_k C_k^T from the last Fock matrix
+                eps, Cp = torch.linalg.eigh(Xt @ F @ X + torch.diag_embed(pad * 1e6))
+                Cm = X @ Cp
+                occ = (torch.arange(nmax, device=dev)[None, :] < nocc[:, None]).to(torch.float64)
+                W = 2.0 * (Cm * (occ * eps)[:, None, :]) @ Cm.transpose(1, 2)
+                g2h = g2.cpu().numpy()
+                grads = []
+                a0 = 0
+                for i, (m, b) in enumerate(zip(mols, bases)):
+                    n = b.nbasis
+                    s.upload_molecule(m, b, pairs=False)
+                    gi = torch.zeros(3 * m.natom, **opts)
+                    Di = Dfin[i, :n, :n].contiguous()
+                    Wi = W[i, :n, :n].contiguous()
+                    rc(L.qb_grad1e_device(p(Di), p(Wi), p(gi)))
+                    grads.append(gi.cpu().numpy() + g2h[3 * a0:3 * (a0 + m.natom)])
+                    a0 += m.natom
+            torch.cuda.synchronize()
+            timings["gradient"] = time.perf_counter() - t2
+            conv_h = converged.cpu().numpy()
+            it_h = iters.cpu().numpy()
+            Dh = Dfin.cpu().numpy()
+            results = [SCFResult(energy=float(energy[i]), e_elec=float(energy[i] - enuc[i]), e_nuc=float(enuc[i]),
+                                 converged=bool(conv_h[i]), iterations=int(it_h[i]),
+                                 D=Dh[i, :ns[i], :ns[i]], C=None, eps=None, nocc=mols[i].n_electrons // 2,
+                                 history=[], seconds=0.0) for i in range(nmol)]
+    finally:
+        L.qb_batch_reset()
+        L.qb_set_stream(None)
+        if own:
+            s.close()
+    timings["total"] = time.perf_counter() - t0
+    return results, grads, timings
