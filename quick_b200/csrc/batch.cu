@@ -84,7 +84,7 @@ struct Batch {
     Buf<unsigned long long> counts, counts32;
     Buf<int> ccount, ccount32, overflow;
     Buf<long long> coff, cend;
-    Buf<int2> quartets;
+    Buf<Quartet> quartets;
     void release()
     {
         prim.release(); pAB.release(); pA.release(); prim32.release(); pbf.release(); psh.release();

@@ -95,7 +95,7 @@ struct Context {
     DevBuf<unsigned long long> d_counts, d_counts32;
     DevBuf<int> d_class_count, d_class_count32, d_overflow;
     DevBuf<long long> d_class_offset, d_class_end;
-    DevBuf<int2> d_quartets;
+    DevBuf<Quartet> d_quartets;
     DevBuf<int2> d_ket_segs;             // constant primitive-count segments of the pair table
     DevBuf<double> d_S1, d_H1, d_D1, d_W1, d_g1;   // host-pointer one-electron entry points
     DevBuf<int> d_shell_first;                      // Ksumtype - 1 (nshell + 1), for the device density screen

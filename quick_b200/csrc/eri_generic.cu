@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(256) fock_generic_kernel(const FockParams P, i
     extern __shared__ double sm[];
     const int tid = threadIdx.x, nt = blockDim.x;
     const int n = fp32_list ? P.class_count32[cls] : P.class_count[cls];
-    const int2* list = fp32_list ? P.quartets + (P.class_end[cls] - n) : P.quartets + P.class_offset[cls];
+    const Quartet* list = fp32_list ? P.quartets + (P.class_end[cls] - n) : P.quartets + P.class_offset[cls];
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
         QuartetCtx q;
         load_quartet(P, list[i], true, q);
@@ -829,7 +829,7 @@ __global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, c
     __shared__ double red[9][4];
     const int na = g_ncart(I.la), nb = g_ncart(I.lb), nc = g_ncart(I.lc), nd = g_ncart(I.ld);
     const int n = I.fp32_list ? P.class_count32[cls] : P.class_count[cls];
-    const int2* list = I.fp32_list ? P.quartets + (P.class_end[cls] - n) : P.quartets + P.class_offset[cls];
+    const Quartet* list = I.fp32_list ? P.quartets + (P.class_end[cls] - n) : P.quartets + P.class_offset[cls];
     for (int qi = blockIdx.x; qi < n; qi += gridDim.x) {
         QuartetCtx q;
         load_quartet(P, list[qi], true, q);

@@ -131,8 +131,8 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
         return fail(4, "qb_fock_device_static: %d basis functions and the f-shell class programs need %zu bytes "
                        "before any quartet; the fixed array holds %zu bytes (use qb_fock_device)", n, off,
                     kFockScratchBytes);
-    auto* quartets = (int2*)(base + off);
-    const long long qcap = (long long)((kFockScratchBytes - off) / sizeof(int2));
+    auto* quartets = (Quartet*)(base + off);
+    const long long qcap = (long long)((kFockScratchBytes - off) / sizeof(Quartet));
 
     std::vector<long long> offs(ncls);
     long long total = 0;

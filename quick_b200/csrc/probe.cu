@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(256) count_prims_kernel(const FockParams P, in
 {
     const int cls = blockIdx.y;
     const int n = P.class_count[cls];
-    const int2* list = P.quartets + P.class_offset[cls];
+    const Quartet* list = P.quartets + P.class_offset[cls];
     unsigned long long mine = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         QuartetCtx q;

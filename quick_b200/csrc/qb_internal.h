@@ -35,7 +35,7 @@ struct HostTables {
 struct ScreenParams {
     const ScreenClass* cls;
     unsigned long long* counts;     // FP64 quartets per class (from the front of the region)
-    int2* out;
+    Quartet* out;
     unsigned long long* counts32;   // FP32 quartets per class (from the back), mixed precision only
 };
 

@@ -51,10 +51,12 @@ __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const
                 int4 sb = make_int4(0, 0, 0, 0);
                 if (!count_only && b < seg.y) sb = P.pair_sh[b];
                 unsigned m[kScreenTile], m32[kScreenTile];
+                double dnm[kScreenTile];
                 int tot = 0, tot32 = 0;
 #pragma unroll
                 for (int t = 0; t < kScreenTile; t++) {
                     bool pass = false, low = false;
+                    dnm[t] = 0.0;
                     // same pair type: kets b >= a only
                     if (t < nt && b < seg.y && (!c.same_type || b >= a0 + t)) {
                         const double yy = Yb * Ya[t];
@@ -62,7 +64,8 @@ __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const
                             if (count_only) {
                                 pass = true;
                             } else {
-                                const double bound = yy * dn_max(P, sa[t].x, sa[t].y, sb.x, sb.y);
+                                dnm[t] = dn_max(P, sa[t].x, sa[t].y, sb.x, sb.y);
+                                const double bound = yy * dnm[t];
                                 pass = bound > cut;
                                 low = pass && bound < P.mixed_cut;
                             }
@@ -86,11 +89,11 @@ __global__ void __launch_bounds__(256) screen_kernel(const ScreenParams S, const
                 for (int t = 0; t < kScreenTile; t++) {
                     if ((m[t] >> lane) & 1u) {
                         const unsigned long long pos = base + __popc(m[t] & below);
-                        if (pos < (unsigned long long)c.capacity) S.out[c.out_offset + pos] = make_int2(a0 + t, b);
+                        if (pos < (unsigned long long)c.capacity) S.out[c.out_offset + pos] = Quartet{a0 + t, b, dnm[t]};
                     } else if ((m32[t] >> lane) & 1u) {
                         const unsigned long long pos = base32 + __popc(m32[t] & below);
                         if (pos < (unsigned long long)c.capacity)
-                            S.out[c.out_offset + c.capacity - 1 - pos] = make_int2(a0 + t, b);
+                            S.out[c.out_offset + c.capacity - 1 - pos] = Quartet{a0 + t, b, dnm[t]};
                     }
                     base += __popc(m[t]);
                     base32 += __popc(m32[t]);
