@@ -205,6 +205,34 @@ static void boys_table(std::vector<double>& tab)
         }
 }
 
+// FP32 records on the finer grid T_k = k/64: F_L, F_{L+1}, F_{L+2}, e^-T_k
+// for L <= kBoysLMax, by the same series and downward recursion.
+static void boys_table32(std::vector<float>& tab)
+{
+    tab.assign(kBoys32Size, 0.0f);
+    const int mtop = kBoysLMax + 2;
+    for (int k = 0; k < kBoys32Points; k++) {
+        long double T = (long double)k / kBoys32PerUnit;
+        long double term = 1.0L / (2 * mtop + 1), sum = term;
+        for (int j = 1; j < 2000; j++) {
+            term *= 2.0L * T / (2 * mtop + 2 * j + 1);
+            sum += term;
+            if (term < sum * 1e-22L) break;
+        }
+        long double e = expl(-T);
+        std::vector<long double> F(mtop + 1);
+        F[mtop] = e * sum;
+        for (int m = mtop - 1; m >= 0; m--) F[m] = (2.0L * T * F[m + 1] + e) / (2 * m + 1);
+        for (int L = 0; L <= kBoysLMax; L++) {
+            float* r = tab.data() + ((size_t)L * kBoys32Points + k) * 4;
+            r[0] = (float)F[L];
+            r[1] = (float)F[L + 1];
+            r[2] = (float)F[L + 2];
+            r[3] = (float)e;
+        }
+    }
+}
+
 // ------------------------------------------------------------- pair list
 // QUICK's shell-pair list (gpu.cu:401-1003, sort_method 0), restated with
 // stable sorts.  QUICK bubble-sorts each (q,p) class with strict
@@ -818,14 +846,8 @@ void gpu_init_(void)
     if (!c.stream) c.stream = c.own_stream;
     std::vector<double> tab;
     boys_table(tab);
-    // FP32 records: F_L .. F_{L+4}, e^-T_k, two pad floats
-    std::vector<float> tab32(kBoys32Size, 0.0f);
-    for (int L = 0; L <= kBoysLMax; L++)
-        for (int k = 0; k < kBoysPoints; k++) {
-            float* r = tab32.data() + ((size_t)L * kBoysPoints + k) * 8;
-            for (int j = 0; j < 5; j++) r[j] = (float)tab[(size_t)k * kBoysCols + L + j];
-            r[5] = (float)tab[(size_t)k * kBoysCols + kBoysExpCol];
-        }
+    std::vector<float> tab32;
+    boys_table32(tab32);
     if (c.d_boys.alloc(tab.size()) != cudaSuccess ||
         cudaMemcpy(c.d_boys.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
         c.d_boys32.alloc(tab32.size()) != cudaSuccess ||
