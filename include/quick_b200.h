@@ -76,9 +76,18 @@ void gpu_grad_(double* grad);
 void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double* belec, double* o);
 /* src/cuda/gpu.cu:1446-1479 */
 void gpu_cleanup_(void);
-/* src/cuda/gpu.cu:1559-1801, 1991-2237: the conventional (stored-integral) path is not built;
-   these report that and record an error. */
+/* src/cuda/gpu.cu:1991-2237: QUICK's conventional (stored-integral) SCF.  Computes every unique
+   integral (ij|kl) of the shell quartets with Y_ij Y_kl > leastIntegralCutoff and writes those
+   with |(ij|kl)| > maxIntegralCutoff to intFileName (blank-terminated, as Fortran passes it) in
+   QUICK's format: blocks of 150000 records written as int IJ[], int KL[], double value[] (the
+   last block short), IJ = i nbasis + j, KL = k nbasis + l, 0-based, i <= j, k <= l,
+   (i, j) <= (k, l), cons-scaled values.  intNum += the number written.  s, p and d shells only
+   (a basis with f shells is rejected).  Replaces the density screen, so gpu_upload_cutoff_
+   must precede the next two-electron build. */
 void gpu_aoint_(double* leastIntegralCutoff, double* maxIntegralCutoff, int* intNum, char* intFileName);
+/* src/cuda/gpu.cu:1559-1801: o <- symmetric (O as uploaded + J - (h/2) K) from the intindex
+   stored integrals of intFileName and the density of the last gpu_upload_calculated_ (h from
+   gpu_upload_method_), as gpu_get2e_ returns it. */
 void gpu_addint_(double* o, int* intindex, char* intFileName);
 
 /* ---- Part 2: additions ---------------------------------------------- */

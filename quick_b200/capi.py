@@ -148,6 +148,30 @@ class Session:
         check()
         return g
 
+    def aoint(self, path, least_cutoff, max_cutoff):
+        """QUICK's gpu_aoint_: the unique integrals into the file at path;
+        returns how many were written."""
+        r = lib()
+        num = C.c_int(0)
+        name = (path + " ").encode()
+        r.gpu_aoint_(C.byref(C.c_double(least_cutoff)), C.byref(C.c_double(max_cutoff)), C.byref(num),
+                     C.c_char_p(name))
+        check()
+        return num.value
+
+    def addint(self, O, dense, path, nint, method=0):
+        """QUICK's gpu_upload_method_ / gpu_upload_calculated_ + gpu_addint_:
+        O + G(dense) from the stored integrals."""
+        r = lib()
+        o = np.array(O, order="F", dtype=np.float64)
+        co = np.zeros((1,), dtype=np.float64)
+        d = np.asfortranarray(dense, dtype=np.float64)
+        r.gpu_upload_method_(_i(method))
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(co), _ptr(d))
+        r.gpu_addint_(_ptr(o), _i(nint), C.c_char_p((path + " ").encode()))
+        check()
+        return o
+
     def autotune(self):
         """Time every lane-group size of every class on the last Fock build's
         quartet lists and keep the fastest (qb_autotune_classes)."""

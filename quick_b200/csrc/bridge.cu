@@ -134,6 +134,7 @@ struct Context {
 };
 
 unsigned long long g_launches = 0;   // kernels launched by this library
+AoIntOut* g_aoint_out = nullptr;      // descriptor of the current gpu_aoint_ slice (launch tables)
 static long long g_geom_counter = 0; // process-wide, so a cached XC grid never outlives its molecule
 static Context* g = nullptr;
 static int g_status = 0;
@@ -1707,15 +1708,206 @@ int qb_class_info(int* nclasses, int* class_L, long long* class_quartets, int ca
     }
     return 0;
 }
+// ------------------------------------------------- stored-integral path
+// QUICK's conventional SCF (quick_method%nodirect, src/shell.f90:118-209 and
+// src/cuda/gpu.cu:1559-2237): gpu_aoint_ computes every unique integral once
+// and writes it to a file, gpu_addint_ reads the file each iteration and
+// adds J and K for the uploaded density.  The file format is QUICK's: blocks
+// of kEriBlock records, each block written as kEriBlock int IJ, then int KL,
+// then double values (the last block short), IJ = i n + j, KL = k n + l.
+constexpr int kEriBlock = 150000;   // BUFFERSIZE, gpu_common.h:44
+
+// Fortran passes the name blank-padded: up to the first blank, like QUICK's trim()
+static std::string fortran_name(const char* s)
+{
+    std::string r;
+    for (int i = 0; i < 4096 && s[i] && s[i] != ' '; i++) r += s[i];
+    return r;
+}
+
+__global__ void fill_kernel(double* p, size_t n, double v)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// Every distinct index permutation (p q|r s) of a stored integral adds
+// D_rs Y to G_pq and -(h/2) D_qs Y to G_pr (the closed-shell two-electron
+// operator summed over the permutations).
+__global__ void addint_kernel(const EriRecord* __restrict__ rec, long long n, const double* __restrict__ D, int nb,
+                              double hx, double* __restrict__ G)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const EriRecord r = rec[t];
+    const int i = r.IJ / nb, j = r.IJ % nb, k = r.KL / nb, l = r.KL % nb;
+    const double y = r.value;
+    const int P[8][4] = {{i, j, k, l}, {j, i, k, l}, {i, j, l, k}, {j, i, l, k},
+                         {k, l, i, j}, {l, k, i, j}, {k, l, j, i}, {l, k, j, i}};
+    for (int u = 0; u < 8; u++) {
+        bool dup = false;
+        for (int v = 0; v < u; v++)
+            dup = dup || (P[u][0] == P[v][0] && P[u][1] == P[v][1] && P[u][2] == P[v][2] && P[u][3] == P[v][3]);
+        if (dup) continue;
+        const int p = P[u][0], q = P[u][1], rr = P[u][2], s = P[u][3];
+        atomicAdd(G + p + (size_t)q * nb, __ldg(D + rr + (size_t)s * nb) * y);
+        if (hx != 0.0) atomicAdd(G + p + (size_t)rr * nb, -0.5 * hx * __ldg(D + q + (size_t)s * nb) * y);
+    }
+}
+
+// Shell quartets with Y_ij Y_kl > leastIntegralCutoff (QUICK's getAOInt
+// screen: no density), integrals with |Y| > maxIntegralCutoff written;
+// intNum += their number.  The class kernels store instead of digesting;
+// classes are processed in slices that fit a 1 GB device record buffer.
 void gpu_aoint_(double* leastIntegralCutoff, double* maxIntegralCutoff, int* intNum, char* intFileName)
 {
-    (void)leastIntegralCutoff; (void)maxIntegralCutoff; (void)intNum; (void)intFileName;
-    set_error(23, "gpu_aoint_: the conventional stored-integral path is not part of this build");
+    Context& c = ctx();
+    if (require(c.have_pairs, "gpu_upload_cutoff_matrix_ must precede gpu_aoint_")) return;
+    if (c.maxL > 2) {
+        set_error(23, "gpu_aoint_: the stored-integral path covers s, p and d shells (this basis has f)");
+        return;
+    }
+    const std::string fname = fortran_name(intFileName);
+    FILE* f = fopen(fname.c_str(), "wb");
+    if (!f) {
+        set_error(24, "gpu_aoint_: cannot open %s", fname.c_str());
+        return;
+    }
+    const double saved_mixed = c.mixed_cut;
+    c.integralCutoff = *leastIntegralCutoff;
+    c.mixed_cut = 0.0;
+    // a density screen of 1/4 everywhere makes DNMax = 1: the Schwarz test alone
+    const size_t ns = c.nshell;
+    if (c.d_cut_matrix.alloc(ns * ns) != cudaSuccess) { fclose(f); set_error(2, "gpu_aoint_: allocation failed"); return; }
+    fill_kernel<<<(unsigned)((ns * ns + 255) / 256), 256, 0, c.stream>>>(c.d_cut_matrix.p, ns * ns, 0.25);
+    ++g_launches;
+    c.have_cutoff = true;
+    auto fail = [&](const char* what) {
+        fclose(f);
+        c.mixed_cut = saved_mixed;
+        c.have_cutoff = false;
+        set_error(2, "gpu_aoint_: %s", what);
+    };
+    if ((g_sized_cutoff != c.integralCutoff || c.d_quartets.p == nullptr) && size_quartet_lists(c)) return fail("sizing");
+    FockParams P = fock_params(c);
+    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p, c.d_counts32.p};
+    cudaMemsetAsync(c.d_counts.p, 0, kNumClasses * sizeof(unsigned long long), c.stream);
+    cudaMemsetAsync(c.d_counts32.p, 0, kNumClasses * sizeof(unsigned long long), c.stream);
+    cudaMemsetAsync(c.d_overflow.p, 0, sizeof(int), c.stream);
+    launch_screen(S, P, kNumClasses, 0, c.nsm, c.stream);
+    launch_finish_counts(S, c.d_class_count.p, c.d_class_count32.p, c.d_overflow.p, kNumClasses, c.stream);
+    std::vector<int> cnt(kNumClasses);
+    if (cudaMemcpyAsync(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream) !=
+            cudaSuccess || cudaStreamSynchronize(c.stream) != cudaSuccess)
+        return fail("screen failed");
+    const long long cap = 64LL << 20;   // records in the device buffer (1 GB)
+    DevBuf<EriRecord> rec;
+    DevBuf<unsigned long long> dcount;
+    if (rec.alloc(cap) != cudaSuccess || dcount.alloc(1) != cudaSuccess) return fail("allocation failed");
+    std::vector<int> A(kEriBlock), B(kEriBlock);
+    std::vector<double> V(kEriBlock);
+    std::vector<EriRecord> host;
+    int nbuf = 0;
+    long long total = 0;
+    auto flush = [&](int m) {
+        fwrite(A.data(), sizeof(int), m, f);
+        fwrite(B.data(), sizeof(int), m, f);
+        fwrite(V.data(), sizeof(double), m, f);
+    };
+    for (int k = 0; k < kNumClasses; k++) {
+        if (cnt[k] == 0) continue;
+        const int* Lk = kClassL[k];
+        const long long ncomp = (long long)(Lk[0] + 1) * (Lk[0] + 2) / 2 * (Lk[1] + 1) * (Lk[1] + 2) / 2 *
+                                (Lk[2] + 1) * (Lk[2] + 2) / 2 * (Lk[3] + 1) * (Lk[3] + 2) / 2;
+        const long long slice = std::max(1LL, cap / ncomp);
+        for (long long q0 = 0; q0 < cnt[k]; q0 += slice) {
+            AoIntOut O{rec.p, dcount.p, cap, *maxIntegralCutoff, c.d_cons.p, c.nbasis, q0,
+                       std::min<long long>(q0 + slice, cnt[k])};
+            cudaMemsetAsync(dcount.p, 0, sizeof(unsigned long long), c.stream);
+            qb::g_aoint_out = &O;
+            launch_class(k, P, -1, (int)(O.qend - O.qbegin), c.nsm, c.stream);
+            qb::g_aoint_out = nullptr;
+            unsigned long long m = 0;
+            if (cudaMemcpyAsync(&m, dcount.p, sizeof m, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+                cudaStreamSynchronize(c.stream) != cudaSuccess)
+                return fail("kernel failed");
+            if ((long long)m > cap) return fail("record buffer overflow (internal sizing error)");
+            host.resize(m);
+            if (m && cudaMemcpy(host.data(), rec.p, m * sizeof(EriRecord), cudaMemcpyDeviceToHost) != cudaSuccess)
+                return fail("download failed");
+            for (const EriRecord& r : host) {
+                A[nbuf] = r.IJ;
+                B[nbuf] = r.KL;
+                V[nbuf] = r.value;
+                if (++nbuf == kEriBlock) flush(nbuf), nbuf = 0;
+            }
+            total += (long long)m;
+        }
+    }
+    flush(nbuf);
+    fclose(f);
+    c.mixed_cut = saved_mixed;
+    c.have_cutoff = false;   // the density screen was replaced: the next build needs gpu_upload_cutoff_
+    if (total > 2147483647LL) {
+        set_error(25, "gpu_aoint_: %lld integrals exceed QUICK's int counter", total);
+        return;
+    }
+    *intNum += (int)total;
 }
+
+// o <- symmetric (O as uploaded + J - (h/2) K) from the stored integrals of
+// gpu_aoint_ and the density of the last gpu_upload_calculated_.
 void gpu_addint_(double* o, int* intindex, char* intFileName)
 {
-    (void)o; (void)intindex; (void)intFileName;
-    set_error(23, "gpu_addint_: the conventional stored-integral path is not part of this build");
+    Context& c = ctx();
+    if (require(c.have_calc, "gpu_upload_calculated_ must precede gpu_addint_")) return;
+    const std::string fname = fortran_name(intFileName);
+    FILE* f = fopen(fname.c_str(), "rb");
+    if (!f) {
+        set_error(24, "gpu_addint_: cannot open %s", fname.c_str());
+        return;
+    }
+    const int n = c.nbasis;
+    const size_t nn = (size_t)n * n;
+    DevBuf<double> G;
+    DevBuf<EriRecord> rec;
+    if (G.alloc(nn) != cudaSuccess || rec.alloc(kEriBlock) != cudaSuccess || c.d_dense_raw.alloc(nn) != cudaSuccess) {
+        fclose(f);
+        set_error(2, "gpu_addint_: allocation failed");
+        return;
+    }
+    cudaMemsetAsync(G.p, 0, nn * sizeof(double), c.stream);
+    cudaMemcpyAsync(c.d_dense_raw.p, c.dense_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream);
+    const double hx = c.method == 0 ? 1.0 : (c.method == 1 ? 0.2 : 0.0);
+    std::vector<int> A(kEriBlock), B(kEriBlock);
+    std::vector<double> V(kEriBlock);
+    std::vector<EriRecord> host(kEriBlock);
+    long long remaining = *intindex;
+    bool ok = true;
+    while (remaining > 0 && ok) {
+        const int m = (int)std::min<long long>(kEriBlock, remaining);
+        ok = fread(A.data(), sizeof(int), m, f) == (size_t)m && fread(B.data(), sizeof(int), m, f) == (size_t)m &&
+             fread(V.data(), sizeof(double), m, f) == (size_t)m;
+        if (!ok) break;
+        for (int i = 0; i < m; i++) host[i] = EriRecord{A[i], B[i], V[i]};
+        ok = cudaMemcpyAsync(rec.p, host.data(), m * sizeof(EriRecord), cudaMemcpyHostToDevice, c.stream) == cudaSuccess;
+        addint_kernel<<<(m + 255) / 256, 256, 0, c.stream>>>(rec.p, m, c.d_dense_raw.p, n, hx, G.p);
+        ++g_launches;
+        // the host buffers are refilled next: wait for this block's copy
+        ok = ok && cudaStreamSynchronize(c.stream) == cudaSuccess;
+        remaining -= m;
+    }
+    fclose(f);
+    if (!ok) {
+        set_error(24, "gpu_addint_: %s is shorter than %d records", fname.c_str(), *intindex);
+        return;
+    }
+    std::vector<double> g(nn);
+    if (cudaMemcpy(g.data(), G.p, nn * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_error(2, "gpu_addint_: download failed");
+        return;
+    }
+    for (size_t i = 0; i < nn; i++) o[i] = c.o_host[i] + g[i];
 }
 
 }  // extern "C"

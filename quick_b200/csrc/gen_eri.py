@@ -372,6 +372,34 @@ def gen_class(la, lb, lc, ld, prec="double"):
     for ln in dg:
         w(ln)
     w("}")
+    if not f32:
+        # store(): the block's unique integrals for QUICK's stored-integral
+        # path (gpu_aoint_), one lane per quartet, instead of the digestion
+        w("__device__ __forceinline__ static void store(const QuartetCtx& q, const FockParams& P, const AoIntOut& O)")
+        w("{")
+        w("    constexpr int L = %d;" % L)
+        for e, f, _ in targets:
+            w("    double c_%s_%s = 0.0;" % (nm(e), nm(f)))
+        w("    for (int ib = 0; ib < q.nbra; ib++) {")
+        for ln in bra_load:
+            w("        " + ln)
+        w("        for (int ik = 0; ik < q.nket; ik++) {")
+        for ln in body:
+            w("            " + ln)
+        w("        }")
+        w("    }")
+        w("    if (!q.active) return;")
+        w("    const double ABx = q.ABx, ABy = q.ABy, ABz = q.ABz, CDx = q.CDx, CDy = q.CDy, CDz = q.CDz;")
+        w("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
+        for ln in hrr.lines:
+            w("    " + ln)
+        w("    const int a0 = q.bfA, b0 = q.bfB, c0 = q.bfC, d0 = q.bfD;")
+        for ia in range(na):
+            for ib in range(nb):
+                for ic in range(nc):
+                    for id_ in range(nd):
+                        w("    aoint_emit(O, q, a0+%d, b0+%d, c0+%d, d0+%d, %s);" % (ia, ib, ic, id_, vals[(ia, ib, ic, id_)]))
+        w("}")
     w("};")
     gs = group_sizes(la, lb, lc, ld)
     kname = "fock_class_kernel32" if f32 else "fock_class_kernel"
@@ -379,6 +407,9 @@ def gen_class(la, lb, lc, ld, prec="double"):
     w("int launch_%s%s(const FockParams& P, int cls, int G, int nq, int nsm, cudaStream_t st)" % (tag, "_f32" if f32 else ""))
     w("{")
     w("    switch (G) {")
+    if not f32:
+        w("    case -1: { auto kern = aoint_class_kernel<%d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, 0, st, P, cls, *g_aoint_out); return -1; }"
+          % (la, lb, lc, ld))
     for g in gs:
         w("    case %d: { auto kern = %s<%d, %d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, %d, nsm), 128, 0, st, P, cls); return %d; }"
           % (g, kname, la, lb, lc, ld, g, g, g))
