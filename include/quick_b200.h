@@ -165,6 +165,14 @@ int qb_last_fock_split(long long* quartets_fp64, long long* quartets_fp32);
    density and of the alpha density.  sigrad2 is a host array (nbasis), as for gpu_getxc_. */
 int qb_xc_device(const double* d_dense, const double* sigrad2, double* d_vxc, double* exc, double* nalpha);
 
+/* Reproducible Fock builds (no counterpart as a switch in QUICK, whose GPU build always
+   accumulates this way, gpu_common.h:115): on = 1 rounds every Coulomb and exchange
+   contribution to a 64-bit fixed-point number of 1e-16 units and adds it with integer atomics,
+   so the Fock matrix is bit-identical whatever the order the quartets run in (lane groups,
+   streams, the screen's list order); on = 0 (default) adds doubles.  Applies to gpu_get2e_,
+   qb_fock_device, qb_fock_device_static and the batched build; gradients stay FP64. */
+int qb_set_fixed_point(int on);
+
 /* Grid of the following qb_xc_device / qb_xc_grad_device calls: 1 = SG1 (default), 2 = the
    75 x 302 Becke grid (gpu_getxc_'s isg = 2).  No counterpart in QUICK. */
 int qb_set_xc_grid(int grid);

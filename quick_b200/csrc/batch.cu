@@ -139,7 +139,7 @@ __global__ void batch_zero_kernel(const MolInfo* __restrict__ mol, double* __res
 // O_out,i(a, b) = O_in,i(a, b) + cons cons G(max, min), packed
 __global__ void batch_finish_kernel(const MolInfo* __restrict__ mol, const double* __restrict__ G,
                                     const double* __restrict__ cons, const double* __restrict__ Oin,
-                                    double* __restrict__ Oout, int ntot)
+                                    double* __restrict__ Oout, int ntot, int fixed)
 {
     const MolInfo m = mol[blockIdx.y];
     const long long nn = (long long)m.n * m.n;
@@ -147,7 +147,9 @@ __global__ void batch_finish_kernel(const MolInfo* __restrict__ mol, const doubl
         const int a = (int)(e % m.n), b = (int)(e / m.n);
         const int ga = m.f0 + a, gb = m.f0 + b;
         const int hi = ga > gb ? ga : gb, lo = ga > gb ? gb : ga;
-        Oout[m.pk + e] = Oin[m.pk + e] + cons[ga] * cons[gb] * G[(size_t)hi * ntot + lo];
+        const size_t x = (size_t)hi * ntot + lo;
+        const double g = fixed ? (double)reinterpret_cast<const long long*>(G)[x] / kFixedScale : G[x];
+        Oout[m.pk + e] = Oin[m.pk + e] + cons[ga] * cons[gb] * g;
     }
 }
 
@@ -405,7 +407,8 @@ extern "C" int qb_batch_fock_device(const double* d_dense, const double* d_o_in,
             if (rc < 0) return report_error(5, "qb_batch_fock_device: a class needs more shared memory than the GPU offers");
         }
     }
-    batch_finish_kernel<<<block_grid(B), 256, 0, s.st>>>(B.dmol.p, B.fock.p, B.cons.p, d_o_in, d_o_out, B.ntot);
+    batch_finish_kernel<<<block_grid(B), 256, 0, s.st>>>(B.dmol.p, B.fock.p, B.cons.p, d_o_in, d_o_out, B.ntot,
+                                                          P.fixed_point);
     ++g_launches;
     BCK(cudaGetLastError());
     return 0;

@@ -122,6 +122,7 @@ struct Context {
     bool stats_pending = false;          // the last Fock build's counts are still on the device
     double mixed_cut = 0.0;      // Fock builds: quartets with Y Y DNMax below this run in FP32 (0: all FP64)
     int xc_grid = 1;             // grid of qb_xc_device: 1 SG1, 2 the 75 x 302 Becke grid
+    int fixed_point = 0;         // Fock builds accumulate 64-bit fixed point (qb_set_fixed_point)
     double last_ms_xc_grad = 0.0;
     XcResult last_xc;
     double last_ms_eri = 0, last_ms_screen = 0;
@@ -550,6 +551,7 @@ static FockParams fock_params(Context& c)
     P.prim32 = c.d_prim32.p;
     P.pair_A = c.d_pair_A.p;
     P.boys32 = c.d_boys32.p;
+    P.fixed_point = c.fixed_point;
     return P;
 }
 
@@ -758,7 +760,7 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
     if (int rc = join_side_streams(c)) return rc;
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[3], c.stream));
-    launch_fock_finish(c.d_fock.p, c.d_cons.p, d_o_in, d_o_out, n, c.stream);
+    launch_fock_finish(c.d_fock.p, c.d_cons.p, d_o_in, d_o_out, n, c.stream, c.fixed_point);
     CK(cudaGetLastError());
     c.stats_pending = true;
     return 0;
@@ -1238,6 +1240,13 @@ int qb_xc_grad_device(const double* d_dense, const double* sigrad2, double* d_gr
     double ms = 0.0;
     if (int rc = xc_gradient(in, d_dense, d_grad, &ms)) return rc;
     c.last_ms_xc_grad = ms;
+    return 0;
+}
+
+int qb_set_fixed_point(int on)
+{
+    Context& c = ctx();
+    c.fixed_point = on ? 1 : 0;
     return 0;
 }
 

@@ -452,7 +452,7 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         else if (t < o_bc) r = a0 + (t - o_ad) / nd, c = d0 + (t - o_ad) % nd, wgt = wk;
         else if (t < o_bd) r = b0 + (t - o_bc) / nc, c = c0 + (t - o_bc) % nc, wgt = wk;
         else r = b0 + (t - o_bd) / nd, c = d0 + (t - o_bd) % nd, wgt = wk;
-        fock_add(P.fock, n, r, c, wgt * Jb[t]);
+        fock_add(P.fock, n, r, c, wgt * Jb[t], P.fixed_point);
     }
     __syncthreads();
 }

@@ -183,7 +183,7 @@ extern "C" int qb_fock_device_static(const double* d_dense, const double* d_o_in
                         L[3], rc);
     }
     CKS(cudaGetLastError());
-    launch_fock_finish(fock, v.cons, d_o_in, d_o_out, n, st);
+    launch_fock_finish(fock, v.cons, d_o_in, d_o_out, n, st, v.P.fixed_point);
     CKS(cudaGetLastError());
     CKS(cudaStreamSynchronize(st));
     return 0;

@@ -63,7 +63,8 @@ void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int cou
 void launch_finish_counts(const ScreenParams& S, int* class_count, int* class_count32, int* overflow, int ncls,
                           cudaStream_t st);
 void launch_scale_density(const double* D, const double* cons, double* Ds, int n, cudaStream_t st);
-void launch_fock_finish(const double* G, const double* cons, const double* Oin, double* Oout, int n, cudaStream_t st);
+void launch_fock_finish(const double* G, const double* cons, const double* Oin, double* Oout, int n, cudaStream_t st,
+                        int fixed = 0);
 // cut (nshell x nshell) = max |D| per shell-pair block; shell_first has nshell + 1 entries (0-based)
 void launch_density_screen(const double* D, const int* shell_first, int nshell, int n, double* cut, cudaStream_t st);
 void launch_add_vector(const double* x, double* y, int n, cudaStream_t st);

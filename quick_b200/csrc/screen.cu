@@ -136,15 +136,18 @@ __global__ void scale_density_kernel(const double* __restrict__ D, const double*
     }
 }
 
-// O_out(i,j) = O_in(i,j) + cons(i) cons(j) G(max(i,j), min(i,j)), column-major, symmetric.
+// O_out(i,j) = O_in(i,j) + cons(i) cons(j) G(max(i,j), min(i,j)), column-major, symmetric;
+// fixed: G holds 64-bit fixed point.
 __global__ void fock_finish_kernel(const double* __restrict__ G, const double* __restrict__ cons,
-                                   const double* __restrict__ Oin, double* __restrict__ Oout, int n)
+                                   const double* __restrict__ Oin, double* __restrict__ Oout, int n, int fixed)
 {
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < (size_t)n * n) {
         const int i = (int)(idx % n), j = (int)(idx / n);
         const int hi = i > j ? i : j, lo = i > j ? j : i;
-        Oout[idx] = Oin[idx] + cons[i] * cons[j] * G[(size_t)hi * n + lo];
+        const size_t e = (size_t)hi * n + lo;
+        const double g = fixed ? (double)reinterpret_cast<const long long*>(G)[e] / kFixedScale : G[e];
+        Oout[idx] = Oin[idx] + cons[i] * cons[j] * g;
     }
 }
 
@@ -167,10 +170,11 @@ void launch_scale_density(const double* D, const double* cons, double* Ds, int n
     QB_LAUNCH(scale_density_kernel, (unsigned)((N + 255) / 256), 256, 0, st, D, cons, Ds, n);
 }
 
-void launch_fock_finish(const double* G, const double* cons, const double* Oin, double* Oout, int n, cudaStream_t st)
+void launch_fock_finish(const double* G, const double* cons, const double* Oin, double* Oout, int n, cudaStream_t st,
+                        int fixed)
 {
     const size_t N = (size_t)n * n;
-    QB_LAUNCH(fock_finish_kernel, (unsigned)((N + 255) / 256), 256, 0, st, G, cons, Oin, Oout, n);
+    QB_LAUNCH(fock_finish_kernel, (unsigned)((N + 255) / 256), 256, 0, st, G, cons, Oin, Oout, n, fixed);
 }
 
 // QUICK's density screen (densityCutoff / DNscreen, src/schwarz.f90:550-600)

@@ -99,3 +99,34 @@ def test_autotuned_lane_groups_keep_the_fock_matrix():
         s.close()
     assert np.abs(F1 - F0).max() < 1e-10
     assert set(int(x) for x in g if x) <= {1, 2, 4, 8, 16, 32}
+
+
+def test_fixed_point_fock_is_bit_reproducible(oracle_lib):
+    """qb_set_fixed_point(1): the Fock matrix is bit-identical over repeated
+    builds (the screen lists the quartets in a different order each time and
+    the atomics land in a different order), within 1e-12 of the FP64 build,
+    and within 1e-13 after the lane groups change (a quartet's primitive sum
+    then runs in another order); the FP64 build matches the oracle to 1e-8."""
+    from quick_b200 import capi
+    m, b = case("water4_631gs")
+    n = b.nbasis
+    Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
+    s = capi.Session(0)
+    try:
+        s.upload_molecule(m, b, Y, cp)
+        D = random_density(n, seed=21)
+        cm = oracle_lib.cutmatrix(b, D)
+        f64 = s.get2e(np.zeros((n, n), order="F"), D, cm, 1e-10, 1e-20)
+        capi.lib().qb_set_fixed_point(1)
+        runs = [s.get2e(np.zeros((n, n), order="F"), D, cm, 1e-10, 1e-20) for _ in range(3)]
+        s.autotune()
+        runs.append(s.get2e(np.zeros((n, n), order="F"), D, cm, 1e-10, 1e-20))
+    finally:
+        capi.lib().qb_set_fixed_point(0)
+        s.close()
+    for r in runs[1:3]:
+        assert np.array_equal(r, runs[0])
+    assert np.abs(runs[3] - runs[0]).max() < 1e-13
+    assert np.abs(runs[0] - f64).max() < 1e-12
+    ref, _ = oracle_lib.fock(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
+    assert np.abs(f64 - ref).max() < 1e-8
