@@ -241,7 +241,7 @@ def run_ours(args, ws, rank, local):
     torch.cuda.synchronize()
     # lanes per quartet of each class autotuned on this build's quartet lists
     # (qb_autotune_classes), then warmed up again
-    sess.autotune()
+    groups64 = sess.autotune()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -331,7 +331,7 @@ def run_ours(args, ws, rank, local):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    sess.autotune()          # lanes per quartet of the FP32 class kernels, on this build's FP32 lists
+    groups32 = sess.autotune()   # lanes per quartet of the FP32 class kernels, on this build's FP32 lists
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -408,7 +408,11 @@ def run_ours(args, ws, rank, local):
         "dtype": "f64",
         "data": "synthetic: seeded (H2O)32 geometry, model density",
         "config": workload_config(n, quartets),
-        "lane_groups": "autotuned per class (qb_autotune_classes)",
+        "lane_groups": {"note": "lanes per quartet, autotuned per class (qb_autotune_classes)",
+                        "fp64": {"%d%d%d%d" % tuple(cl[4 * i:4 * i + 4]): int(groups64[i])
+                                 for i in range(k) if cq[i] > 0 and sum(cl[4 * i:4 * i + 4]) < 6},
+                        "fp32": {"%d%d%d%d" % tuple(cl[4 * i:4 * i + 4]): int(groups32[i])
+                                 for i in range(k) if cq[i] > 0 and sum(cl[4 * i:4 * i + 4]) < 6}},
         "parity_vs_quick": parity,
         "e2e": {"value": quartets * ws / (e2e_ms * 1e-3), "unit": "quartets/s",
                 "h2d_bytes_per_step": int(2 * n * n * 8 + b.nshell ** 2 * 8),
