@@ -479,9 +479,11 @@ def run_scf(args, ws, rank, local):
                                       **kw)
             secs.append(r.seconds)
             runs.append((r, g))
+        phases_each = [{k: round(v, 3) for k, v in rr.timings.items() if k in ("setup", "scf", "gradient")}
+                       for rr, _ in runs]
         r, g = runs[-1]
         res[tag] = dict(seconds_per_molecule=max_over_ranks(float(np.median(secs)), ws),
-                        seconds_each=[round(x, 4) for x in secs],
+                        seconds_each=[round(x, 4) for x in secs], phases_each=phases_each,
                         molecules_per_s=ws / max_over_ranks(float(np.median(secs)), ws),
                         energy=r.energy, iterations=r.iterations, converged=bool(r.converged),
                         fock_builds=r.fock_builds,
