@@ -40,6 +40,28 @@ def _extra_flags(src):
     return []
 
 
+# f classes with straight-line kernels: total angular momentum up to this
+# (gen_eri.py, F_MAX_L)
+F_MAX_L = 8
+
+
+def _generated_class(src):
+    """A generated straight-line class file (Fock, FP32 Fock, gradient)."""
+    b = os.path.basename(src)
+    return any(b.startswith(pre) and b[len(pre):len(pre) + 4].isdigit()
+               for pre in ("eri_", "eri32_", "grad_", "grad32_"))
+
+
+def _flags(src):
+    """nvcc flags of one source.  The generated class files are built
+    without -lineinfo: their line tables (a line per recurrence term) double
+    their objects, and the library with them would pass 400 MB.  Every
+    hand-written source keeps -lineinfo."""
+    if _generated_class(src):
+        return [f for f in FLAGS if f != "-lineinfo"]
+    return FLAGS
+
+
 _INC = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
 
 
@@ -81,13 +103,11 @@ def build(lmax=2, jobs=None, verbose=False):
     keep = []
     for s in srcs:
         b = os.path.basename(s)
-        for pre in ("eri_", "eri32_", "grad_"):
+        for pre in ("eri_", "eri32_", "grad_", "grad32_"):
             if b.startswith(pre) and b[len(pre):len(pre) + 4].isdigit():
                 ls = [int(ch) for ch in b[len(pre):len(pre) + 4]]
-                # Fock classes: up to lmax, plus the f classes with L sum <= 6;
-                # gradient classes: up to lmax, plus the f classes with L sum
-                # <= 6 (gen_eri.py)
-                if max(ls) > lmax and sum(ls) > 6:
+                # classes up to lmax, plus the f classes with L sum <= F_MAX_L
+                if max(ls) > lmax and sum(ls) > F_MAX_L:
                     break
         else:
             keep.append(s)
@@ -102,7 +122,7 @@ def build(lmax=2, jobs=None, verbose=False):
 
     def cc(so):
         s, o = so
-        cmd = [NVCC] + ARCH + FLAGS + _extra_flags(s) + ["-c", s, "-o", o]
+        cmd = [NVCC] + ARCH + _flags(s) + _extra_flags(s) + ["-c", s, "-o", o]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("nvcc failed on %s:\n%s" % (s, r.stderr[-4000:]))

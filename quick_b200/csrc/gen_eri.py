@@ -172,7 +172,12 @@ class HRR:
 # gradient classes with total angular momentum >= this get one kernel per
 # derivative centre (two accumulator sets each instead of four)
 GRAD_SPLIT_L = int(os.environ.get("QB_GRAD_SPLIT_L", "4"))
-GRAD_F_MAX_L = 6
+# f classes with straight-line kernels: total angular momentum up to
+# F_MAX_L for the Fock build and the gradient (the larger ones run the
+# generic kernels of eri_generic.cu), FP32 variants up to F32_MAX_L (the
+# FP32 lists of the classes between run their FP64 kernels)
+F_MAX_L = 8
+F32_MAX_L = 6
 
 
 def grad_group_sizes(la, lb, lc, ld):
@@ -194,7 +199,7 @@ def group_sizes(la, lb, lc, ld):
     return [1]
 
 
-def gen_class(la, lb, lc, ld, prec="double"):
+def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
     """One angular class of the Fock build.  prec = "float": the FP32 variant
     of the mixed-precision split (vertical and horizontal recurrences,
     contraction and Boys function in FP32 from FP64 pair data and geometry;
@@ -411,12 +416,21 @@ def gen_class(la, lb, lc, ld, prec="double"):
         w("    case -1: { auto kern = aoint_class_kernel<%d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, 0, st, P, cls, *g_aoint_out); return -1; }"
           % (la, lb, lc, ld))
     for g in gs:
-        w("    case %d: { auto kern = %s<%d, %d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, %d, nsm), 128, 0, st, P, cls); return %d; }"
-          % (g, kname, la, lb, lc, ld, g, g, g))
-    w("    default: { auto kern = %s<%d, %d, %d, %d, 1>; QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, 0, st, P, cls); return 1; }"
-      % (kname, la, lb, lc, ld))
+        w("    case %d: { auto kern = %s<%d, %d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, %d, nsm), 128, 0, st, P, cls%s); return %d; }"
+          % (g, kname, la, lb, lc, ld, g, g, "" if f32 else ", 0", g))
+    w("    default: { auto kern = %s<%d, %d, %d, %d, 1>; QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, 0, st, P, cls%s); return 1; }"
+      % (kname, la, lb, lc, ld, "" if f32 else ", 0"))
     w("    }")
     w("}")
+    if list32_launcher:
+        # no FP32 kernel for this class: its FP32 list runs in FP64
+        w("int launch_%s_f32(const FockParams& P, int cls, int G, int nq, int nsm, cudaStream_t st)" % tag)
+        w("{")
+        w("    (void)G;")
+        w("    auto kern = fock_class_kernel<%d, %d, %d, %d, 1>;" % (la, lb, lc, ld))
+        w("    QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, 0, st, P, cls, 1);")
+        w("    return 1;")
+        w("}")
     w("}  // namespace qb")
     stats = dict(vrr_flops=vrr.nflops, vrr_nodes=len(vrr.lines), hrr_flops=hrr.nflops, targets=len(targets),
                  ncomp=na * nb * nc * nd)
@@ -753,13 +767,13 @@ def main(outdir, lmax=2, lmax_all=3):
     os.makedirs(outdir, exist_ok=True)
     cls_all = classes(lmax_all)
     # straight-line kernels: every class up to lmax, and the f classes whose
-    # total angular momentum is at most 6 (the larger ones run the generic
-    # kernel; their straight-line code would take hours to compile)
-    cls = [c for c in cls_all if max(c) <= lmax or sum(c) <= 6]
-    # gradient: every class up to lmax, and the f classes with total angular
-    # momentum <= GRAD_F_MAX_L (the larger ones run the generic gradient
+    # total angular momentum is at most F_MAX_L (the larger ones run the
+    # generic kernel; their straight-line code spills most of its values)
+    cls = [c for c in cls_all if max(c) <= lmax or sum(c) <= F_MAX_L]
+    cls32 = set(c for c in cls if max(c) <= lmax or sum(c) <= F32_MAX_L)
+    # gradient: the same classes (the larger ones run the generic gradient
     # kernel, eri_generic.cu, which is slow for the many small quartets)
-    cls_grad = [c for c in cls_all if max(c) <= lmax or sum(c) <= GRAD_F_MAX_L]
+    cls_grad = list(cls)
     lines = ["// generated by gen_eri.py", "#pragma once", "namespace qb {",
              "static const int kNumClasses = %d;" % len(cls_all),
              "static const int kClassL[%d][4] = {%s};" % (len(cls_all), ", ".join("{%d,%d,%d,%d}" % c for c in cls_all)),
@@ -774,11 +788,14 @@ def main(outdir, lmax=2, lmax_all=3):
         fh.write("\n".join(lines) + "\n")
     stats = {}
     for c in cls:
-        src, st = gen_class(*c)
+        src, st = gen_class(*c, list32_launcher=c not in cls32)
         stats[c] = st
         write_if_changed(os.path.join(outdir, "eri_%d%d%d%d.cu" % c), src)
-        src32, _ = gen_class(*c, prec="float")
-        write_if_changed(os.path.join(outdir, "eri32_%d%d%d%d.cu" % c), src32)
+        if c in cls32:
+            src32, _ = gen_class(*c, prec="float")
+            write_if_changed(os.path.join(outdir, "eri32_%d%d%d%d.cu" % c), src32)
+        elif os.path.exists(os.path.join(outdir, "eri32_%d%d%d%d.cu" % c)):
+            os.remove(os.path.join(outdir, "eri32_%d%d%d%d.cu" % c))
     # launch table
     lt = ['#include "eri_common.cuh"', '#include "eri_classes.h"', "namespace qb {"]
     for c in cls:
@@ -829,10 +846,11 @@ def main(outdir, lmax=2, lmax_all=3):
             tg = "%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1])
             gstats[tg] = st_
             write_if_changed(os.path.join(outdir, "grad_%s.cu" % tg), src)
-            src32, _ = gen_grad_class(*c, part=pt, prec="float")
-            write_if_changed(os.path.join(outdir, "grad32_%s.cu" % tg), src32)
             gl.append("int launch_grad_%s(const FockParams& P, const GradExtra& G, int cls, int GS, int nq, int nsm, cudaStream_t st);" % tg)
-            gl.append("int launch_grad32_%s(const FockParams& P, const GradExtra& G, int cls, int GS, int nq, int nsm, cudaStream_t st);" % tg)
+            if c in cls32:
+                src32, _ = gen_grad_class(*c, part=pt, prec="float")
+                write_if_changed(os.path.join(outdir, "grad32_%s.cu" % tg), src32)
+                gl.append("int launch_grad32_%s(const FockParams& P, const GradExtra& G, int cls, int GS, int nq, int nsm, cudaStream_t st);" % tg)
     gl += ["// returns 0, or -1 for a class without a gradient kernel (f shells)",
            "int launch_grad_class(int cls, const FockParams& P, const GradExtra& G, int GS, int nq, int nsm, cudaStream_t st)",
            "{", "    switch (cls) {"]
@@ -849,8 +867,13 @@ def main(outdir, lmax=2, lmax_all=3):
     for k, c in enumerate(cls_all):
         if c not in parts:
             continue
-        calls = " ".join("launch_grad32_%s(P, G, %d, GS, nq, nsm, st);" % ("%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1]), k)
-                         for pt in parts[c])
+        if c in cls32:
+            calls = " ".join("launch_grad32_%s(P, G, %d, GS, nq, nsm, st);" % ("%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1]), k)
+                             for pt in parts[c])
+        else:   # no FP32 kernel: the FP64 one on the FP32 list
+            calls = "{ GradExtra G32 = G; G32.list32 = 1; %s }" % " ".join(
+                "launch_grad_%s(P, G32, %d, GS, nq, nsm, st);" % ("%d%d%d%d" % c + ("" if pt == 0 else "_" + "abc"[pt - 1]), k)
+                for pt in parts[c])
         gl.append("    case %d: %s return 0;" % (k, calls))
     gl += ["    default: return -1;", "    }", "}"]
     gl += ["int grad_max_group(int cls)", "{", "    switch (cls) {"]
@@ -860,11 +883,14 @@ def main(outdir, lmax=2, lmax_all=3):
     gl += ["    default: return 1;", "    }", "}", "}  // namespace qb"]
     write_if_changed(os.path.join(outdir, "grad_launch.cu"), "\n".join(gl) + "\n")
     write_if_changed(os.path.join(outdir, "grad_flops.json"), json.dumps(gstats, indent=1))
-    # per-centre files left over from a build with another split threshold
+    # per-centre files left over from a build with another split threshold,
+    # and FP32 files of classes that have no FP32 kernel now
     for f in os.listdir(outdir):
         for pre in ("grad_", "grad32_"):
-            if f.startswith(pre) and f.endswith(".cu") and f != "grad_launch.cu" and f[len(pre):-3] not in gstats:
-                os.remove(os.path.join(outdir, f))
+            if f.startswith(pre) and f.endswith(".cu") and f != "grad_launch.cu":
+                tg = f[len(pre):-3]
+                if tg not in gstats or (pre == "grad32_" and tuple(int(ch) for ch in tg[:4]) not in cls32):
+                    os.remove(os.path.join(outdir, f))
     # Schwarz kernels, one per pair type
     st = ['#include "eri_common.cuh"', '#include "schwarz.cuh"', '#include "eri_classes.h"', "namespace qb {"]
     for t in pair_types(lmax):

@@ -1,7 +1,9 @@
-"""f shells (cc-pVTZ: d on H, f on O): every class with an f shell runs the
-generic block-per-quartet kernels (eri_generic.cu).  Fock matrices and the
-two-electron gradient against the oracle (itself pinned to QUICK's CUDA_SPDF
-kernels where those are right and to finite differences,
+"""f shells (cc-pVTZ: d on H, f on O): the f classes with total angular
+momentum up to 8 run generated straight-line kernels (FP64 only above 6:
+their FP32 lists of the mixed split run the FP64 kernels), the larger ones
+the generic block-per-quartet kernels (eri_generic.cu).  Fock matrices and
+the two-electron gradient against the oracle (itself pinned to QUICK's
+CUDA_SPDF kernels where those are right and to finite differences,
 tests/test_oracle_fshell.py) at 1e-8; Schwarz bounds for f pair types on the
 GPU."""
 import numpy as np
@@ -78,9 +80,9 @@ def test_fshell_schwarz_bounds_on_gpu(session, oracle_lib):
 
 @pytest.mark.parametrize("grid", [(1, 1, 1), (2, 1, 1)])
 def test_fshell_gradient_matches_oracle(session, oracle_lib, grid):
-    """The generic f-class gradient kernel (with the straight-line s/p/d
-    gradient classes) against the oracle's two-electron gradient: 1e-8
-    Eh/bohr absolute on gradients of order 1e2."""
+    """The f-class gradient kernels (straight-line up to total angular
+    momentum 8, generic above) with the s/p/d classes against the oracle's
+    two-electron gradient: 1e-8 Eh/bohr absolute on gradients of order 1e2."""
     m, b = _mol(grid)
     Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
     session.upload_molecule(m, b, Y, cp)
@@ -90,3 +92,24 @@ def test_fshell_gradient_matches_oracle(session, oracle_lib, grid):
     got = session.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
     ref = oracle_lib.grad2e(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
     assert np.abs(got - ref).max() < TOL
+
+
+def test_fshell_mixed_gradient(session, oracle_lib):
+    """The mixed split on the gradient with f shells: FP32 kernels for the
+    classes up to total angular momentum 6, the FP64 kernels on the FP32
+    lists of the f classes of 7 and 8, the generic kernel above; against the
+    oracle's FP64 gradient at 1e-6 Eh/bohr (the FP32 quartets' bound is 1e-3
+    Eh per quartet before the density)."""
+    m, b = _mol((2, 1, 1))
+    Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
+    session.upload_molecule(m, b, Y, cp)
+    D = random_density(b.nbasis, seed=5, scale=0.05)
+    cm = oracle_lib.cutmatrix(b, D)
+    ref = oracle_lib.grad2e(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
+    try:
+        session.set_mixed_precision(1e-3)
+        session.get2e(np.zeros((b.nbasis, b.nbasis), order="F"), D, cm, 1e-10, 1e-20, method=0)
+        got = session.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
+    finally:
+        session.set_mixed_precision(0.0)
+    assert np.abs(got - ref).max() < 1e-6
