@@ -479,8 +479,8 @@ def run_scf(args, ws, rank, local):
                                       **kw)
             secs.append(r.seconds)
             runs.append((r, g))
-        phases_each = [{k: round(v, 3) for k, v in rr.timings.items() if k in ("setup", "scf", "gradient")}
-                       for rr, _ in runs]
+        phases_each = [dict({k: round(v, 3) for k, v in rr.timings.items() if k in ("setup", "scf", "gradient")},
+                            slowest_iteration=round(max(h[2] for h in rr.history), 4)) for rr, _ in runs]
         r, g = runs[-1]
         res[tag] = dict(seconds_per_molecule=max_over_ranks(float(np.median(secs)), ws),
                         seconds_each=[round(x, 4) for x in secs], phases_each=phases_each,

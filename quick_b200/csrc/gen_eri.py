@@ -565,31 +565,45 @@ def gen_grad_class(la, lb, lc, ld, part=0, prec="double"):
     for k, lst in acc.items():
         for e, f, _ in lst:
             w("    %s %s_%s_%s = 0.0%s;" % (R, k, nm(e), nm(f), sfx))
-    # GS lanes per quartet stride over the flattened primitive quartets
-    w("    const int nk = q.nket, npq = q.nbra * nk;")
-    w("    for (int t = (GS == 1 ? 0 : sub); t < npq; t += GS) {")
-    w("        const int ib = t / nk, ik = t - ib * nk;")
     if f32:
-        w("        const PrimRec32 pb = load_prim32(P.prim32, q.bra_off + ib);")
-        w("        const float a2 = 2.0f * pb.alpha;")
-        w("        const float b2 = 2.0f * pb.p - a2;")
-        w("        {")
-        w("            const PrimRec32 pk = load_prim32(P.prim32, q.ket_off + ik);")
-        w("            if (!prim_survives(q, pb.cp, pk.cp, P.prim_limit)) continue;")
-        w("            const float c2 = 2.0f * pk.alpha;")
+        bra = ["const PrimRec32 pb = load_prim32(P.prim32, q.bra_off + ib);",
+               "const float a2 = 2.0f * pb.alpha;",
+               "const float b2 = 2.0f * pb.p - a2;"]
+        ket = ["const PrimRec32 pk = load_prim32(P.prim32, q.ket_off + ik);",
+               "if (!prim_survives(q, pb.cp, pk.cp, P.prim_limit)) continue;",
+               "const float c2 = 2.0f * pk.alpha;"]
     else:
-        w("        const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);")
-        w("        const PrimPair pb = load_prim(P, q.bra_off + ib, xb);")
-        w("        const double a2 = 2.0 * xb.y;")
-        w("        const double b2 = 2.0 * pb.p - a2;")
-        w("        {")
-        w("            const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
-        w("            const PrimPair pk = load_prim(P, q.ket_off + ik, xk);")
-        w("            if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
-        w("            const double c2 = 2.0 * xk.y;")
-    for ln in inner:
+        bra = ["const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);",
+               "const PrimPair pb = load_prim(P, q.bra_off + ib, xb);",
+               "const double a2 = 2.0 * xb.y;",
+               "const double b2 = 2.0 * pb.p - a2;"]
+        ket = ["const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);",
+               "const PrimPair pk = load_prim(P, q.ket_off + ik, xk);",
+               "if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;",
+               "const double c2 = 2.0 * xk.y;"]
+    # one lane per quartet: the bra x ket primitive double loop (each bra
+    # record read once); GS lanes: they stride over the flattened primitive
+    # quartets
+    w("    if constexpr (GS == 1) {")
+    w("    for (int ib = 0; ib < q.nbra; ib++) {")
+    for ln in bra:
+        w("        " + ln)
+    w("        for (int ik = 0; ik < q.nket; ik++) {")
+    for ln in ket + inner:
         w("            " + ln)
     w("        }")
+    w("    }")
+    w("    } else {")
+    w("    const int nk = q.nket, npq = q.nbra * nk;")
+    w("    for (int t = sub; t < npq; t += GS) {")
+    w("        const int ib = t / nk, ik = t - ib * nk;")
+    for ln in bra:
+        w("        " + ln)
+    w("        {")
+    for ln in ket + inner:
+        w("            " + ln)
+    w("        }")
+    w("    }")
     w("    }")
     w("    if constexpr (GS > 1) {")
     for k, lst in acc.items():
