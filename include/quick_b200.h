@@ -208,13 +208,27 @@ int qb_xc_functional(int method, int n, const double* rho, const double* sigma, 
 
 /* No counterpart in QUICK.  Autotunes the lanes per shell quartet of each straight-line Fock
    class: after a Fock build (gpu_get2e_ or qb_fock_device) or a gradient, times every compiled
-   lane-group size of every class on that call's quartet lists (into a scratch matrix; the Fock
-   matrix is untouched) and keeps the fastest for the following builds.  After an all-FP64 call
+   variant of every class on that call's quartet lists (into a scratch matrix; the Fock matrix
+   is untouched) and keeps the fastest for the following builds.  A variant is a lane-group
+   size (1, 2, 4, ... lanes per quartet), or 256 + lanes for the FP64 kernels of the classes
+   with total angular momentum <= 2 that first stage the Boys-function records in shared
+   memory.  After an all-FP64 call
    it tunes the FP64 class kernels, after a call with the mixed split (qb_set_mixed_precision)
    the FP32 ones on the FP32 lists.  The choice stays for the rest of the session, later
-   molecules included (gpu_shutdown_ forgets it).  Writes the chosen sizes, one per class, to
+   molecules included (gpu_shutdown_ forgets it).  Writes the chosen variants, one per class, to
    groups (cap entries at most).  Synchronises the library stream. */
 int qb_autotune_classes(int* groups, int cap);
+
+/* No counterpart in QUICK.  Sets the variant of every straight-line class (n = the number of
+   classes, one code each, as qb_autotune_classes writes them) for the FP64 kernels (fp32 = 0)
+   or the FP32 kernels of the mixed split (fp32 = 1), as if tuned: a saved choice reused, or a
+   test that runs one variant.  After gpu_upload_basis_; a code that is not a variant of its
+   class is an error (status 1) and changes nothing. */
+int qb_set_class_groups(const int* groups, int n, int fp32);
+
+/* No counterpart in QUICK.  The variants of class cls (0 .. the class count of qb_class_info
+   - 1) for the FP64 or the FP32 kernels: writes up to cap codes, returns how many there are. */
+int qb_class_variants(int cls, int fp32, int* codes, int cap);
 
 /* Device form of gpu_upload_cutoff_: the integral and primitive cutoffs, and QUICK's density
    screen cutMatrix(I, J) = max |D| over the shell-pair block (densityCutoff / DNscreen,

@@ -180,6 +180,19 @@ class Session:
         check()
         return g
 
+    def set_class_groups(self, groups, fp32=False):
+        """Set every class's launch variant (qb_set_class_groups)."""
+        g = np.ascontiguousarray(groups, dtype=np.int32)
+        lib().qb_set_class_groups(_ptr(g), C.c_int(len(g)), C.c_int(1 if fp32 else 0))
+        check()
+
+    @staticmethod
+    def class_variants(cls, fp32=False):
+        """The launch variants of class cls (qb_class_variants)."""
+        codes = np.zeros(32, dtype=np.int32)
+        n = lib().qb_class_variants(C.c_int(cls), C.c_int(1 if fp32 else 0), _ptr(codes), C.c_int(32))
+        return [int(x) for x in codes[:n]]
+
     def oneint(self):
         """(S, H): the overlap of fullx and the core Hamiltonian of get1e."""
         n = self.nbasis

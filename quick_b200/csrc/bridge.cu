@@ -1119,10 +1119,42 @@ int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out)
     return fock_build(c, d_o_in, d_o_out);
 }
 
+// The launch variants of class cls (codes as qb_autotune_classes writes them).
+int qb_class_variants(int cls, int fp32, int* codes, int cap)
+{
+    if (cls < 0 || cls >= kNumClasses) return 0;
+    return class_variants(cls, fp32 ? 1 : 0, codes, cap);
+}
+
+// Sets the launch variant of every class (the codes qb_autotune_classes
+// writes), as if tuned: each code must be one of the class's variants.
+int qb_set_class_groups(const int* groups, int n, int fp32)
+{
+    Context& c = ctx();
+    if (require(c.have_basis, "gpu_upload_basis_ must precede qb_set_class_groups")) return 1;
+    if (require(n == kNumClasses, "qb_set_class_groups: one code per class expected")) return 1;
+    std::vector<int> v(groups, groups + n);
+    for (int k = 0; k < n; k++) {
+        int codes[16];
+        const int nv = class_variants(k, fp32 ? 1 : 0, codes, 16);
+        bool ok = false;
+        for (int i = 0; i < nv; i++) ok = ok || codes[i] == v[k];
+        if (!ok) {
+            set_error(1, "qb_set_class_groups: code %d is not a variant of class %d", v[k], k);
+            return 1;
+        }
+    }
+    (fp32 ? c.class_group32 : c.class_group) = v;
+    (fp32 ? c.tuned32 : c.tuned64) = true;
+    return 0;
+}
+
 // Per-class autotuning of the lanes per shell quartet: after a Fock build,
-// every compiled lane-group size of every straight-line class is timed on
-// that build's quartet lists (writing into a scratch Fock matrix), and the
-// fastest is kept for the following builds of this molecule.
+// every compiled variant of every straight-line class (each lane-group size,
+// and for the light classes the kernels that stage the Boys records in
+// shared memory, code kSbFlag + lanes) is timed on that build's quartet
+// lists (writing into a scratch Fock matrix), and the fastest is kept for
+// the following builds of the session.
 int qb_autotune_classes(int* groups, int cap)
 {
     Context& c = ctx();
@@ -1153,7 +1185,10 @@ int qb_autotune_classes(int* groups, int cap)
         const int nq = (int)std::min<long long>(capk, 1LL << 30);
         int best_g = groups_k[k];
         float best_t = 1e30f;
-        for (int g = 1; g <= class_max_group(k); g *= 2) {
+        int codes[16];
+        const int nv = class_variants(k, f32 ? 1 : 0, codes, 16);
+        for (int vi = 0; vi < nv; vi++) {
+            const int g = codes[vi];
             float tmin = 1e30f;
             for (int rep = 0; rep < 2; rep++) {
                 CK(cudaEventRecord(e0, c.stream));

@@ -199,6 +199,24 @@ def group_sizes(la, lb, lc, ld):
     return [1]
 
 
+SB_FLAG = 256     # kSbFlag of eri_common.cuh
+SB_MAX_L = 2      # kSbMaxL of eri_common.cuh
+
+
+def sb_group_sizes(la, lb, lc, ld):
+    """Lanes per quartet of the staged-Boys kernels of a class (FP64, the
+    light classes, whose per-primitive Boys reads are their largest load;
+    FP32 variants were measured slower than the plain FP32 kernels on every
+    light class of (H2O)32/6-31G** and are not built)."""
+    return [1, 2, 4] if la + lb + lc + ld <= SB_MAX_L else []
+
+
+def class_variants(la, lb, lc, ld):
+    """Every launch code of a class the autotuner tries: lanes per quartet,
+    then SB_FLAG + lanes for the staged-Boys kernels."""
+    return group_sizes(la, lb, lc, ld) + [SB_FLAG + g for g in sb_group_sizes(la, lb, lc, ld)]
+
+
 def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
     """One angular class of the Fock build.  prec = "float": the FP32 variant
     of the mixed-precision split (vertical and horizontal recurrences,
@@ -232,7 +250,7 @@ def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
     w("namespace qb {")
     ev = "ClassEval32" if f32 else "ClassEval"
     w("template <> struct %s<%d, %d, %d, %d> {" % (ev, la, lb, lc, ld))
-    w("template <int G>")
+    w("template <int G, int SB = 0>   // SB: Boys records staged in shared memory by the kernel")
     w("__device__ __forceinline__ static void run(const QuartetCtx& q, const FockParams& P, int sub)")
     w("{")
     w("    constexpr int L = %d;" % L)
@@ -257,7 +275,7 @@ def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
         b("if (!prim_survives(q, xb.z, xk.z, P.prim_limit)) continue;")
         b("PrimQuartet s;")
         b("double Fm[L + 1];")
-        b("prim_quartet<L>(pb, pk, P, s, Fm);")
+        b("prim_quartet<L, SB>(pb, pk, P, s, Fm);")
         b("const double PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
         b("const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
         bra_load = ["const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);",
@@ -383,6 +401,7 @@ def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
         w("__device__ __forceinline__ static void store(const QuartetCtx& q, const FockParams& P, const AoIntOut& O)")
         w("{")
         w("    constexpr int L = %d;" % L)
+        w("    constexpr int SB = 0;   // the Boys table from global memory")
         for e, f, _ in targets:
             w("    double c_%s_%s = 0.0;" % (nm(e), nm(f)))
         w("    for (int ib = 0; ib < q.nbra; ib++) {")
@@ -418,6 +437,12 @@ def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
     for g in gs:
         w("    case %d: { auto kern = %s<%d, %d, %d, %d, %d>; QB_LAUNCH(kern, class_grid(nq, %d, nsm), 128, 0, st, P, cls%s); return %d; }"
           % (g, kname, la, lb, lc, ld, g, g, "" if f32 else ", 0", g))
+    for g in ([] if f32 else sb_group_sizes(la, lb, lc, ld)):
+        # staged-Boys variant (eri_common.cuh): code kSbFlag + lanes per quartet
+        w("    case %d: { auto kern = fock_class_kernel_sb<%d, %d, %d, %d, %d>; static const bool a_ = "
+          "cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBoysSmemBytes) == cudaSuccess; (void)a_; "
+          "QB_LAUNCH(kern, class_grid_sb(nq, %d, nsm, kSbBlock, 2), kSbBlock, kBoysSmemBytes, st, P, cls, 0); return %d; }"
+          % (SB_FLAG + g, la, lb, lc, ld, g, g, SB_FLAG + g))
     w("    default: { auto kern = %s<%d, %d, %d, %d, 1>; QB_LAUNCH(kern, class_grid(nq, 1, nsm), 128, 0, st, P, cls%s); return 1; }"
       % (kname, la, lb, lc, ld, "" if f32 else ", 0"))
     w("    }")
@@ -837,7 +862,20 @@ def main(outdir, lmax=2, lmax_all=3):
     lt += ["int class_max_group(int cls)", "{", "    switch (cls) {"]
     for k, c in enumerate(cls_all):
         lt.append("    case %d: return %d;" % (k, max(group_sizes(*c)) if c in gen_set else 1))
-    lt += ["    default: return 1;", "    }", "}", "}  // namespace qb"]
+    lt += ["    default: return 1;", "    }", "}"]
+    lt += ["// launch codes of a class for the autotuner (lanes per quartet, kSbFlag + lanes",
+           "// for the staged-Boys kernels); fp32: the FP32 kernels' codes",
+           "int class_variants(int cls, int fp32, int* codes, int cap)", "{", "    int n = 0;", "    switch (cls) {"]
+    for k, c in enumerate(cls_all):
+        if c not in gen_set:
+            continue
+        v64 = class_variants(*c)
+        v32 = group_sizes(*c) if c in cls32 else [1]
+        lt.append("    case %d: { static const int a[] = {%s}, b[] = {%s}; const int* v = fp32 ? b : a; n = fp32 ? %d : %d; "
+                  "for (int i = 0; i < n && i < cap; i++) codes[i] = v[i]; break; }"
+                  % (k, ", ".join(map(str, v64)), ", ".join(map(str, v32)), len(v32), len(v64)))
+    lt += ["    default: if (cap > 0) codes[0] = 1; n = 1; break;", "    }", "    return n < cap ? n : cap;", "}",
+           "}  // namespace qb"]
     write_if_changed(os.path.join(outdir, "eri_launch.cu"), "\n".join(lt) + "\n")
     import json
     for c in cls_all:

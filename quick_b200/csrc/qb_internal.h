@@ -73,6 +73,9 @@ void launch_add_vector(const double* x, double* y, int n, cudaStream_t st);
 int launch_class(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st);
 int launch_class32(int cls, const FockParams& P, int G, int nq, int nsm, cudaStream_t st);
 int class_max_group(int cls);
+// launch codes of a class for the autotuner: lanes per quartet, and
+// kSbFlag + lanes for the staged-Boys kernels of the light classes
+int class_variants(int cls, int fp32, int* codes, int cap);
 // The warp-per-quartet kernel of eri_generic.cu for any class (shells <= f);
 // fp32_list: walk the class's FP32 list.  Returns -1 if the class needs more
 // shared memory than the GPU offers.

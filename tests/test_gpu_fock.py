@@ -98,7 +98,49 @@ def test_autotuned_lane_groups_keep_the_fock_matrix():
     finally:
         s.close()
     assert np.abs(F1 - F0).max() < 1e-10
-    assert set(int(x) for x in g if x) <= {1, 2, 4, 8, 16, 32}
+    # lanes per quartet, or 256 + lanes for the staged-Boys kernels
+    assert set(int(x) for x in g if x) <= {1, 2, 4, 8, 16, 32, 257, 258, 260}
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 4])
+def test_staged_boys_kernels_match_oracle(oracle_lib, lanes):
+    """The light classes' kernels that stage the Boys records in shared
+    memory (variant 256 + lanes, forced with qb_set_class_groups) give the
+    oracle's Fock matrix (1e-8), also with the mixed split on (FP32 lists in
+    the plain FP32 kernels: within 1e-6)."""
+    from quick_b200 import capi
+    m, b = case("water4_631gs")
+    Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
+    s = capi.Session(0)
+    try:
+        s.upload_molecule(m, b, Y, cp)
+        D = random_density(b.nbasis, seed=7)
+        cm = oracle_lib.cutmatrix(b, D)
+        ref, _ = oracle_lib.fock(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20, hybrid=1.0)
+        n_c = capi.C.c_int(0)
+        cl = np.zeros(4 * 128, dtype=np.int32)
+        cq = np.zeros(128, dtype=np.int64)
+        capi.lib().qb_class_info(capi.C.byref(n_c), capi._ptr(cl), capi._ptr(cq), 128)
+        ncls = n_c.value
+        staged = []
+        for fp32 in (False, True):
+            codes = []
+            for k in range(ncls):
+                v = capi.Session.class_variants(k, fp32)
+                codes.append(256 + lanes if 256 + lanes in v else v[0])
+            staged.append(sum(c > 256 for c in codes))
+            s.set_class_groups(codes, fp32=fp32)
+        got = s.get2e(np.zeros((b.nbasis, b.nbasis), order="F"), D, cm, 1e-10, 1e-20, method=0)
+        s.set_mixed_precision(1e-3)
+        mixed = s.get2e(np.zeros((b.nbasis, b.nbasis), order="F"), D, cm, 1e-10, 1e-20, method=0)
+        with pytest.raises(capi.QuickB200Error):
+            s.set_class_groups([999] * ncls)
+    finally:
+        s.set_mixed_precision(0.0)
+        s.close()
+    assert staged[0] == 5 and staged[1] == 0    # ssss, psss, psps, ppss, dsss; no FP32 variant
+    assert np.abs(got - ref).max() < TOL
+    assert np.abs(mixed - ref).max() < 1e-6
 
 
 def test_fixed_point_fock_is_bit_reproducible(oracle_lib):
