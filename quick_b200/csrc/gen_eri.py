@@ -268,6 +268,8 @@ def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
         b("const float PAx = pb.PAx, PAy = pb.PAy, PAz = pb.PAz;")
         b("const float QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
         bra_load = ["const PrimRec32 pb = load_prim32(P.prim32, q.bra_off + ib);"]
+        bra_decl = ["PrimRec32 pb = {};"]
+        bra_fetch = ["pb = load_prim32(P.prim32, q.bra_off + ib);"]
     else:
         # the ket's three vectors are requested together, ahead of the screen
         b("const double4 xk = load_prim_aux(P.prim, q.ket_off + ik);")
@@ -280,6 +282,8 @@ def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
         b("const double QCx = pk.PAx, QCy = pk.PAy, QCz = pk.PAz;")
         bra_load = ["const double4 xb = load_prim_aux(P.prim, q.bra_off + ib);",
                     "const PrimPair pb = load_prim(P, q.bra_off + ib, xb);"]
+        bra_decl = ["double4 xb = make_double4(0.0, 0.0, 0.0, 0.0);", "PrimPair pb = {};"]
+        bra_fetch = ["xb = load_prim_aux(P.prim, q.bra_off + ib);", "pb = load_prim(P, q.bra_off + ib, xb);"]
     b("const %s WPx = s.WPx, WPy = s.WPy, WPz = s.WPz, WQx = s.WQx, WQy = s.WQy, WQz = s.WQz;" % R)
     b("const %s o2p = s.o2p, o2q = s.o2q, o2pq = s.o2pq, rp = s.rp, rq = s.rq;" % R)
     b("(void)PAx; (void)PAy; (void)PAz; (void)QCx; (void)QCy; (void)QCz; (void)WPx; (void)WPy; (void)WPz;")
@@ -299,13 +303,20 @@ def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
         w("            " + ln)
     w("        }")
     w("    }")
-    # G > 1: the G lanes of a group stride over the flattened primitive quartets
+    # G > 1: the G lanes of a group stride over the flattened primitive
+    # quartets (ket fastest); a lane keeps its bra record until its bra
+    # primitive changes
     w("    } else {")
-    w("    const int nk = q.nket, npq = q.nbra * nk;")
-    w("    for (int t = sub; t < npq; t += G) {")
-    w("        const int ib = t / nk, ik = t - ib * nk;")
-    for ln in bra_load:
-        w("        " + ln)
+    w("    const int nk = q.nket;")
+    w("    int ib = nk > 0 ? sub / nk : 0, ik = sub - ib * nk, cur = -1;")
+    for ln in bra_decl:
+        w("    " + ln)
+    w("    for (; nk > 0 && ib < q.nbra; step_pq(ib, ik, G, nk)) {")
+    w("        if (ib != cur) {")
+    for ln in bra_fetch:
+        w("            " + ln)
+    w("            cur = ib;")
+    w("        }")
     w("        {")
     for ln in body:
         w("            " + ln)
