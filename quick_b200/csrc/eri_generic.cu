@@ -759,6 +759,7 @@ struct GenGradInfo {
     long long per_block;    // scratch doubles per block
     long long x_off[5];     // ket-transformed sums: 2a (c,d), 1 (c,d), 2b (c,d), 2g (c+1,d), 1 (c-1,d)
     int fp32_list;          // walk the class's FP32 list of the mixed split (evaluated in FP64 here)
+    long long y_off[6];     // both sides transferred: (a+1 b|, (a-1 b|, (a b+1|, (a b-1|, |c+1 d), |c-1 d)
 };
 
 __device__ __forceinline__ int gen_gidx(int x, int y, int z, int lo)
@@ -813,6 +814,21 @@ __device__ __forceinline__ double gen_bra_sum(const double* X, int cols, int col
                 s += kBinomD[b[0]][kx] * kBinomD[b[1]][ky] * kBinomD[b[2]][kz] * ABp[b[0] - kx] * ABp[8 + b[1] - ky] *
                      ABp[16 + b[2] - kz] * X[(size_t)gen_gidx(a[0] + kx, a[1] + ky, a[2] + kz, I.elo) * cols + col];
     return s;
+}
+
+// Y[a'][b'][col] = bra transfer of X for every a' in shell lax, b' in shell
+// lbx and ket column col (canonical orders), the block's threads sharing it.
+__device__ void gen_bra_table(const double* X, int cols, int lax, int lbx, double* Y, const GenGradInfo& I,
+                              const double* ABp, int tid, int nt)
+{
+    const int nax = g_ncart(lax), nbx = g_ncart(lbx);
+    for (int t = tid; t < nax * nbx * cols; t += nt) {
+        const int col = t % cols, r = t / cols;
+        int a[3], b[3];
+        gen_uncanon(lax, r / nbx, a);
+        gen_uncanon(lbx, r % nbx, b);
+        Y[t] = gen_bra_sum(X, cols, col, a, b, I, ABp);
+    }
 }
 
 __global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, const GradExtra X, int cls,
@@ -918,17 +934,34 @@ __global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, c
         gen_ket_transform(Ec, XCp, I, I.lc + 1, I.ld, CDp, tid, nt);
         if (I.lc > 0) gen_ket_transform(E1, XCm, I, I.lc - 1, I.ld, CDp, tid, nt);
         __syncthreads();
+        // bra side of the transfer once per (a', b') and ket column: the
+        // derivative integrals of every output then read these tables
+        const int na_ = g_ncart(I.la), nb_ = g_ncart(I.lb), nc_ = g_ncart(I.lc), nd_ = g_ncart(I.ld);
+        const int ccd = nc_ * nd_, ccp = g_ncart(I.lc + 1) * nd_, ccm = g_ncart(I.lc - 1) * nd_;
+        double* YA = sm + I.y_off[0];
+        double* Y1a = sm + I.y_off[1];
+        double* YB = sm + I.y_off[2];
+        double* Y1b = sm + I.y_off[3];
+        double* YCp = sm + I.y_off[4];
+        double* YCm = sm + I.y_off[5];
+        gen_bra_table(XA, ccd, I.la + 1, I.lb, YA, I, ABp, tid, nt);
+        if (I.la > 0) gen_bra_table(X1, ccd, I.la - 1, I.lb, Y1a, I, ABp, tid, nt);
+        gen_bra_table(XB, ccd, I.la, I.lb + 1, YB, I, ABp, tid, nt);
+        if (I.lb > 0) gen_bra_table(X1, ccd, I.la, I.lb - 1, Y1b, I, ABp, tid, nt);
+        gen_bra_table(XCp, ccp, I.la, I.lb, YCp, I, ABp, tid, nt);
+        if (I.lc > 0) gen_bra_table(XCm, ccm, I.la, I.lb, YCm, I, ABp, tid, nt);
+        __syncthreads();
         const double* Dm = P.dense;
         const int nbf = P.nbasis;
         const double hx = P.hybrid;
-        const int ndd = nd, ccd = nc * nd, ccp = g_ncart(I.lc + 1) * nd, ccm = g_ncart(I.lc - 1) * nd;
+        const int nbp = g_ncart(I.lb + 1), nbm = g_ncart(I.lb - 1);
         double gs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        const int nout = na * nb * nc * nd;
+        const int nout = na_ * nb_ * nc_ * nd_;
         for (int o = tid; o < nout; o += nt) {
             int r = o;
-            const int id = r % nd; r /= nd;
-            const int ic = r % nc; r /= nc;
-            const int ibb = r % nb; r /= nb;
+            const int id = r % nd_; r /= nd_;
+            const int ic = r % nc_; r /= nc_;
+            const int ibb = r % nb_; r /= nb_;
             const int ia = r;
             int a[3], b[3], c[3], d[3];
             for (int k = 0; k < 3; k++) {
@@ -943,29 +976,30 @@ __global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, c
             const double Dad = __ldg(Dm + (size_t)fa * nbf + fd), Dbc = __ldg(Dm + (size_t)fb * nbf + fc);
             const double g = 4.0 * Dab * Dcd - hx * (Dac * Dbd + Dad * Dbc);
             if (g == 0.0) continue;
+            const int ca = gen_canon(a[1], a[2]), cb = gen_canon(b[1], b[2]);
             const int dcan = gen_canon(d[1], d[2]);
-            const int colcd = gen_canon(c[1], c[2]) * ndd + dcan;
+            const int colcd = gen_canon(c[1], c[2]) * nd_ + dcan;
             for (int i = 0; i < 3; i++) {
                 int u[3] = {a[0], a[1], a[2]};
                 u[i]++;
-                double dA = gen_bra_sum(XA, ccd, colcd, u, b, I, ABp);
+                double dA = YA[((size_t)gen_canon(u[1], u[2]) * nb_ + cb) * ccd + colcd];
                 if (a[i] > 0) {
                     u[i] -= 2;
-                    dA -= a[i] * gen_bra_sum(X1, ccd, colcd, u, b, I, ABp);
+                    dA -= a[i] * Y1a[((size_t)gen_canon(u[1], u[2]) * nb_ + cb) * ccd + colcd];
                 }
                 int v[3] = {b[0], b[1], b[2]};
                 v[i]++;
-                double dB = gen_bra_sum(XB, ccd, colcd, a, v, I, ABp);
+                double dB = YB[((size_t)ca * nbp + gen_canon(v[1], v[2])) * ccd + colcd];
                 if (b[i] > 0) {
                     v[i] -= 2;
-                    dB -= b[i] * gen_bra_sum(X1, ccd, colcd, a, v, I, ABp);
+                    dB -= b[i] * Y1b[((size_t)ca * nbm + gen_canon(v[1], v[2])) * ccd + colcd];
                 }
                 int w[3] = {c[0], c[1], c[2]};
                 w[i]++;
-                double dC = gen_bra_sum(XCp, ccp, gen_canon(w[1], w[2]) * ndd + dcan, a, b, I, ABp);
+                double dC = YCp[((size_t)ca * nb_ + cb) * ccp + gen_canon(w[1], w[2]) * nd_ + dcan];
                 if (c[i] > 0) {
                     w[i] -= 2;
-                    dC -= c[i] * gen_bra_sum(XCm, ccm, gen_canon(w[1], w[2]) * ndd + dcan, a, b, I, ABp);
+                    dC -= c[i] * YCm[((size_t)ca * nb_ + cb) * ccm + gen_canon(w[1], w[2]) * nd_ + dcan];
                 }
                 gs[i] += g * dA;
                 gs[3 + i] += g * dB;
@@ -1019,7 +1053,7 @@ int launch_generic_grad_class(int cls, int la, int lb, int lc, int ld, const Foc
     const int elo = la > 0 ? la - 1 : 0, flo = lc > 0 ? lc - 1 : 0;
     const GenCached* gc = gen_cached(elo, la + lb + 1 - elo, flo, lc + ld + 1 - flo, true);
     if (!gc) return -1;
-    GenGradInfo I{la, lb, lc, ld, elo, flo, gc->G.ne, gc->G.nf, 0, {0, 0, 0, 0, 0}, fp32_list};
+    GenGradInfo I{la, lb, lc, ld, elo, flo, gc->G.ne, gc->G.nf, 0, {0, 0, 0, 0, 0}, fp32_list, {0, 0, 0, 0, 0, 0}};
     const long long nacc = (long long)I.ne * I.nf, ndd = g_ncart(ld);
     const long long cols[5] = {g_ncart(lc) * ndd, g_ncart(lc) * ndd, g_ncart(lc) * ndd, g_ncart(lc + 1) * ndd,
                                g_ncart(lc - 1) * ndd};
@@ -1027,6 +1061,14 @@ int launch_generic_grad_class(int cls, int la, int lb, int lc, int ld, const Foc
     for (int k = 0; k < 5; k++) {
         I.x_off[k] = off;
         off += (long long)I.ne * cols[k];
+    }
+    const long long na = g_ncart(la), nb = g_ncart(lb);
+    const long long ny[6] = {g_ncart(la + 1) * nb * cols[0], g_ncart(la - 1) * nb * cols[0],
+                             na * g_ncart(lb + 1) * cols[0], na * g_ncart(lb - 1) * cols[0], na * nb * cols[3],
+                             na * nb * cols[4]};
+    for (int k = 0; k < 6; k++) {
+        I.y_off[k] = off;
+        off += ny[k];
     }
     I.per_block = off;
     // scratch of at most 256 MB: four blocks per SM where it allows
