@@ -15,6 +15,13 @@ namespace xcg {
 
 constexpr int BM = 64, BN = 64, BK = 16;
 constexpr int LDS = BM + 8;   // shared row stride (doubles): fragment loads hit each bank pair twice, the minimum
+
+// Column j of tile row k sits at k * LDS + swz(j, k): the XOR of the low three
+// bits with k spreads the tile stores of an operand whose unit stride is
+// along K (16 consecutive k of one column per half-warp) over all banks
+// instead of two (8-way conflicts before), and leaves the fragment loads
+// and the other operand's stores at the two-wavefront minimum.
+__device__ __forceinline__ int swz(int j, int k) { return j ^ (k & 7); }
 constexpr int kThreads = 128; // 2 x 2 warps, 32 x 32 of C each
 
 struct GemmArgs {
@@ -54,7 +61,7 @@ __device__ __forceinline__ void store_tile(double* s, const double* r)
         int j, k;
         if (KFAST) { k = t & 15; j = (t >> 4) + 8 * i; }
         else { j = t & 63; k = (t >> 6) + 2 * i; }
-        s[k * LDS + j] = r[i];
+        s[k * LDS + swz(j, k)] = r[i];
     }
 }
 
@@ -103,9 +110,9 @@ __global__ void __launch_bounds__(kThreads) dmma_gemm_kernel(const GemmArgs g)
         for (int kk = 0; kk < BK; kk += 4) {
             double fa[4], fb[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++) fa[i] = as[(kk + tig) * LDS + wm + 8 * i + gid];
+            for (int i = 0; i < 4; i++) fa[i] = as[(kk + tig) * LDS + swz(wm + 8 * i + gid, kk + tig)];
 #pragma unroll
-            for (int j = 0; j < 4; j++) fb[j] = bs[(kk + tig) * LDS + wn + 8 * j + gid];
+            for (int j = 0; j < 4; j++) fb[j] = bs[(kk + tig) * LDS + swz(wn + 8 * j + gid, kk + tig)];
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
