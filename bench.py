@@ -364,6 +364,9 @@ def run_ours(args, ws, rank, local):
     g_in = np.zeros(3 * m.natom)
     for _ in range(args.warmup):
         sess.grad(g_in, D, cm, cutoff, plim)
+    ggroups64 = sess.autotune_grad()   # lanes per quartet of the light gradient classes
+    for _ in range(args.warmup):
+        sess.grad(g_in, D, cm, cutoff, plim)
     gr_ms, gr_e2e = [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
@@ -376,13 +379,19 @@ def run_ours(args, ws, rank, local):
     lib.qb_set_mixed_precision(capi.C.c_double(MIXED_CUT))
     for _ in range(args.warmup):
         sess.grad(g_in, D, cm, cutoff, plim)
+    ggroups32 = sess.autotune_grad()
+    for _ in range(args.warmup):
+        sess.grad(g_in, D, cm, cutoff, plim)
     grm_ms = []
     for _ in range(args.steps):
         gmx = sess.grad(g_in, D, cm, cutoff, plim)
         grm_ms.append(sess.grad_stats()["ms"])
     lib.qb_set_mixed_precision(capi.C.c_double(0.0))
     grm = max_over_ranks(float(np.mean(grm_ms)), ws)
+    light = [i for i in range(k) if cq[i] > 0 and sum(cl[4 * i:4 * i + 4]) <= 2]
     grad_line = {"metric": "two-electron gradient shell quartets/s (FP64)", "quartets_per_call": gq,
+                 "lane_groups": {"fp64": {"%d%d%d%d" % tuple(cl[4 * i:4 * i + 4]): int(ggroups64[i]) for i in light},
+                                 "fp32": {"%d%d%d%d" % tuple(cl[4 * i:4 * i + 4]): int(ggroups32[i]) for i in light}},
                  "kernel_ms": max_over_ranks(float(np.mean(gr_ms)), ws),
                  "value": gq * ws / (max_over_ranks(float(np.mean(gr_ms)), ws) * 1e-3), "unit": "quartets/s",
                  "e2e_ms_per_call": max_over_ranks(float(np.mean(gr_e2e)), ws),
@@ -460,13 +469,15 @@ def run_scf(args, ws, rank, local):
     nmol = max(1, min(args.steps, 5))
     # one session for every molecule (the library's tables and buffers are
     # reused); warm-up molecules, all-FP64 and mixed, each followed by the
-    # lane-group autotuner (FP64 class kernels, then FP32 ones)
+    # lane-group autotuners of the Fock and gradient kernels (FP64, then FP32)
     sess = capi.Session(local)
     scf.run_rhf_device(m, WORKLOAD["basis"], 1e-10, 1e-20, conv=1e-8, device=local, session=sess)
     sess.autotune()
+    sess.autotune_grad()
     scf.run_rhf_device(m, WORKLOAD["basis"], 1e-10, 1e-20, conv=1e-8, device=local, session=sess,
                        mixed_cut=MIXED_CUT)
     sess.autotune()
+    sess.autotune_grad()
     res = {}
     # every variant but the first replays each SCF iteration from a CUDA graph
     for tag, kw in (("fp64_eager", {}), ("fp64", dict(graph=True)), ("mixed", dict(mixed_cut=MIXED_CUT, graph=True)),

@@ -226,6 +226,20 @@ int qb_autotune_classes(int* groups, int cap);
    class is an error (status 1) and changes nothing. */
 int qb_set_class_groups(const int* groups, int n, int fp32);
 
+/* No counterpart in QUICK.  The gradient counterpart of qb_autotune_classes: after a gradient
+   call (gpu_grad_ or qb_grad_device), times every compiled lanes-per-quartet size (1, 2, 4) of
+   the gradient kernels of the classes with total angular momentum <= 2 on that call's quartet
+   lists (into a scratch gradient) and keeps the fastest for the session's later gradients; the
+   FP32 kernels after a call with the mixed split.  Writes the chosen sizes, one per class, to
+   groups (cap entries at most).  Synchronises the library stream. */
+int qb_autotune_grad(int* groups, int cap);
+
+/* No counterpart in QUICK.  Sets the lanes per quartet of every gradient class (n = the number
+   of classes; 1, or 2 and 4 where qb_autotune_grad may choose them) for the FP64 or the FP32
+   kernels, as if tuned.  A size that is not compiled for its class is an error (status 1) and
+   changes nothing. */
+int qb_set_grad_groups(const int* groups, int n, int fp32);
+
 /* No counterpart in QUICK.  The variants of class cls (0 .. the class count of qb_class_info
    - 1) for the FP64 or the FP32 kernels: writes up to cap codes, returns how many there are. */
 int qb_class_variants(int cls, int fp32, int* codes, int cap);

@@ -180,6 +180,20 @@ class Session:
         check()
         return g
 
+    def autotune_grad(self):
+        """Time the lanes-per-quartet sizes of the light gradient classes on
+        the last gradient call's lists and keep the fastest (qb_autotune_grad)."""
+        g = np.zeros(1024, dtype=np.int32)
+        lib().qb_autotune_grad(_ptr(g), 1024)
+        check()
+        return g
+
+    def set_grad_groups(self, groups, fp32=False):
+        """Set every gradient class's lanes per quartet (qb_set_grad_groups)."""
+        g = np.ascontiguousarray(groups, dtype=np.int32)
+        lib().qb_set_grad_groups(_ptr(g), C.c_int(len(g)), C.c_int(1 if fp32 else 0))
+        check()
+
     def set_class_groups(self, groups, fp32=False):
         """Set every class's launch variant (qb_set_class_groups)."""
         g = np.ascontiguousarray(groups, dtype=np.int32)

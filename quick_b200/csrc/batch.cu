@@ -426,8 +426,8 @@ extern "C" int qb_batch_grad_device(const double* d_dense, double* d_grad)
     for (int k = 0; k < kNumClasses; k++) {
         if (B.cap[k] == 0) continue;
         const int nq = (int)std::min<long long>(B.cap[k], 1LL << 30);
-        const int GS = std::min(s.g64.empty() ? 1 : std::max(s.g64[k], 1), grad_max_group(k));
         for (int f32 = 0; f32 < (s.mixed_cut > 0.0 ? 2 : 1); f32++) {
+            const int GS = session_grad_lanes(k, f32);
             const int rc = f32 ? launch_grad_class32(k, P, GX, GS, nq, s.nsm, s.st)
                                : launch_grad_class(k, P, GX, GS, nq, s.nsm, s.st);
             if (rc < 0) {

@@ -103,6 +103,7 @@ struct Context {
     std::vector<ScreenClass> screen_cls;
     std::vector<int> class_group;        // lanes per shell quartet of each class kernel
     std::vector<int> class_group32;      // the same for the FP32 class kernels of the mixed split
+    std::vector<int> grad_group, grad_group32;   // lanes per quartet of the gradient kernels (empty: 1)
     HostTables host;                     // host copies of the pair and primitive tables (build_tables)
     bool tuned64 = false, tuned32 = false;   // set by qb_autotune_classes
     int generic_min_l = 99;              // classes with L sum >= this run the generic kernel (QB_GENERIC_MIN_L)
@@ -664,6 +665,13 @@ static int join_side_streams(Context& c)
 }
 
 // Two-electron gradient into d_grad (3 natom), same quartet lists.
+// Lanes per quartet of gradient class k (qb_autotune_grad's choice, else 1).
+static int grad_lanes(const Context& c, int k, int f32)
+{
+    const std::vector<int>& g = f32 ? c.grad_group32 : c.grad_group;
+    return g.empty() ? 1 : std::min(std::max(g[k], 1), grad_max_group(k));
+}
+
 static int grad_build(Context& c)
 {
     std::vector<int> cnt, cnt32;
@@ -684,7 +692,7 @@ static int grad_build(Context& c)
         for (int f32 = 0; f32 < 2; f32++) {
             const int nq = f32 ? cnt32[k] : cnt[k];
             if (nq == 0) continue;
-            const int GS = std::min(c.class_group.empty() ? 1 : std::max(c.class_group[k], 1), grad_max_group(k));
+            const int GS = grad_lanes(c, k, f32);
             cudaStream_t st = side_stream(c, turn++);
             const int rc = f32 ? launch_grad_class32(k, P, G, GS, nq, c.nsm, st) : launch_grad_class(k, P, G, GS, nq, c.nsm, st);
             if (rc < 0) {
@@ -795,6 +803,12 @@ static Context& ctx()
 {
     if (!g) g = new Context();
     return *g;
+}
+
+// Lanes per quartet of the gradient kernels of class k for the batched gradient (the session's choice).
+int session_grad_lanes(int k, int f32)
+{
+    return grad_lanes(ctx(), k, f32);
 }
 
 }  // namespace qb
@@ -1117,6 +1131,82 @@ int qb_fock_device(const double* d_dense, const double* d_o_in, double* d_o_out)
     CK(c.d_dense_raw.alloc(nn));
     CK(cudaMemcpyAsync(c.d_dense_raw.p, d_dense, nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
     return fock_build(c, d_o_in, d_o_out);
+}
+
+// Gradient counterpart of qb_autotune_classes: after a gradient call, every
+// compiled lanes-per-quartet size of every gradient class with more than one
+// (the light classes) is timed on that call's quartet lists into a scratch
+// gradient, and the fastest is kept for the session's later gradients (the
+// FP32 kernels after a call with the mixed split).
+int qb_autotune_grad(int* groups, int cap)
+{
+    Context& c = ctx();
+    if (require(c.have_pairs && c.have_cutoff && c.d_quartets.p != nullptr && c.natom > 0,
+                "a gradient call must precede qb_autotune_grad"))
+        return 1;
+    DevBuf<double> scratch;
+    CK(scratch.alloc(3 * (size_t)c.natom));
+    CK(cudaMemsetAsync(scratch.p, 0, 3 * (size_t)c.natom * sizeof(double), c.stream));
+    FockParams P = fock_params(c);
+    GradExtra G{c.d_shell_atom.p, c.d_pair_sh.p, scratch.p, c.natom, 3 * c.natom * 8 <= 48 * 1024 ? 1 : 0};
+    const bool verbose = getenv("QB_AUTOTUNE_VERBOSE") && atoi(getenv("QB_AUTOTUNE_VERBOSE")) > 0;
+    std::vector<int> cnt(kNumClasses), cnt32(kNumClasses);
+    CK(cudaMemcpy(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cnt32.data(), c.d_class_count32.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost));
+    const bool f32 = c.mixed_cut > 0.0;
+    std::vector<int>& gg = f32 ? c.grad_group32 : c.grad_group;
+    if (gg.empty()) gg.assign(kNumClasses, 1);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int k = 0; k < kNumClasses; k++) {
+        const int nq = f32 ? cnt32[k] : cnt[k];
+        if (nq == 0 || grad_max_group(k) < 2) continue;
+        int best_g = gg[k];
+        float best_t = 1e30f;
+        for (int g = 1; g <= grad_max_group(k); g *= 2) {
+            float tmin = 1e30f;
+            for (int rep = 0; rep < 2; rep++) {
+                CK(cudaEventRecord(e0, c.stream));
+                const int rc = f32 ? launch_grad_class32(k, P, G, g, nq, c.nsm, c.stream)
+                                   : launch_grad_class(k, P, G, g, nq, c.nsm, c.stream);
+                CK(cudaEventRecord(e1, c.stream));
+                CK(cudaEventSynchronize(e1));
+                if (rc < 0) break;
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                tmin = std::min(tmin, ms);
+            }
+            if (verbose)
+                fprintf(stderr, "autotune grad %s (%d%d|%d%d) GS=%d %.4f ms\n", f32 ? "fp32" : "fp64", kClassL[k][0],
+                        kClassL[k][1], kClassL[k][2], kClassL[k][3], g, tmin);
+            if (tmin < best_t) best_t = tmin, best_g = g;
+        }
+        gg[k] = best_g;
+    }
+    CK(cudaGetLastError());
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    scratch.release();
+    for (int k = 0; k < std::min(cap, kNumClasses); k++) groups[k] = gg[k];
+    return 0;
+}
+
+// Sets the lanes per quartet of every gradient class, as if tuned: each
+// must be a compiled size (a power of two up to the class's maximum).
+int qb_set_grad_groups(const int* groups, int n, int fp32)
+{
+    Context& c = ctx();
+    if (require(n == kNumClasses, "qb_set_grad_groups: one size per class expected")) return 1;
+    for (int k = 0; k < n; k++) {
+        const int g = groups[k];
+        if (g < 1 || g > grad_max_group(k) || (g & (g - 1))) {
+            set_error(1, "qb_set_grad_groups: %d lanes is not compiled for class %d", g, k);
+            return 1;
+        }
+    }
+    (fp32 ? c.grad_group32 : c.grad_group).assign(groups, groups + n);
+    return 0;
 }
 
 // The launch variants of class cls (codes as qb_autotune_classes writes them).

@@ -181,10 +181,10 @@ F32_MAX_L = 6
 
 
 def grad_group_sizes(la, lb, lc, ld):
-    """Lanes per shell quartet compiled for a gradient class.  One: measured
-    on (H2O)32/6-31G**, groups of 2-4 lanes for the light classes made the
-    gradient 6% slower (274 vs 259 ms)."""
-    return [1]
+    """Lanes per shell quartet compiled for a gradient class: 1, 2 and 4 for
+    the classes with total angular momentum <= 2 (qb_autotune_grad picks
+    one per class), 1 for the others."""
+    return [1, 2, 4] if la + lb + lc + ld <= 2 else [1]
 
 
 def group_sizes(la, lb, lc, ld):

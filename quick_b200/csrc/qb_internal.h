@@ -101,6 +101,7 @@ int launch_generic_grad_class(int cls, int la, int lb, int lc, int ld, const Foc
                               int nsm, int fp32_list, cudaStream_t st);
 void generic_release();
 int grad_max_group(int cls);
+int session_grad_lanes(int k, int f32);   // the session's gradient lanes per quartet of class k
 int fma_probe(int fp64, int nsm, double* gflops, cudaStream_t st);
 void launch_count_prims(const FockParams& P, int ncls, unsigned long long* out, int nsm, cudaStream_t st);
 
