@@ -234,6 +234,14 @@ int qb_set_class_groups(const int* groups, int n, int fp32);
    groups (cap entries at most).  Synchronises the library stream. */
 int qb_autotune_grad(int* groups, int cap);
 
+/* No counterpart in QUICK.  Passes per Fock build or gradient: the screened quartet lists are
+   written in passes over disjoint ranges of bra pairs when the whole list (16 bytes a quartet)
+   would take more than the list budget, QB_LIST_BUDGET_MB megabytes or else 35% of the free
+   device memory when the lists are sized (at the first build after a change of cutoff or
+   molecule).  Returns the current count (1: one pass).  The stored-integral path (gpu_aoint_)
+   needs one pass and reports an error otherwise. */
+int qb_list_passes(void);
+
 /* No counterpart in QUICK.  Sets the lanes per quartet of every gradient class (n = the number
    of classes; 1, or 2 and 4 where qb_autotune_grad may choose them) for the FP64 or the FP32
    kernels, as if tuned.  A size that is not compiled for its class is an error (status 1) and

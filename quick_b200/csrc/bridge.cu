@@ -101,6 +101,15 @@ struct Context {
     DevBuf<int> d_shell_first;                      // Ksumtype - 1 (nshell + 1), for the device density screen
     long long shell_first_version = -1;
     std::vector<ScreenClass> screen_cls;
+    // The quartet lists of one build are written in npass passes over
+    // disjoint bra ranges when the whole list would pass the memory budget
+    // (list_budget_bytes): pass p's classes are pass_cls[p * kNumClasses + k],
+    // all passes sharing d_quartets.  npass = 1: one pass, the full ranges.
+    int npass = 1;
+    std::vector<ScreenClass> pass_cls;
+    DevBuf<ScreenClass> d_pass_cls;
+    DevBuf<long long> d_pass_offset, d_pass_end;
+    DevBuf<int> d_total_count, d_total_count32;   // per class, summed over a build's passes
     std::vector<int> class_group;        // lanes per shell quartet of each class kernel
     std::vector<int> class_group32;      // the same for the FP32 class kernels of the mixed split
     std::vector<int> grad_group, grad_group32;   // lanes per quartet of the gradient kernels (empty: 1)
@@ -534,7 +543,10 @@ static FockParams fock_params(Context& c)
     P.pair_Y = c.d_pair_Y.p;
     P.pair_AB = c.d_pair_AB.p;
     P.quartets = c.d_quartets.p;
-    P.class_offset = c.d_class_offset.p;
+    // the lists in the buffer: the last pass's (the only one unless the
+    // lists were cut into passes)
+    const size_t last = (size_t)(c.npass - 1) * kNumClasses;
+    P.class_offset = c.d_pass_offset.p ? c.d_pass_offset.p + last : c.d_class_offset.p;
     P.class_count = c.d_class_count.p;
     P.dense = c.d_dense.p;
     P.fock = c.d_fock.p;
@@ -547,7 +559,7 @@ static FockParams fock_params(Context& c)
     P.integral_cutoff = c.integralCutoff;
     P.mixed_cut = c.mixed_cut;
     P.class_count32 = c.d_class_count32.p;
-    P.class_end = c.d_class_end.p;
+    P.class_end = c.d_pass_end.p ? c.d_pass_end.p + last : c.d_class_end.p;
     P.ket_segs = c.d_ket_segs.p;
     P.prim32 = c.d_prim32.p;
     P.pair_A = c.d_pair_A.p;
@@ -559,6 +571,18 @@ static FockParams fock_params(Context& c)
 // Size the per-class quartet lists by the Schwarz-only count (an upper bound
 // for every density), once per geometry and cutoff.
 static double g_sized_cutoff = -1.0;
+
+// Device memory the quartet lists of one pass may take: QB_LIST_BUDGET_MB,
+// else 35% of the device memory free when the lists are sized.
+static double list_budget_bytes(const Context& c)
+{
+    (void)c;
+    const char* mb = getenv("QB_LIST_BUDGET_MB");
+    if (mb && atof(mb) > 0) return atof(mb) * 1048576.0;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 16.0 * 1073741824.0;
+    return 0.35 * (double)fr;
+}
 static int size_quartet_lists(Context& c)
 {
     CK(c.d_screen_cls.alloc(kNumClasses));
@@ -587,17 +611,87 @@ static int size_quartet_lists(Context& c)
         off += (long long)cnt[k];
         ends[k] = off;
     }
-    CK(c.d_quartets.alloc((size_t)std::max<long long>(off, 1)));
     CK(cudaMemcpy(c.d_screen_cls.p, c.screen_cls.data(), kNumClasses * sizeof(ScreenClass), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.d_class_offset.p, offs.data(), kNumClasses * sizeof(long long), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.d_class_end.p, ends.data(), kNumClasses * sizeof(long long), cudaMemcpyHostToDevice));
+    // passes over disjoint bra ranges when the whole list would pass the
+    // budget: each class's bra range cut into npass equal parts, counted
+    // again per pass; npass doubles until the largest pass fits (or 64)
+    const int K = kNumClasses;
+    const double budget = list_budget_bytes(c);
+    int npass = 1;
+    long long longest = off;
+    std::vector<ScreenClass> pc(c.screen_cls);
+    if ((double)off * sizeof(Quartet) > budget) {
+        npass = std::min(64, (int)std::ceil((double)off * sizeof(Quartet) / budget));
+        std::vector<unsigned long long> pcnt;
+        for (;;) {
+            pc.assign((size_t)npass * K, ScreenClass{});
+            for (int p = 0; p < npass; p++)
+                for (int k = 0; k < K; k++) {
+                    ScreenClass s = c.screen_cls[k];
+                    const long long nb = s.bra_end - s.bra_begin;
+                    s.bra_end = s.bra_begin + (int)(nb * (p + 1) / npass);
+                    s.bra_begin = s.bra_begin + (int)(nb * p / npass);
+                    pc[(size_t)p * K + k] = s;
+                }
+            CK(c.d_pass_cls.alloc(pc.size()));
+            CK(cudaMemcpy(c.d_pass_cls.p, pc.data(), pc.size() * sizeof(ScreenClass), cudaMemcpyHostToDevice));
+            pcnt.assign((size_t)npass * K, 0);
+            longest = 0;
+            for (int p = 0; p < npass; p++) {
+                CK(cudaMemsetAsync(c.d_counts.p, 0, K * sizeof(unsigned long long), c.stream));
+                ScreenParams Sp{c.d_pass_cls.p + (size_t)p * K, c.d_counts.p, nullptr, c.d_counts32.p};
+                launch_screen(Sp, P, K, 1, c.nsm, c.stream);
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(pcnt.data() + (size_t)p * K, c.d_counts.p, K * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, c.stream));
+            }
+            CK(cudaStreamSynchronize(c.stream));
+            for (int p = 0; p < npass; p++) {
+                long long o = 0;
+                for (int k = 0; k < K; k++) {
+                    ScreenClass& s = pc[(size_t)p * K + k];
+                    s.out_offset = o;
+                    s.capacity = (long long)pcnt[(size_t)p * K + k];
+                    o += s.capacity;
+                }
+                longest = std::max(longest, o);
+            }
+            if ((double)longest * sizeof(Quartet) <= budget || npass >= 64) break;
+            npass = std::min(64, 2 * npass);
+        }
+    }
+    c.npass = npass;
+    c.pass_cls = pc;
+    std::vector<long long> po((size_t)npass * K), pe((size_t)npass * K);
+    for (size_t i = 0; i < pc.size(); i++) {
+        po[i] = pc[i].out_offset;
+        pe[i] = pc[i].out_offset + pc[i].capacity;
+    }
+    CK(c.d_pass_cls.alloc(pc.size()));
+    CK(c.d_pass_offset.alloc(pc.size()));
+    CK(c.d_pass_end.alloc(pc.size()));
+    CK(c.d_total_count.alloc(K));
+    CK(c.d_total_count32.alloc(K));
+    CK(cudaMemcpy(c.d_pass_cls.p, pc.data(), pc.size() * sizeof(ScreenClass), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.d_pass_offset.p, po.data(), po.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.d_pass_end.p, pe.data(), pe.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(c.d_quartets.alloc((size_t)std::max<long long>(longest, 1)));
     g_sized_cutoff = c.integralCutoff;
     return 0;
 }
 
+// Class counts of the last build, summed over its passes.
+static const int* build_counts(const Context& c, int f32)
+{
+    if (c.npass > 1) return f32 ? c.d_total_count32.p : c.d_total_count.p;
+    return f32 ? c.d_class_count32.p : c.d_class_count.p;
+}
+
 // Screening into the per-class quartet lists for the current density; the
 // class counts come back to the host to size the class launches.
-static int screen_quartets(Context& c, std::vector<int>& cnt, std::vector<int>& cnt32)
+static int screen_quartets(Context& c, int pass, std::vector<int>& cnt, std::vector<int>& cnt32)
 {
     if (require(c.have_pairs, "gpu_upload_cutoff_matrix_ must precede the two-electron kernels")) return 1;
     if (require(c.have_cutoff, "gpu_upload_cutoff_ must precede the two-electron kernels")) return 1;
@@ -608,9 +702,11 @@ static int screen_quartets(Context& c, std::vector<int>& cnt, std::vector<int>& 
     CK(cudaMemsetAsync(c.d_counts32.p, 0, kNumClasses * sizeof(unsigned long long), c.stream));
     CK(cudaMemsetAsync(c.d_overflow.p, 0, sizeof(int), c.stream));
     CK(c.d_dense.alloc((size_t)n * n));
-    launch_scale_density(c.d_dense_raw.p, c.d_cons.p, c.d_dense.p, n, c.stream);
+    if (pass == 0) launch_scale_density(c.d_dense_raw.p, c.d_cons.p, c.d_dense.p, n, c.stream);
     FockParams P = fock_params(c);   // with the mixed split: the FP32 list from the back of each class region
-    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p, c.d_counts32.p};
+    P.class_offset = c.d_pass_offset.p + (size_t)pass * kNumClasses;
+    P.class_end = c.d_pass_end.p + (size_t)pass * kNumClasses;
+    ScreenParams S{c.d_pass_cls.p + (size_t)pass * kNumClasses, c.d_counts.p, c.d_quartets.p, c.d_counts32.p};
     launch_screen(S, P, kNumClasses, 0, c.nsm, c.stream);
     launch_finish_counts(S, c.d_class_count.p, c.d_class_count32.p, c.d_overflow.p, kNumClasses, c.stream);
     CK(cudaGetLastError());
@@ -675,16 +771,22 @@ static int grad_lanes(const Context& c, int k, int f32)
 static int grad_build(Context& c)
 {
     std::vector<int> cnt, cnt32;
-    if (int rc = screen_quartets(c, cnt, cnt32)) return rc;
+    if (require(c.have_pairs && c.have_cutoff, "gpu_upload_cutoff_ must precede the gradient")) return 1;
+    if (g_sized_cutoff != c.integralCutoff || c.d_quartets.p == nullptr)
+        if (size_quartet_lists(c)) return 2;
     CK(c.d_grad.alloc(3 * (size_t)c.natom));
     CK(cudaMemsetAsync(c.d_grad.p, 0, 3 * (size_t)c.natom * sizeof(double), c.stream));
-    FockParams P = fock_params(c);
     // per-block shared accumulation while 3 natom doubles fit the default 48 KB
     GradExtra G{c.d_shell_atom.p, c.d_pair_sh.p, c.d_grad.p, c.natom, 3 * c.natom * 8 <= 48 * 1024 ? 1 : 0};
     for (int k = 0; k < 4; k++)
         if (!c.ev[k]) CK(cudaEventCreate(&c.ev[k]));
-    CK(cudaEventRecord(c.ev[2], c.stream));
     long long total = 0;
+    for (int pass = 0; pass < c.npass; pass++) {
+    if (int rc = screen_quartets(c, pass, cnt, cnt32)) return rc;
+    FockParams P = fock_params(c);
+    P.class_offset = c.d_pass_offset.p + (size_t)pass * kNumClasses;
+    P.class_end = c.d_pass_end.p + (size_t)pass * kNumClasses;
+    if (pass == 0) CK(cudaEventRecord(c.ev[2], c.stream));
     for (int k = 0; k < kNumClasses; k++) total += cnt[k] + cnt32[k];
     if (int rc = fork_side_streams(c)) return rc;
     int turn = 0;
@@ -705,6 +807,7 @@ static int grad_build(Context& c)
             }
         }
     if (int rc = join_side_streams(c)) return rc;
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[3], c.stream));
     CK(cudaStreamSynchronize(c.stream));
@@ -731,24 +834,43 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
     CK(cudaMemsetAsync(c.d_overflow.p, 0, sizeof(int), c.stream));
     CK(c.d_dense.alloc((size_t)n * n));
     launch_scale_density(c.d_dense_raw.p, c.d_cons.p, c.d_dense.p, n, c.stream);
-    FockParams P = fock_params(c);
-    ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p, c.d_counts32.p};
+    const int K = kNumClasses;
     for (int k = 0; k < 4; k++)
         if (!c.ev[k]) CK(cudaEventCreate(&c.ev[k]));
-    CK(cudaEventRecord(c.ev[0], c.stream));
-    launch_screen(S, P, kNumClasses, 0, c.nsm, c.stream);
-    launch_finish_counts(S, c.d_class_count.p, c.d_class_count32.p, c.d_overflow.p, kNumClasses, c.stream);
+    if (c.npass > 1) {
+        CK(cudaMemsetAsync(c.d_total_count.p, 0, K * sizeof(int), c.stream));
+        CK(cudaMemsetAsync(c.d_total_count32.p, 0, K * sizeof(int), c.stream));
+    }
+    // one pass per bra range (one pass unless the lists pass the memory
+    // budget); a pass's class kernels finish (join) before the next pass's
+    // screen rewrites the shared list buffer
+    for (int pass = 0; pass < c.npass; pass++) {
+    FockParams P = fock_params(c);
+    P.class_offset = c.d_pass_offset.p + (size_t)pass * K;
+    P.class_end = c.d_pass_end.p + (size_t)pass * K;
+    ScreenParams S{c.d_pass_cls.p + (size_t)pass * K, c.d_counts.p, c.d_quartets.p, c.d_counts32.p};
+    if (pass > 0) {
+        CK(cudaMemsetAsync(c.d_counts.p, 0, K * sizeof(unsigned long long), c.stream));
+        CK(cudaMemsetAsync(c.d_counts32.p, 0, K * sizeof(unsigned long long), c.stream));
+    }
+    if (pass == 0) CK(cudaEventRecord(c.ev[0], c.stream));
+    launch_screen(S, P, K, 0, c.nsm, c.stream);
+    launch_finish_counts(S, c.d_class_count.p, c.d_class_count32.p, c.d_overflow.p, K, c.stream);
+    if (c.npass > 1)
+        launch_add_counts(c.d_class_count.p, c.d_class_count32.p, c.d_total_count.p, c.d_total_count32.p, K, c.stream);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(c.ev[1], c.stream));
+    if (pass == 0) {
+        CK(cudaEventRecord(c.ev[1], c.stream));
+        CK(cudaEventRecord(c.ev[2], c.stream));
+    }
     // The class kernels read their quartet counts on the device; the host
     // sizes their grids by the Schwarz-only capacity of each class (an upper
     // bound), so nothing between screening and digestion waits for the host
     // and the whole build can be captured in a CUDA graph.
-    CK(cudaEventRecord(c.ev[2], c.stream));
     if (int rc = fork_side_streams(c)) return rc;
     int turn = 0;
-    for (int k = 0; k < kNumClasses; k++) {
-        const long long cap = c.screen_cls[k].capacity;
+    for (int k = 0; k < K; k++) {
+        const long long cap = c.pass_cls[(size_t)pass * K + k].capacity;
         if (cap == 0) continue;
         const int nq = (int)std::min<long long>(cap, 1LL << 30);
         for (int f32 = 0; f32 < (c.mixed_cut > 0.0 ? 2 : 1); f32++) {
@@ -766,6 +888,7 @@ static int fock_build(Context& c, const double* d_o_in, double* d_o_out)
         }
     }
     if (int rc = join_side_streams(c)) return rc;
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(c.ev[3], c.stream));
     launch_fock_finish(c.d_fock.p, c.d_cons.p, d_o_in, d_o_out, n, c.stream, c.fixed_point);
@@ -782,8 +905,8 @@ static int fock_stats_resolve(Context& c)
     c.stats_pending = false;
     std::vector<int> cnt(kNumClasses), cnt32(kNumClasses);
     int ovf = 0;
-    CK(cudaMemcpyAsync(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaMemcpyAsync(cnt32.data(), c.d_class_count32.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(cnt.data(), build_counts(c, 0), kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(cnt32.data(), build_counts(c, 1), kNumClasses * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaMemcpyAsync(&ovf, c.d_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     if (ovf) return set_error(3, "quartet list overflow (internal sizing error)"), 3;
@@ -904,6 +1027,13 @@ void gpu_shutdown_(void)
     c.d_overflow.release();
     c.d_class_offset.release();
     c.d_class_end.release();
+    c.d_pass_cls.release();
+    c.d_pass_offset.release();
+    c.d_pass_end.release();
+    c.d_total_count.release();
+    c.d_total_count32.release();
+    c.npass = 1;
+    c.pass_cls.clear();
     c.d_quartets.release();
     c.d_ket_segs.release();
     for (auto& e : c.ev)
@@ -1207,6 +1337,13 @@ int qb_set_grad_groups(const int* groups, int n, int fp32)
     }
     (fp32 ? c.grad_group32 : c.grad_group).assign(groups, groups + n);
     return 0;
+}
+
+// Bra-range passes of the current quartet lists (1 unless the lists pass the
+// memory budget).
+int qb_list_passes(void)
+{
+    return ctx().npass;
 }
 
 // The launch variants of class cls (codes as qb_autotune_classes writes them).
@@ -1835,7 +1972,7 @@ int qb_class_info(int* nclasses, int* class_L, long long* class_quartets, int ca
     *nclasses = kNumClasses;
     if (cap < kNumClasses) return 1;
     std::vector<int> cnt(kNumClasses, 0);
-    if (c.d_class_count.p) CK(cudaMemcpy(cnt.data(), c.d_class_count.p, kNumClasses * sizeof(int), cudaMemcpyDeviceToHost));
+    if (c.d_class_count.p) CK(cudaMemcpy(cnt.data(), build_counts(c, 0), kNumClasses * sizeof(int), cudaMemcpyDeviceToHost));
     for (int k = 0; k < kNumClasses; k++) {
         for (int j = 0; j < 4; j++) class_L[4 * k + j] = kClassL[k][j];
         class_quartets[k] = cnt[k];
@@ -1923,6 +2060,7 @@ void gpu_aoint_(double* leastIntegralCutoff, double* maxIntegralCutoff, int* int
         set_error(2, "gpu_aoint_: %s", what);
     };
     if ((g_sized_cutoff != c.integralCutoff || c.d_quartets.p == nullptr) && size_quartet_lists(c)) return fail("sizing");
+    if (c.npass > 1) return fail("the quartet lists exceed the list memory budget (QB_LIST_BUDGET_MB); this path needs them whole");
     FockParams P = fock_params(c);
     ScreenParams S{c.d_screen_cls.p, c.d_counts.p, c.d_quartets.p, c.d_counts32.p};
     cudaMemsetAsync(c.d_counts.p, 0, kNumClasses * sizeof(unsigned long long), c.stream);

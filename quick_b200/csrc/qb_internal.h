@@ -62,6 +62,7 @@ void launch_screen(const ScreenParams& S, const FockParams& P, int ncls, int cou
                    int gx = 0);
 void launch_finish_counts(const ScreenParams& S, int* class_count, int* class_count32, int* overflow, int ncls,
                           cudaStream_t st);
+void launch_add_counts(const int* cnt, const int* cnt32, int* tot, int* tot32, int ncls, cudaStream_t st);
 void launch_scale_density(const double* D, const double* cons, double* Ds, int n, cudaStream_t st);
 void launch_fock_finish(const double* G, const double* cons, const double* Oin, double* Oout, int n, cudaStream_t st,
                         int fixed = 0);

@@ -164,6 +164,22 @@ void launch_finish_counts(const ScreenParams& S, int* class_count, int* class_co
     QB_LAUNCH(finish_counts_kernel, (ncls + 63) / 64, 64, 0, st, S, class_count, class_count32, overflow, ncls);
 }
 
+// Class counts of one pass added to the build's totals.
+__global__ void add_counts_kernel(const int* __restrict__ cnt, const int* __restrict__ cnt32, int* tot, int* tot32,
+                                  int ncls)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ncls) {
+        tot[c] += cnt[c];
+        tot32[c] += cnt32[c];
+    }
+}
+
+void launch_add_counts(const int* cnt, const int* cnt32, int* tot, int* tot32, int ncls, cudaStream_t st)
+{
+    QB_LAUNCH(add_counts_kernel, (ncls + 63) / 64, 64, 0, st, cnt, cnt32, tot, tot32, ncls);
+}
+
 void launch_scale_density(const double* D, const double* cons, double* Ds, int n, cudaStream_t st)
 {
     const size_t N = (size_t)n * n;

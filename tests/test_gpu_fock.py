@@ -172,3 +172,38 @@ def test_fixed_point_fock_is_bit_reproducible(oracle_lib):
     assert np.abs(runs[0] - f64).max() < 1e-12
     ref, _ = oracle_lib.fock(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
     assert np.abs(f64 - ref).max() < 1e-8
+
+
+def test_fock_and_gradient_in_bra_range_passes(oracle_lib):
+    """With a quartet-list budget far below the whole list (QB_LIST_BUDGET_MB
+    = 0.25), the lists are written and consumed in passes over disjoint bra
+    ranges; the Fock matrix, the gradient and the screened-quartet count
+    equal the one-pass results (Fock and gradient to the oracle at 1e-8)."""
+    import os
+    from quick_b200 import capi
+    m, b = case("water4_631gs")
+    Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
+    D = random_density(b.nbasis, seed=7, scale=0.05)
+    cm = oracle_lib.cutmatrix(b, D)
+    ref, _ = oracle_lib.fock(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20, hybrid=1.0)
+    gref = oracle_lib.grad2e(b, m.xyz_bohr, Y, cp, cm, D, 1e-10, 1e-20)
+    out = {}
+    for budget in (None, "0.25"):
+        if budget:
+            os.environ["QB_LIST_BUDGET_MB"] = budget
+        s = capi.Session(0)
+        try:
+            s.upload_molecule(m, b, Y, cp)
+            F = s.get2e(np.zeros((b.nbasis, b.nbasis), order="F"), D, cm, 1e-10, 1e-20, method=0)
+            q = s.fock_stats()["quartets"]
+            g = s.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
+            out[budget] = (F, q, g, capi.lib().qb_list_passes())
+        finally:
+            os.environ.pop("QB_LIST_BUDGET_MB", None)
+            s.close()
+    F1, q1, g1, p1 = out[None]
+    Fp, qp, gp, pp = out["0.25"]
+    assert p1 == 1 and pp > 1
+    assert qp == q1
+    assert np.abs(F1 - ref).max() < TOL and np.abs(Fp - ref).max() < TOL
+    assert np.abs(g1 - gref).max() < TOL and np.abs(gp - gref).max() < TOL
