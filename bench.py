@@ -23,6 +23,7 @@ small clusters (batch); and the CPU baseline, QUICK's own kernel compiled for
 the host cores.
 """
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -485,6 +486,10 @@ def run_scf(args, ws, rank, local):
                     ("mixed_delta_d", dict(mixed_cut=MIXED_CUT, incremental=True, graph=True))):
         secs, runs = [], []
         for _ in range(nmol):
+            # the previous molecule's objects (engines, graphs, device tensors)
+            # are collected before this molecule's clock starts
+            gc.collect()
+            torch.cuda.synchronize()
             barrier(ws)
             r, g = scf.run_rhf_device(m, WORKLOAD["basis"], 1e-10, 1e-20, conv=1e-8, device=local, session=sess,
                                       **kw)
