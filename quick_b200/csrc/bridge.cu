@@ -117,8 +117,12 @@ struct Context {
     bool tuned64 = false, tuned32 = false;   // set by qb_autotune_classes
     int generic_min_l = 99;              // classes with L sum >= this run the generic kernel (QB_GENERIC_MIN_L)
     // per-iteration
-    std::vector<double> o_host;          // O as uploaded (one-electron part)
-    std::vector<double> dense_host;
+    // O (one-electron part) and the density as uploaded by
+    // gpu_upload_calculated_, on the device; the host copy of O is made when
+    // a host-side path (gpu_getxc_, gpu_addint_) first needs it
+    DevBuf<double> d_o_up, d_dense_up;
+    std::vector<double> o_host;
+    bool o_host_valid = false;
     bool have_calc = false;
     double integralCutoff = 1e-7, primLimit = 1e-7, DMCutoff = 1e-9, gradCutoff = 1e-7;
     std::vector<double> cutMatrix;
@@ -1052,6 +1056,8 @@ void gpu_shutdown_(void)
     c.d_H1.release();
     c.d_D1.release();
     c.d_W1.release();
+    c.d_o_up.release();
+    c.d_dense_up.release();
     c.d_g1.release();
     c.d_shell_first.release();
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
@@ -1203,15 +1209,41 @@ void gpu_upload_cutoff_matrix_(double* YCutoff, double* cutPrim)
     c.have_pairs = true;
 }
 
+// Copies O and the density to the device at the call (QUICK copies them at
+// this call too, gpu.cu): straight from the caller's arrays, one DMA each
+// when the caller's memory is pinned; the call returns once both are copied,
+// so the caller may reuse its arrays.
 void gpu_upload_calculated_(double* o, double* co, double* vec, double* dense)
 {
     (void)co;
     (void)vec;
     Context& c = ctx();
     size_t nn = (size_t)c.nbasis * c.nbasis;
-    c.o_host.assign(o, o + nn);
-    c.dense_host.assign(dense, dense + nn);
+    if (c.d_o_up.alloc(nn) != cudaSuccess || c.d_dense_up.alloc(nn) != cudaSuccess ||
+        cudaMemcpyAsync(c.d_o_up.p, o, nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
+        cudaMemcpyAsync(c.d_dense_up.p, dense, nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
+        cudaStreamSynchronize(c.stream) != cudaSuccess) {
+        set_error(2, "upload of the density / operator failed");
+        return;
+    }
+    c.o_host_valid = false;
     c.have_calc = true;
+}
+
+// The uploaded O on the host (for the paths that add to it there).
+static const std::vector<double>& host_o(Context& c)
+{
+    if (!c.o_host_valid) {
+        const size_t nn = (size_t)c.nbasis * c.nbasis;
+        c.o_host.resize(nn);
+        if (cudaMemcpyAsync(c.o_host.data(), c.d_o_up.p, nn * sizeof(double), cudaMemcpyDeviceToHost, c.stream) ==
+                cudaSuccess &&
+            cudaStreamSynchronize(c.stream) == cudaSuccess)
+            c.o_host_valid = true;
+        else
+            set_error(2, "download of the uploaded operator failed");
+    }
+    return c.o_host;
 }
 
 void gpu_upload_cutoff_(double* cutMatrix, double* integralCutoff, double* primLimit, double* DMCutoff)
@@ -1240,9 +1272,9 @@ void gpu_get2e_(double* o)
         set_error(2, "cannot allocate %zu-element matrices", nn);
         return;
     }
-    if (cudaMemcpyAsync(c.d_dense_raw.p, c.dense_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
-        cudaMemcpyAsync(c.d_o_in.p, c.o_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess) {
-        set_error(2, "upload of density / operator failed");
+    if (cudaMemcpyAsync(c.d_dense_raw.p, c.d_dense_up.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess ||
+        cudaMemcpyAsync(c.d_o_in.p, c.d_o_up.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess) {
+        set_error(2, "copy of density / operator failed");
         return;
     }
     if (fock_build(c, c.d_o_in.p, c.d_o_out.p)) return;
@@ -1759,8 +1791,8 @@ void gpu_grad_(double* grad)
     if (require(c.have_calc, "gpu_upload_calculated_ must precede gpu_grad_")) return;
     size_t nn = (size_t)c.nbasis * c.nbasis;
     if (c.d_dense_raw.alloc(nn) != cudaSuccess ||
-        cudaMemcpyAsync(c.d_dense_raw.p, c.dense_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess) {
-        set_error(2, "upload of the density failed");
+        cudaMemcpyAsync(c.d_dense_raw.p, c.d_dense_up.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess) {
+        set_error(2, "copy of the density failed");
         return;
     }
     if (grad_build(c)) return;
@@ -1789,7 +1821,7 @@ void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double*
         set_error(2, "cannot allocate %zu-element matrices", nn);
         return;
     }
-    if (cudaMemcpyAsync(c.d_dense_raw.p, c.dense_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
+    if (cudaMemcpyAsync(c.d_dense_raw.p, c.d_dense_up.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess ||
         cudaMemsetAsync(c.d_o_out.p, 0, nn * sizeof(double), c.stream) != cudaSuccess) {
         set_error(2, "upload of the density failed");
         return;
@@ -1820,10 +1852,12 @@ void gpu_getxc_(int* isg, double* sigrad2, double* Eelxc, double* aelec, double*
         return;
     }
     const int n = c.nbasis;
+    const std::vector<double>& oh = host_o(c);
+    if (g_status) return;
     for (int i = 0; i < n; i++)
         for (int j = i; j < n; j++) {
             const size_t lo = (size_t)j + (size_t)i * n;   // (j, i), j >= i
-            const double val = c.o_host[lo] + v[lo];
+            const double val = oh[lo] + v[lo];
             o[(size_t)i + (size_t)j * n] = val;
             o[lo] = val;
         }
@@ -2149,7 +2183,7 @@ void gpu_addint_(double* o, int* intindex, char* intFileName)
         return;
     }
     cudaMemsetAsync(G.p, 0, nn * sizeof(double), c.stream);
-    cudaMemcpyAsync(c.d_dense_raw.p, c.dense_host.data(), nn * sizeof(double), cudaMemcpyHostToDevice, c.stream);
+    cudaMemcpyAsync(c.d_dense_raw.p, c.d_dense_up.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, c.stream);
     const double hx = c.method == 0 ? 1.0 : (c.method == 1 ? 0.2 : 0.0);
     std::vector<int> A(kEriBlock), B(kEriBlock);
     std::vector<double> V(kEriBlock);
@@ -2179,7 +2213,9 @@ void gpu_addint_(double* o, int* intindex, char* intFileName)
         set_error(2, "gpu_addint_: download failed");
         return;
     }
-    for (size_t i = 0; i < nn; i++) o[i] = c.o_host[i] + g[i];
+    const std::vector<double>& oh = host_o(c);
+    if (g_status) return;
+    for (size_t i = 0; i < nn; i++) o[i] = oh[i] + g[i];
 }
 
 }  // extern "C"
