@@ -44,6 +44,9 @@ from quick_b200.scf import shell_cut_matrix  # noqa: E402
 WORKLOAD = dict(name="(H2O)32 6-31G** RHF Fock build", grid=(4, 4, 2), basis="6-31G**", seed=0,
                 integral_cutoff=1e-10, prim_limit=1e-20)
 # mixed-precision split: shell quartets whose Y_ab Y_cd DNMax bound is below this run in FP32
+# DRAM bytes (read + write) of the class kernels of one FP64 build of the
+# workload, from one ncu capture (cold caches): the roofline's traffic
+FOCK_BUILD_DRAM_BYTES = 27.1e9
 MIXED_CUT = 1e-3
 
 
@@ -428,7 +431,10 @@ def run_ours(args, ws, rank, local):
                 "h2d_bytes_per_step": int(2 * n * n * 8 + b.nshell ** 2 * 8),
                 "d2h_bytes_per_step": int(n * n * 8), "ms_per_step": e2e_ms},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "frac": achieved / peak if peak else None, "traffic": FOCK_BUILD_DRAM_BYTES,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the class "
+                                       "kernels of one FP64 build (cold caches), "
+                                       "profiles/fock_class_kernels_water32_631gss.md",
                      "kernel": "fock_class_kernel<LA,LB,LC,LD> (all classes of one build)",
                      "peak_source": "measured: FP64 FMA-chain probe run in this process (qb_fma_peak)",
                      "flops_per_step": alg_flops, "kernel_ms": mean_eri,
