@@ -121,6 +121,11 @@ struct Context {
     // gpu_upload_calculated_, on the device; the host copy of O is made when
     // a host-side path (gpu_getxc_, gpu_addint_) first needs it
     DevBuf<double> d_o_up, d_dense_up;
+    // gpu_schwarz_'s work arrays, kept between calls (grow only): a
+    // cudaMalloc / cudaFree pair per call took from milliseconds to a second
+    DevBuf<double4> sw_prim, sw_ab;
+    DevBuf<int4> sw_bf;
+    DevBuf<double> sw_oc, sw_op;
     std::vector<double> o_host;
     bool o_host_valid = false;
     bool have_calc = false;
@@ -1058,6 +1063,11 @@ void gpu_shutdown_(void)
     c.d_W1.release();
     c.d_o_up.release();
     c.d_dense_up.release();
+    c.sw_prim.release();
+    c.sw_ab.release();
+    c.sw_bf.release();
+    c.sw_oc.release();
+    c.sw_op.release();
     c.d_g1.release();
     c.d_shell_first.release();
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
@@ -1915,18 +1925,15 @@ int gpu_schwarz_(double* YCutoff, double* cutPrim)
         tend[e.type] = i + 1;
     }
     int nprimpair = (int)prim.size() / 3;
-    DevBuf<double4> d_prim, d_ab;
-    DevBuf<int4> d_bf;
-    DevBuf<double> d_oc, d_op;
-    CK(d_prim.alloc(prim.size()));
-    CK(d_ab.alloc(nrec));
-    CK(d_bf.alloc(nrec));
-    CK(d_oc.alloc(nrec));
-    CK(d_op.alloc(nprimpair));
-    CK(cudaMemcpy(d_prim.p, prim.data(), prim.size() * sizeof(double4), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_ab.p, pAB.data(), nrec * sizeof(double4), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_bf.p, pbf.data(), nrec * sizeof(int4), cudaMemcpyHostToDevice));
-    SchwarzParams S{d_prim.p, d_bf.p, d_ab.p, c.d_cons.p, c.d_boys.p, d_oc.p, d_op.p};
+    CK(c.sw_prim.alloc(prim.size()));
+    CK(c.sw_ab.alloc(nrec));
+    CK(c.sw_bf.alloc(nrec));
+    CK(c.sw_oc.alloc(nrec));
+    CK(c.sw_op.alloc(nprimpair));
+    CK(cudaMemcpyAsync(c.sw_prim.p, prim.data(), prim.size() * sizeof(double4), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.sw_ab.p, pAB.data(), nrec * sizeof(double4), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaMemcpyAsync(c.sw_bf.p, pbf.data(), nrec * sizeof(int4), cudaMemcpyHostToDevice, c.stream));
+    SchwarzParams S{c.sw_prim.p, c.sw_bf.p, c.sw_ab.p, c.d_cons.p, c.d_boys.p, c.sw_oc.p, c.sw_op.p};
     for (int t = 0; t < kNumPairTypes; t++) {
         if (tend[t] <= tbeg[t]) continue;
         int n = tend[t] - tbeg[t];
@@ -1943,10 +1950,9 @@ int gpu_schwarz_(double* YCutoff, double* cutPrim)
     }
     CK(cudaGetLastError());
     std::vector<double> oc(nrec), op(nprimpair);
-    CK(cudaMemcpyAsync(oc.data(), d_oc.p, nrec * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    CK(cudaMemcpyAsync(op.data(), d_op.p, nprimpair * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(oc.data(), c.sw_oc.p, nrec * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(op.data(), c.sw_op.p, nprimpair * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
-    d_prim.release(); d_ab.release(); d_bf.release(); d_oc.release(); d_op.release();
     int ns = c.nshell;
     std::vector<double> ymax((size_t)ns * ns, 0.0), pmax((size_t)c.jbasis * c.jbasis, 0.0);
     for (int i = 0; i < nrec; i++) {
