@@ -65,6 +65,7 @@ class SCFResult:
     seconds: float = 0.0
     fock_builds: int = 0
     timings: dict = field(default_factory=dict)   # wall seconds per phase (run_rhf_device)
+    graph_timings: dict = field(default_factory=dict)   # graph SCF: wall seconds of its steps
 
     @property
     def W(self):
@@ -420,6 +421,7 @@ class DeviceRHF:
         n = S.shape[0]
         m = X.shape[1]
         opts = self.opts
+        gt = {"orthogonaliser": time.perf_counter() - t_start}
         D = torch.as_tensor(np.ascontiguousarray(D0), **opts).clone()
         D_built = torch.zeros_like(D)
         dIn = torch.zeros_like(D)
@@ -472,6 +474,7 @@ class DeviceRHF:
         graphs = {}
         if not converged:
             torch.cuda.synchronize()
+            t_cap = time.perf_counter()
             for incr in ((False, True) if incremental else (False,)):
                 g = torch.cuda.CUDAGraph()
                 pool = graphs[False].pool() if graphs else None
@@ -479,6 +482,7 @@ class DeviceRHF:
                     step(incr)
                 self.nfock -= 1          # captured, not built
                 graphs[incr] = g
+            gt["capture"] = time.perf_counter() - t_cap
             for it in range(2, max_iter + 1):
                 t0 = time.perf_counter()
                 graphs[incremental and (it - 1) % rebuild_every != 0].replay()
@@ -489,14 +493,20 @@ class DeviceRHF:
                     converged = True
                     break
         e_elec = float(vals[0])
+        t_fin = time.perf_counter()
         eps, Cp = torch.linalg.eigh(Xt @ F2 @ X)
         Cm = X @ Cp
         self.D_dev, self.C_dev, self.eps_dev = D_built.clone(), Cm, eps
         torch.cuda.synchronize()
+        gt["final_eigh"] = time.perf_counter() - t_fin
+        t_rel = time.perf_counter()
         graphs.clear()
-        return SCFResult(energy=e_elec + enuc, e_elec=e_elec, e_nuc=enuc, converged=converged, iterations=it,
-                         D=D_built.cpu().numpy(), C=Cm.cpu().numpy(), eps=eps.cpu().numpy(), nocc=nocc,
-                         history=history, seconds=time.perf_counter() - t_start)
+        gt["release"] = time.perf_counter() - t_rel
+        res = SCFResult(energy=e_elec + enuc, e_elec=e_elec, e_nuc=enuc, converged=converged, iterations=it,
+                        D=D_built.cpu().numpy(), C=Cm.cpu().numpy(), eps=eps.cpu().numpy(), nocc=nocc,
+                        history=history, seconds=time.perf_counter() - t_start)
+        res.graph_timings = {k: round(v, 4) for k, v in gt.items()}
+        return res
 
     def _run(self, nocc, D0, conv, max_iter, diis_size, incremental, rebuild_every):
         torch = self.torch
