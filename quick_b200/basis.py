@@ -14,6 +14,7 @@ package's C ABI or the reference's own.
 Array shapes follow the Fortran declarations; every 2-D array is stored
 column-major (``order='F'``) exactly as the Fortran caller passes it.
 """
+import copy
 import json
 import math
 import os
@@ -131,12 +132,27 @@ class Basis:
         return int(self.Qfinal.max())
 
 
+_BASIS_CACHE = {}
+
+
 def build_basis(atoms, basis_name):
     """Build QUICK's basis arrays for ``atoms`` (list of element symbols).
 
     Follows readbasis' second pass (src/basis.f90:376-757) shell by shell and
-    its post-processing (src/basis.f90:797-897).
+    its post-processing (src/basis.f90:797-897).  The arrays depend only on
+    the element list and the basis name: each distinct (elements, basis) is
+    built once per process and later calls get their own copy.
     """
+    key = (tuple(a.upper() for a in atoms), basis_name)
+    if key not in _BASIS_CACHE:
+        if len(_BASIS_CACHE) > 256:
+            _BASIS_CACHE.clear()
+        _BASIS_CACHE[key] = _build_basis(atoms, basis_name)
+    return copy.deepcopy(_BASIS_CACHE[key])
+
+
+def _build_basis(atoms, basis_name):
+    """build_basis without the cache."""
     data = _basis_data()[basis_name]
     atoms = [a.upper() for a in atoms]
     natom = len(atoms)

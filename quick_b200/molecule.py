@@ -43,13 +43,11 @@ class Molecule:
         return int(self.atomic_numbers.sum()) - self.charge
 
     def nuclear_repulsion(self):
+        """sum_{i<j} Z_i Z_j / |R_i - R_j|."""
         z = self.atomic_numbers.astype(np.float64)
         x = self.xyz_bohr.T
-        e = 0.0
-        for i in range(self.natom):
-            for j in range(i):
-                e += z[i] * z[j] / np.linalg.norm(x[i] - x[j])
-        return e
+        i, j = np.tril_indices(self.natom, -1)
+        return float(np.sum(z[i] * z[j] / np.linalg.norm(x[i] - x[j], axis=1)))
 
 
 def _random_rotation(rng):

@@ -754,13 +754,20 @@ def run_batch_rhf(mols, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
             for i, n in enumerate(ns):
                 real[i, :n] = True
             pad = (~real).to(torch.float64)
-            # symmetric orthogonalisers, identity on the padding
+            # Cholesky orthogonalisers X = L^-T (S = L L^T, X^T S X = 1),
+            # identity on the padding: one batched factorisation and
+            # triangular solve instead of a batched eigh (0.8 s for 256
+            # molecules); the converged densities do not depend on the
+            # choice.  A pivot L_ii^2 bounds the smallest eigenvalue of S from
+            # above, so a pivot below 1e-4 means a near-linear dependence,
+            # which this driver does not remove (run_rhf_device does).
             Sid = S + torch.diag_embed(pad)
-            sv, U = torch.linalg.eigh(Sid)
-            if bool((sv < 1e-4).any()):
-                raise QuickB200Error(1, "run_batch_rhf: an overlap eigenvalue below 1e-4 (use run_rhf_device)")
-            X = U @ torch.diag_embed(sv.rsqrt()) @ U.transpose(1, 2)
-            Xt = X.transpose(1, 2)
+            Lc, info = torch.linalg.cholesky_ex(Sid)
+            if bool((info != 0).any()) or bool((Lc.diagonal(dim1=1, dim2=2).square() < 1e-4).any()):
+                raise QuickB200Error(1, "run_batch_rhf: the overlap is near-singular (use run_rhf_device)")
+            eye = torch.eye(nmax, **opts).expand(nmol, nmax, nmax)
+            Xt = torch.linalg.solve_triangular(Lc, eye, upper=False).contiguous()
+            X = Xt.transpose(1, 2)
             Hp = pack(H)
             enuc = torch.tensor([m.nuclear_repulsion() for m in mols], **opts)
             nel = torch.tensor(ns, **opts) ** 2
@@ -837,11 +844,10 @@ def run_batch_rhf(mols, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
             if gradient:
                 g2 = torch.zeros(3 * int(na_.sum()), **opts)
                 rc(L.qb_batch_grad_device(p(Dbuilt), p(g2)))
-                # W = 2 sum_occ e_k C_k C_k^T from the last Fock matrix
-                eps, Cp = torch.linalg.eigh(Xt @ F @ X + torch.diag_embed(pad * 1e6))
-                Cm = X @ Cp
-                occ = (torch.arange(nmax, device=dev)[None, :] < nocc[:, None]).to(torch.float64)
-                W = 2.0 * (Cm * (occ * eps)[:, None, :]) @ Cm.transpose(1, 2)
+                # W = 2 sum_occ e_k C_k C_k^T = D F D / 2 for the converged
+                # closed-shell density (D = 2 C_occ C_occ^T, F C = S C e):
+                # two batched products instead of a batched eigh
+                W = 0.5 * (Dfin @ F @ Dfin)
                 g2h = g2.cpu().numpy()
                 grads = []
                 a0 = 0
