@@ -532,8 +532,11 @@ static int build_tables(Context& c)
     for (int k = 0; k < kNumClasses; k++) {
         double est = type_prims[pair_type_index(kClassL[k][0], kClassL[k][1])] *
                      type_prims[pair_type_index(kClassL[k][2], kClassL[k][3])] / div;
+        // at most 2 lanes before tuning: qb_autotune_classes on
+        // (H2O)32/6-31G** picks 1 or 2 lanes for every class (4 for two FP32
+        // light classes), and 8 lanes ran psss 1.8x slower than 2
         int g = 1;
-        while (g * 2 <= est && g < 32) g *= 2;
+        while (g * 2 <= est && g < 2) g *= 2;
         if (gf && atoi(gf) > 0) g = atoi(gf);   // QB_FOCK_G forces one value
         c.class_group[k] = std::min(g, class_max_group(k));
     }
