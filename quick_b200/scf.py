@@ -848,17 +848,22 @@ def run_batch_rhf(mols, basis_name, integral_cutoff=1e-10, prim_limit=1e-20, con
                 # closed-shell density (D = 2 C_occ C_occ^T, F C = S C e):
                 # two batched products instead of a batched eigh
                 W = 0.5 * (Dfin @ F @ Dfin)
-                g2h = g2.cpu().numpy()
-                grads = []
+                # one-electron terms per molecule into one device vector (the
+                # molecules' atoms in order, like g2), read back once
+                g1 = torch.zeros_like(g2)
                 a0 = 0
                 for i, (m, b) in enumerate(zip(mols, bases)):
                     n = b.nbasis
                     s.upload_molecule(m, b, pairs=False)
-                    gi = torch.zeros(3 * m.natom, **opts)
                     Di = Dfin[i, :n, :n].contiguous()
                     Wi = W[i, :n, :n].contiguous()
-                    rc(L.qb_grad1e_device(p(Di), p(Wi), p(gi)))
-                    grads.append(gi.cpu().numpy() + g2h[3 * a0:3 * (a0 + m.natom)])
+                    rc(L.qb_grad1e_device(p(Di), p(Wi), p(g1[3 * a0:3 * (a0 + m.natom)])))
+                    a0 += m.natom
+                gh = (g1 + g2).cpu().numpy()
+                grads = []
+                a0 = 0
+                for m in mols:
+                    grads.append(gh[3 * a0:3 * (a0 + m.natom)].copy())
                     a0 += m.natom
             torch.cuda.synchronize()
             timings["gradient"] = time.perf_counter() - t2
