@@ -81,9 +81,9 @@ void gpu_cleanup_(void);
    with |(ij|kl)| > maxIntegralCutoff to intFileName (blank-terminated, as Fortran passes it) in
    QUICK's format: blocks of 150000 records written as int IJ[], int KL[], double value[] (the
    last block short), IJ = i nbasis + j, KL = k nbasis + l, 0-based, i <= j, k <= l,
-   (i, j) <= (k, l), cons-scaled values.  intNum += the number written.  s, p and d shells only
-   (a basis with f shells is rejected).  Replaces the density screen, so gpu_upload_cutoff_
-   must precede the next two-electron build. */
+   (i, j) <= (k, l), cons-scaled values.  intNum += the number written.  s, p, d and f shells.
+   Replaces the density screen, so gpu_upload_cutoff_ must precede the next two-electron
+   build. */
 void gpu_aoint_(double* leastIntegralCutoff, double* maxIntegralCutoff, int* intNum, char* intFileName);
 /* src/cuda/gpu.cu:1559-1801: o <- symmetric (O as uploaded + J - (h/2) K) from the intindex
    stored integrals of intFileName and the density of the last gpu_upload_calculated_ (h from

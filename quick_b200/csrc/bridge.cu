@@ -2077,10 +2077,6 @@ void gpu_aoint_(double* leastIntegralCutoff, double* maxIntegralCutoff, int* int
 {
     Context& c = ctx();
     if (require(c.have_pairs, "gpu_upload_cutoff_matrix_ must precede gpu_aoint_")) return;
-    if (c.maxL > 2) {
-        set_error(23, "gpu_aoint_: the stored-integral path covers s, p and d shells (this basis has f)");
-        return;
-    }
     const std::string fname = fortran_name(intFileName);
     FILE* f = fopen(fname.c_str(), "wb");
     if (!f) {
@@ -2139,9 +2135,16 @@ void gpu_aoint_(double* leastIntegralCutoff, double* maxIntegralCutoff, int* int
             AoIntOut O{rec.p, dcount.p, cap, *maxIntegralCutoff, c.d_cons.p, c.nbasis, q0,
                        std::min<long long>(q0 + slice, cnt[k])};
             cudaMemsetAsync(dcount.p, 0, sizeof(unsigned long long), c.stream);
-            qb::g_aoint_out = &O;
-            launch_class(k, P, -1, (int)(O.qend - O.qbegin), c.nsm, c.stream);
-            qb::g_aoint_out = nullptr;
+            const bool gen = kClassGeneric[k] || Lk[0] + Lk[1] + Lk[2] + Lk[3] >= c.generic_min_l;
+            if (gen) {
+                // the classes without straight-line kernels: the block-per-quartet store
+                if (launch_generic_store(k, Lk[0], Lk[1], Lk[2], Lk[3], P, O, c.nsm, c.stream) < 0)
+                    return fail("a class needs more shared memory than this GPU offers");
+            } else {
+                qb::g_aoint_out = &O;
+                launch_class(k, P, -1, (int)(O.qend - O.qbegin), c.nsm, c.stream);
+                qb::g_aoint_out = nullptr;
+            }
             unsigned long long m = 0;
             if (cudaMemcpyAsync(&m, dcount.p, sizeof m, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
                 cudaStreamSynchronize(c.stream) != cudaSuccess)

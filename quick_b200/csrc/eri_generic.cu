@@ -351,16 +351,17 @@ __device__ void generic_quartet(const QuartetCtx& q, const FockParams& P, const 
 // integral into I) and the Coulomb/exchange contraction into six
 // shared-memory blocks, flushed once per quartet with the weights of
 // digest_coulomb / digest_exchange.
-__device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const GenLayout& G, const GenProgram& R,
-                               double* sm, int tid, int nt)
+// The horizontal recurrence of the quartet (its contracted [e0|f0] in acc):
+// the ket side into X, then the quartet's integrals I[ab][cd] (component
+// order of the basis functions) at G.i_off.  Ends with a barrier.
+__device__ void generic_transfer(const QuartetCtx& q, const GenLayout& G, const GenProgram& R, double* sm, int tid,
+                                 int nt)
 {
     const int na = g_ncart(G.la), nb = g_ncart(G.lb), nc = g_ncart(G.lc), nd = g_ncart(G.ld);
     const int ncd = nc * nd;
     const double* acc = sm + G.acc_off;
     double* X = sm + G.x_off;
     double* pw = sm + G.pw_off;
-    double* Db = sm + G.d_off;
-    double* Jb = sm + G.j_off;
     if (tid < 24) {
         const double AB[3] = {q.ABx, q.ABy, q.ABz}, CD[3] = {q.CDx, q.CDy, q.CDz};
         const double base = tid < 12 ? AB[tid / 4] : CD[(tid - 12) / 4];
@@ -368,6 +369,40 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         for (int k = 0; k < (tid & 3); k++) v *= base;
         pw[tid] = v;
     }
+    __syncthreads();
+    // ket side: X[e][cd] = sum_k C * CD^pw * acc[e][f]
+    for (int t = tid; t < G.ne * ncd; t += nt) {
+        const int e = t / ncd, cd = t - e * ncd;
+        double v = 0.0;
+        for (int j = R.kstart[cd]; j < R.kstart[cd + 1]; j++) {
+            const int4 k = R.kterm[j];
+            v += k.z * pw[12 + (k.y & 15)] * pw[16 + ((k.y >> 4) & 15)] * pw[20 + (k.y >> 8)] * acc[e * G.nf + k.x];
+        }
+        X[t] = v;
+    }
+    __syncthreads();
+    const int nab = na * nb, nout = nab * ncd;
+    // the quartet's integrals I[ab][cd] (bra side of the horizontal recurrence)
+    double* I = sm + G.i_off;
+    for (int o = tid; o < nout; o += nt) {
+        const int ab = o / ncd, cd = o - ab * ncd;
+        double v = 0.0;
+        for (int j = R.bstart[ab]; j < R.bstart[ab + 1]; j++) {
+            const int4 k = R.bterm[j];
+            v += k.z * pw[k.y & 15] * pw[4 + ((k.y >> 4) & 15)] * pw[8 + (k.y >> 8)] * X[k.x * ncd + cd];
+        }
+        I[o] = v;
+    }
+    __syncthreads();
+}
+
+__device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const GenLayout& G, const GenProgram& R,
+                               double* sm, int tid, int nt)
+{
+    const int na = g_ncart(G.la), nb = g_ncart(G.lb), nc = g_ncart(G.lc), nd = g_ncart(G.ld);
+    const int ncd = nc * nd;
+    double* Db = sm + G.d_off;
+    double* Jb = sm + G.j_off;
     const int o_ab = 0, o_cd = o_ab + na * nb, o_ac = o_cd + nc * nd, o_ad = o_ac + na * nc, o_bc = o_ad + na * nd,
               o_bd = o_bc + nb * nc, nblk = o_bd + nb * nd;
     const double* Dm = P.dense;
@@ -384,32 +419,10 @@ __device__ void generic_digest(const QuartetCtx& q, const FockParams& P, const G
         Db[t] = __ldg(Dm + (size_t)r * n + c);
         Jb[t] = 0.0;
     }
-    __syncthreads();
-    // ket side: X[e][cd] = sum_k C * CD^pw * acc[e][f]
-    for (int t = tid; t < G.ne * ncd; t += nt) {
-        const int e = t / ncd, cd = t - e * ncd;
-        double v = 0.0;
-        for (int j = R.kstart[cd]; j < R.kstart[cd + 1]; j++) {
-            const int4 k = R.kterm[j];
-            v += k.z * pw[12 + (k.y & 15)] * pw[16 + ((k.y >> 4) & 15)] * pw[20 + (k.y >> 8)] * acc[e * G.nf + k.x];
-        }
-        X[t] = v;
-    }
-    __syncthreads();
+    generic_transfer(q, G, R, sm, tid, nt);   // its first barrier covers the density blocks
     const bool exch = P.hybrid != 0.0;
-    const int nab = na * nb, nout = nab * ncd;
-    // the quartet's integrals I[ab][cd] (bra side of the horizontal recurrence)
-    double* I = sm + G.i_off;
-    for (int o = tid; o < nout; o += nt) {
-        const int ab = o / ncd, cd = o - ab * ncd;
-        double v = 0.0;
-        for (int j = R.bstart[ab]; j < R.bstart[ab + 1]; j++) {
-            const int4 k = R.bterm[j];
-            v += k.z * pw[k.y & 15] * pw[4 + ((k.y >> 4) & 15)] * pw[8 + (k.y >> 8)] * X[k.x * ncd + cd];
-        }
-        I[o] = v;
-    }
-    __syncthreads();
+    const int nab = na * nb;
+    const double* I = sm + G.i_off;
     // contraction with the density, one thread per output element of each of
     // the six blocks (no atomics): J_ab = sum_cd D_cd I, J_cd = sum_ab D_ab I,
     // K_ac = sum_bd D_bd I, K_ad = sum_bc D_bc I, K_bc = sum_ad D_ad I,
@@ -474,6 +487,33 @@ __global__ void __launch_bounds__(256) fock_generic_kernel(const FockParams P, i
         load_quartet(P, list[i], true, q);
         generic_quartet(q, P, G, R, sm, tid, nt);
         generic_digest(q, P, G, R, sm, tid, nt);
+    }
+}
+
+// gpu_aoint_'s counterpart for these classes: the integrals of quartets
+// [O.qbegin, O.qend) of the class list, each kept once (aoint_emit), instead
+// of their digestion.
+__global__ void __launch_bounds__(256) aoint_generic_kernel(const FockParams P, int cls, const GenLayout G,
+                                                           const GenProgram R, const AoIntOut O)
+{
+    extern __shared__ double sm[];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int n = P.class_count[cls];
+    const Quartet* list = P.quartets + P.class_offset[cls];
+    const long long end = O.qend < n ? O.qend : n;
+    const int nb = g_ncart(G.lb), nc = g_ncart(G.lc), nd = g_ncart(G.ld), ncd = nc * nd;
+    const int nout = g_ncart(G.la) * nb * ncd;
+    for (long long i = O.qbegin + blockIdx.x; i < end; i += gridDim.x) {
+        QuartetCtx q;
+        load_quartet(P, list[i], true, q);
+        generic_quartet(q, P, G, R, sm, tid, nt);
+        generic_transfer(q, G, R, sm, tid, nt);
+        const double* I = sm + G.i_off;
+        for (int o = tid; o < nout; o += nt) {
+            const int ab = o / ncd, cd = o - ab * ncd;
+            aoint_emit(O, q, q.bfA + ab / nb, q.bfB + ab % nb, q.bfC + cd / nd, q.bfD + cd % nd, I[o]);
+        }
+        __syncthreads();
     }
 }
 
@@ -695,6 +735,31 @@ int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockPara
     size_t bytes = 0;
     if (generic_launch_shape(gc->G, nq, nsm, &nt, &bytes, &grid)) return -1;
     QB_LAUNCH(fock_generic_kernel, grid, nt, bytes, st, P, cls, gc->G, gc->R, fp32_list);
+    return nt;
+}
+
+// The stored-integral kernel of a generic class over the slice of O.
+int launch_generic_store(int cls, int la, int lb, int lc, int ld, const FockParams& P, const AoIntOut& O, int nsm,
+                         cudaStream_t st)
+{
+    const long long nq = O.qend - O.qbegin;
+    if (nq <= 0) return 0;
+    const GenCached* gc = gen_cached(la, lb, lc, ld);
+    if (!gc) return -1;
+    int nt = 0, grid = 0;
+    size_t bytes = 0;
+    if (generic_launch_shape(gc->G, (int)std::min<long long>(nq, 1 << 30), nsm, &nt, &bytes, &grid)) return -1;
+    int dev = 0, maxsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    static int configured = 0;
+    if (bytes > 48 * 1024 && configured < maxsm) {
+        if (cudaFuncSetAttribute(aoint_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm) !=
+            cudaSuccess)
+            return -1;
+        configured = maxsm;
+    }
+    QB_LAUNCH(aoint_generic_kernel, grid, nt, bytes, st, P, cls, gc->G, gc->R, O);
     return nt;
 }
 

@@ -80,6 +80,9 @@ int class_variants(int cls, int fp32, int* codes, int cap);
 // The warp-per-quartet kernel of eri_generic.cu for any class (shells <= f);
 // fp32_list: walk the class's FP32 list.  Returns -1 if the class needs more
 // shared memory than the GPU offers.
+struct AoIntOut;
+int launch_generic_store(int cls, int la, int lb, int lc, int ld, const FockParams& P, const AoIntOut& O, int nsm,
+                         cudaStream_t st);
 int launch_generic_class(int cls, int la, int lb, int lc, int ld, const FockParams& P, int nq, int nsm, int fp32_list,
                          cudaStream_t st);
 // Device bytes of the generic kernel's program of class (la lb|lc ld), and
