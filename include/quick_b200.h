@@ -65,6 +65,10 @@ void gpu_upload_cutoff_(double* cutMatrix, double* integralCutoff, double* primL
 void gpu_get2e_(double* o);
 /* src/cuda/gpu.cu:1393-1444: grad(3 natom) accumulates, gradCutoff */
 void gpu_upload_grad_(double* grad, double* gradCutoff);
+
+/* Declared in QUICK's src/cuda/gpu.h:31 and defined nowhere in QUICK (no caller): kept for a
+   complete drop-in; stores the energy, which nothing here reads. */
+void gpu_upload_energy_(double* E);
 /* src/cuda/gpu.cu:1481-1551: grad <- grad + two-electron gradient */
 void gpu_grad_(double* grad);
 /* src/cuda/gpu.cu:1866-1975: XC quadrature on QUICK's SG1 grid for the method of the last

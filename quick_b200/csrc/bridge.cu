@@ -134,6 +134,7 @@ struct Context {
     bool have_cutoff = false;
     std::vector<double> grad_host;
     bool have_grad = false;
+    double uploaded_energy = 0.0;        // gpu_upload_energy_ (no reader)
     // stats
     long long last_quartets = 0, last_quartets32 = 0;
     long long last_grad_quartets = 0;
@@ -1785,6 +1786,11 @@ void gpu_cleanup_(void)
     if (!g) return;
     Context& c = *g;
     c.have_basis = c.have_pairs = c.have_calc = c.have_cutoff = false;
+}
+
+void gpu_upload_energy_(double* E)
+{
+    ctx().uploaded_energy = E ? *E : 0.0;
 }
 
 void gpu_upload_grad_(double* grad, double* gradCutoff)
