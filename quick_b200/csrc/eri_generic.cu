@@ -833,7 +833,16 @@ __device__ __forceinline__ int gen_gidx(int x, int y, int z, int lo)
     return g_ncum(n - 1) - g_ncum(lo - 1) + t * (t + 1) / 2 + z;
 }
 
-__constant__ int kBinomD[6][6] = {{1}, {1, 1}, {1, 2, 1}, {1, 3, 3, 1}, {1, 4, 6, 4, 1}, {1, 5, 10, 10, 5, 1}};
+// C(n, k) for 0 <= k <= n <= 5 from two immediates (rows packed 4 bits per
+// entry, entry n(n+1)/2 + k): the lanes of a warp ask for different entries,
+// which a __constant__ table would serve one address at a time.
+__device__ __forceinline__ int binom5(int n, int k)
+{
+    constexpr unsigned long long lo = 0x146411331121111ull;   // entries 0..14
+    constexpr unsigned long long hi = 0x15aa51ull;              // entries 15..20
+    const int idx = n * (n + 1) / 2 + k;
+    return idx < 15 ? (int)((lo >> (4 * idx)) & 15ull) : (int)((hi >> (4 * (idx - 15))) & 15ull);
+}
 
 // canonical index of (x, y, z) inside its shell, and back
 __device__ __forceinline__ int gen_canon(int y, int z) { const int t = y + z; return t * (t + 1) / 2 + z; }
@@ -862,7 +871,7 @@ __device__ void gen_ket_transform(const double* E, double* X, const GenGradInfo&
         for (int kx = 0; kx <= d[0]; kx++)
             for (int ky = 0; ky <= d[1]; ky++)
                 for (int kz = 0; kz <= d[2]; kz++)
-                    v += kBinomD[d[0]][kx] * kBinomD[d[1]][ky] * kBinomD[d[2]][kz] * CDp[d[0] - kx] *
+                    v += binom5(d[0], kx) * binom5(d[1], ky) * binom5(d[2], kz) * CDp[d[0] - kx] *
                          CDp[8 + d[1] - ky] * CDp[16 + d[2] - kz] * Er[gen_gidx(c[0] + kx, c[1] + ky, c[2] + kz, I.flo)];
         X[t] = v;
     }
@@ -876,7 +885,7 @@ __device__ __forceinline__ double gen_bra_sum(const double* X, int cols, int col
     for (int kx = 0; kx <= b[0]; kx++)
         for (int ky = 0; ky <= b[1]; ky++)
             for (int kz = 0; kz <= b[2]; kz++)
-                s += kBinomD[b[0]][kx] * kBinomD[b[1]][ky] * kBinomD[b[2]][kz] * ABp[b[0] - kx] * ABp[8 + b[1] - ky] *
+                s += binom5(b[0], kx) * binom5(b[1], ky) * binom5(b[2], kz) * ABp[b[0] - kx] * ABp[8 + b[1] - ky] *
                      ABp[16 + b[2] - kz] * X[(size_t)gen_gidx(a[0] + kx, a[1] + ky, a[2] + kz, I.elo) * cols + col];
     return s;
 }
@@ -908,6 +917,10 @@ __global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, c
     double* Eb = Ea + nacc;
     double* Ec = Eb + nacc;
     __shared__ double red[9][4];
+    // QUICK's Cartesian orders in shared memory: the lanes of a warp read
+    // different entries, which a __constant__ table serves one at a time
+    __shared__ int sCart[4 * 10 * 3];
+    for (int i = tid; i < 4 * 10 * 3; i += nt) sCart[i] = (&kQuickCartD[0][0][0])[i];
     const int na = g_ncart(I.la), nb = g_ncart(I.lb), nc = g_ncart(I.lc), nd = g_ncart(I.ld);
     const int n = I.fp32_list ? P.class_count32[cls] : P.class_count[cls];
     const Quartet* list = I.fp32_list ? P.quartets + (P.class_end[cls] - n) : P.quartets + P.class_offset[cls];
@@ -1030,10 +1043,10 @@ __global__ void __launch_bounds__(128) grad_generic_kernel(const FockParams P, c
             const int ia = r;
             int a[3], b[3], c[3], d[3];
             for (int k = 0; k < 3; k++) {
-                a[k] = kQuickCartD[I.la][ia][k];
-                b[k] = kQuickCartD[I.lb][ibb][k];
-                c[k] = kQuickCartD[I.lc][ic][k];
-                d[k] = kQuickCartD[I.ld][id][k];
+                a[k] = sCart[(I.la * 10 + ia) * 3 + k];
+                b[k] = sCart[(I.lb * 10 + ibb) * 3 + k];
+                c[k] = sCart[(I.lc * 10 + ic) * 3 + k];
+                d[k] = sCart[(I.ld * 10 + id) * 3 + k];
             }
             const int fa = q.bfA + ia, fb = q.bfB + ibb, fc = q.bfC + ic, fd = q.bfD + id;
             const double Dab = __ldg(Dm + (size_t)fa * nbf + fb), Dcd = __ldg(Dm + (size_t)fc * nbf + fd);
