@@ -19,8 +19,9 @@ entry points (e2e), replayed from a CUDA graph, and with the mixed FP32/FP64
 split; the two-electron gradient; the XC quadrature (xc); SCF + gradient
 seconds per molecule, all-FP64 and mixed, with full and delta-D Fock builds,
 plus a Kohn-Sham and a cc-pVTZ case (scf); molecules per second for many
-small clusters (batch); and the CPU baseline, QUICK's own kernel compiled for
-the host cores.
+small clusters (batch); the CPU baseline, QUICK's own kernel compiled for
+the host cores; and reference_gpu, QUICK's own CUDA built for sm_100a and
+run on the same GPU on the same workload (in a process of its own).
 """
 import argparse
 import gc
@@ -179,6 +180,51 @@ def cpu_reference(threads, steps=1, warmup=0):
     assert len(counts) == 1, counts
     raw, nq = counts.pop()
     return nq / np.mean(ts), nq, float(np.mean(ts)), raw
+
+
+def gpu_reference(steps, warmup, device=0):
+    """QUICK's own GPU path on this GPU: src/cuda/gpu.cu, gpu_type.cu,
+    gpu_get2e.cu and gpu_getxc.cu built unchanged by nvcc for sm_100a with
+    QUICK's flags and configuration (oracle/_ref/gpu, build_ref.py --gpu),
+    driven through QUICK's gpu_init_ / gpu_upload_* / gpu_get2e_ sequence on
+    the same (H2O)32 workload.  A step is QUICK's per-iteration sequence
+    (src/hfoperator.f90:76-98): gpu_upload_method_, gpu_upload_calculated_
+    (host O and D), gpu_upload_cutoff_ (cutMatrix), gpu_get2e_ (its kernel,
+    the download of the fixed-point O and the conversion on the host),
+    timed by wall clock (the bridge returns only after its download); the
+    kernel's own time is QUICK's CUDA-event timer around its launch.  The
+    shell-quartet count is QUICK's own walk on the same inputs (the config-1
+    fixture, counted by QUICK's kernel on the host).  Warm-up steps run the
+    same workload.  Loads nothing from quick_b200's library."""
+    import oracle
+    from quick_b200.basis import build_basis
+    from quick_b200.molecule import water_cluster
+    cut, plim = WORKLOAD["integral_cutoff"], WORKLOAD["prim_limit"]
+    m = water_cluster(WORKLOAD["grid"], seed=WORKLOAD["seed"])
+    b = build_basis(m.symbols, WORKLOAD["basis"])
+    Y, cp = oracle.schwarz(b, m.xyz_bohr)
+    keep = oracle.ref_upload_molecule(m, b, Y, cp, spdf="gpu", device=device)  # noqa: F841
+    D = model_density(m, b, seed=WORKLOAD["seed"])
+    cm = shell_cut_matrix(b, D)
+    for _ in range(warmup):
+        oracle.ref_get2e_gpu_timed(np.zeros_like(D), D, cm, cut, plim)
+    walls, kerns = [], []
+    for _ in range(steps):
+        O, wall, kern = oracle.ref_get2e_gpu_timed(np.zeros_like(D), D, cm, cut, plim)
+        walls.append(wall)
+        kerns.append(kern)
+    z = np.load(os.path.join(ROOT, "tests", "golden", "config1_water32_631gss.npz"))
+    nq = int(z["unique_quartets"])
+    par = quick_parity(np.ascontiguousarray(O.T), nq, b.nbasis) or {}
+    wall, kern = float(np.mean(walls)), float(np.mean(kerns))
+    return {"value": nq / wall, "unit": "quartets/s", "ms_per_step": wall * 1e3,
+            "kernel_ms": kern, "kernel_quartets_per_s": nq / (kern * 1e-3), "quartets_per_step": nq,
+            "steps": steps, "warmup": warmup,
+            "max_abs_dF_vs_quick_host_sampled": par.get("max_abs_dF_sampled"),
+            "what": "QUICK's own CUDA (gpu.cu bridge + get2e_kernel, spd build, -O3 -use_fast_math, QUICK's "
+                    "config.cuda.h) built unchanged for sm_100a and run on this GPU on %s; value: the whole "
+                    "gpu_upload_calculated_/gpu_upload_cutoff_/gpu_get2e_ sequence from host buffers (its e2e), "
+                    "kernel_ms: QUICK's own CUDA-event timer around get2e_kernel" % WORKLOAD["name"]}
 
 
 def quick_parity(G, quartets, n):
@@ -750,11 +796,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--classes", action="store_true", help="add per-class quartet counts")
     ap.add_argument("--batch", type=int, default=256, help="molecules in the batch line")
-    ap.add_argument("--part", default="all", choices=["all", "fock", "xc", "scf", "batch"],
+    ap.add_argument("--part", default="all", choices=["all", "fock", "xc", "scf", "batch", "quick-gpu"],
                     help="fock: the Fock build line only; xc: the XC quadrature line only; "
-                         "scf: the SCF+gradient line only; batch: the many-small-molecules line only")
+                         "scf: the SCF+gradient line only; batch: the many-small-molecules line only; "
+                         "quick-gpu (with --impl reference): QUICK's own GPU path on the Fock-build workload")
+    ap.add_argument("--no-quick-gpu", action="store_true", help="skip the reference_gpu object")
     args = ap.parse_args()
     threads = os.cpu_count() or 1
+    if args.impl == "reference" and args.part == "quick-gpu":
+        # QUICK's own GPU path only (run by the default line in a process of its own)
+        print(json.dumps(gpu_reference(args.steps, args.warmup, int(os.environ.get("LOCAL_RANK", "0")))))
+        return
     if args.impl == "reference":
         # QUICK's own kernel on the host cores; under torchrun rank 0 alone
         # runs it and the other ranks exit without work (no process group)
@@ -772,6 +824,11 @@ def main():
                    "cpu_baseline": {"value": qps, "unit": "quartets/s", "cores": threads, "kind": "reference",
                                     "sample": sample},
                    "e2e": {"value": qps, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            import torch
+            if torch.cuda.is_available() and not args.no_quick_gpu:
+                # QUICK's own CUDA path on the same box's GPU, beside its host-core run
+                out["reference_gpu"] = quick_gpu_subprocess(max(3, min(args.steps, 10)), 2,
+                                                            int(os.environ.get("LOCAL_RANK", "0")))
             print(json.dumps(out))
         return
     ws, rank, local = dist_setup()
@@ -795,11 +852,35 @@ def main():
                                          "gpu_get2e_subs.h kernel and gpu.cu bridge compiled for the host cores"
                                          % (WORKLOAD["name"], nq, sec),
                                "quartets_equal_gpu_count": nq == out["config"]["quartets_per_step"]}
+    if rank == 0 and not args.no_quick_gpu:
+        out["reference_gpu"] = quick_gpu_subprocess(max(3, min(args.steps, 10)), 2, local)
+        if "value" in out["reference_gpu"]:
+            rg = out["reference_gpu"]
+            rg["e2e_speedup_of_this_build"] = out["e2e"]["value"] / rg["value"]
+            rg["kernel_speedup_of_this_build"] = out["value"] / rg["kernel_quartets_per_s"]
     if rank == 0:
         print(json.dumps(out))
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def quick_gpu_subprocess(steps, warmup, device):
+    """gpu_reference in a process of its own (QUICK's library never shares
+    a process with this package's): its JSON object, or the reason it is
+    missing."""
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "gpu", "libquickref.so")):
+        return {"unavailable": "QUICK's GPU build (oracle/_ref/gpu) was not built"}
+    env = dict(os.environ, LOCAL_RANK=str(device))
+    for k in ("RANK", "WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--part",
+                        "quick-gpu", "--steps", str(steps), "--warmup", str(warmup)],
+                       capture_output=True, text=True, env=env, timeout=900)
+    for line in reversed(p.stdout.splitlines()):
+        if line.startswith("{"):
+            return json.loads(line)
+    return {"unavailable": "QUICK's GPU path exited %d: %s" % (p.returncode, (p.stderr or p.stdout)[-300:])}
 
 
 if __name__ == "__main__":

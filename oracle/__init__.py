@@ -9,7 +9,10 @@ Two checkers live here:
   * ``libquickref.so`` (build_ref.py): QUICK's own CUDA bridge and kernels
     (src/cuda/gpu.cu, gpu_get2e.cu, gpu_getxc.cu) compiled as host code and
     driven through QUICK's own ``gpu_*_`` entry points, in the call order of
-    src/main.f90:81-177 and src/hfoperator.f90:76-104.
+    src/main.f90:81-177 and src/hfoperator.f90:76-104;
+  * ``gpu/libquickref.so`` (build_ref.py --gpu): the same QUICK sources built
+    unchanged by nvcc for sm_100a and driven the same way on a GPU -- QUICK's
+    own GPU path, the GPU-side baseline and a second checker.
 """
 import contextlib
 import ctypes as C
@@ -241,8 +244,11 @@ def grad1e(basis, mol, dense, wdense):
 def _ref_dir(spdf):
     """spdf: False (default build), True (CUDA_SPDF: QUICK's f-shell kernels)
     or "boys" (CUDA_SPDF with QUICK's FmT replaced by an accurate Boys
-    function, build_ref.py --accurate-boys)."""
-    return {False: LIBDIR, True: os.path.join(LIBDIR, "spdf"), "boys": os.path.join(LIBDIR, "spdf_boys")}[spdf]
+    function, build_ref.py --accurate-boys), or "gpu" (QUICK's sources built
+    unchanged by nvcc for sm_100a, build_ref.py --gpu: QUICK's own GPU path,
+    which needs a GPU; it has no quartet counter and no host threads)."""
+    return {False: LIBDIR, True: os.path.join(LIBDIR, "spdf"), "boys": os.path.join(LIBDIR, "spdf_boys"),
+            "gpu": os.path.join(LIBDIR, "gpu")}[spdf]
 
 
 def ref_available(spdf=False):
@@ -278,6 +284,55 @@ def _quiet():
         os.close(devnull)
 
 
+@contextlib.contextmanager
+def _capture(lines):
+    """Like _quiet, but the text QUICK's bridge prints is kept: appended to
+    the list ``lines`` when the block ends."""
+    import sys
+    import tempfile
+    sys.stdout.flush()
+    saved = os.dup(1)
+    with tempfile.TemporaryFile(mode="w+b") as tmp:
+        os.dup2(tmp.fileno(), 1)
+        try:
+            yield
+        finally:
+            C.CDLL(None).fflush(None)
+            os.dup2(saved, 1)
+            os.close(saved)
+            tmp.seek(0)
+            lines.extend(tmp.read().decode("latin-1").splitlines())
+
+
+def ref_get2e_gpu_timed(O, dense, cutMatrix, integral_cutoff, prim_limit, method=0):
+    """One Fock build through QUICK's GPU build (ref_lib("gpu")), the
+    sequence of ref_get2e.  Returns (O, wall seconds of the four bridge
+    calls, QUICK's own event time of its get2e_kernel launch in ms).  QUICK's
+    stock configuration defines DEBUG, under which QUICK_SAFE_CALL brackets
+    the launch with CUDA events and prints "this cycle:<ms> ms"
+    (src/cuda/gpu_common.h:90-146); that line is read back here."""
+    import time
+    r = ref_lib("gpu")
+    n = O.shape[0]
+    o = np.array(O, order="F", dtype=np.float64)
+    co = np.zeros((n, n), order="F")
+    vec = np.zeros((n, n), order="F")
+    d = np.array(dense, order="F", dtype=np.float64)
+    cm = np.array(cutMatrix, order="F", dtype=np.float64)
+    lines = []
+    with _capture(lines):
+        t0 = time.perf_counter()
+        r.gpu_upload_method_(_i(method))
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(vec), _ptr(d))
+        r.gpu_upload_cutoff_(_ptr(cm), _d(integral_cutoff), _d(prim_limit), None)
+        r.gpu_get2e_(_ptr(o))
+        wall = time.perf_counter() - t0
+    kern = [float(x.split("this cycle:")[1].split("ms")[0]) for x in lines if "this cycle:" in x]
+    if len(kern) != 1:
+        raise RuntimeError("expected one timed QUICK launch, got %r" % (kern,))
+    return o, wall, kern[0]
+
+
 def _i(v):
     return C.byref(C.c_int(int(v)))
 
@@ -289,12 +344,13 @@ def _d(v):
 _ref_nshell = 0
 
 
-def ref_upload_molecule(mol, basis, YCutoff, cutPrim, threads=None, spdf=False):
-    """QUICK's start-up upload sequence (src/main.f90:84-177)."""
+def ref_upload_molecule(mol, basis, YCutoff, cutPrim, threads=None, spdf=False, device=0):
+    """QUICK's start-up upload sequence (src/main.f90:84-177); device: the
+    CUDA device of the "gpu" build (gpu_set_device_, src/cuda/gpu.cu:18)."""
     global _ref_nshell
     _ref_nshell = basis.nshell
     r = ref_lib(spdf)
-    if threads:
+    if threads and spdf != "gpu":
         r.qref_set_threads(int(threads))
     b = basis
     keep = []
@@ -306,6 +362,8 @@ def ref_upload_molecule(mol, basis, YCutoff, cutPrim, threads=None, spdf=False):
 
     with _quiet():
         r.qref_reset()
+        if spdf == "gpu":
+            r.gpu_set_device_(_i(device))
         r.gpu_init_()
         r.gpu_setup_(_i(mol.natom), _i(b.nbasis), _i(mol.n_electrons), _i(mol.mult), _i(mol.charge),
                      _i(len(set(mol.symbols))))
@@ -356,7 +414,8 @@ def ref_get2e(O, dense, cutMatrix, integral_cutoff, prim_limit, method=0, spdf=F
     (src/hfoperator.f90:76-98).  Returns the new O; ref_quartet_counts()
     then gives its shell-quartet counts."""
     r = ref_lib(spdf)
-    r.qref_reset_counts()
+    if spdf != "gpu":
+        r.qref_reset_counts()
     n = O.shape[0]
     o = np.array(O, order="F", dtype=np.float64)
     co = np.zeros((n, n), order="F")

@@ -6,6 +6,13 @@ shim in ``oracle/ref_shim`` supplies a host stand-in for the CUDA runtime and
 the launch geometry.  Build outputs go to ``oracle/_ref`` only.
 
     python oracle/build_ref.py [--quick-root DIR] [--spdf] [--accurate-boys]
+    python oracle/build_ref.py [--quick-root DIR] --gpu
+
+--gpu compiles the same QUICK sources unchanged with nvcc for sm_100a into
+``oracle/_ref/gpu/libquickref.so`` (QUICK's spd build, its own flags -O3
+-use_fast_math from makein/make.in.gnu.cuda:52, plus a register cap so that
+its 512-thread blocks can launch): QUICK's GPU path, timed on the B200
+beside this package as a baseline.
 
 The QUICK tree is DIR, else the environment variable QUICK_ROOT, else
 /root/reference (quick_root()).
@@ -101,10 +108,57 @@ def build(quick_root, spdf=False, accurate_boys=False, jobs=8, opt="-O2"):
     return lib
 
 
+def build_gpu(quick_root, jobs=4):
+    """QUICK's bridge and kernels (src/cuda/gpu.cu, gpu_type.cu, gpu_get2e.cu,
+    gpu_getxc.cu; the units of src/cuda/Makefile:16-19) built by nvcc for
+    sm_100a, unchanged, into oracle/_ref/gpu/libquickref.so."""
+    out = os.path.join(HERE, "_ref", "gpu")
+    src = os.path.join(quick_root, "src", "cuda")
+    if not os.path.isdir(src):
+        raise FileNotFoundError("QUICK sources not found at %s" % src)
+    os.makedirs(os.path.join(out, "inc"), exist_ok=True)
+    # QUICK's own CUDA configuration, as its Makefile copies it to src/config.h
+    # (Makefile:181 copies config/config.cuda.h; it defines DEBUG, which QUICK_SAFE_CALL's
+    # event timer around every kernel launch needs, gpu_common.h:90-134)
+    with open(os.path.join(quick_root, "src", "config", "config.cuda.h")) as fh:
+        cfg = fh.read()
+    with open(os.path.join(out, "config.h"), "w") as fh:
+        fh.write(cfg)
+    nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    # -maxrregcount=128: QUICK launches its kernels with 512 threads per block
+    # (gpu_common.h:180-190, gpu_init_) and declares no launch bounds; left
+    # alone, ptxas gives get2e_kernel 255 registers on sm_100a and such a
+    # block cannot launch (65,536 registers per SM).  QUICK's own flag line
+    # for its first GPUs capped registers the same way (-maxrregcount=63,
+    # makein/make.in.gnu.cuda:50).
+    flags = ["-O3", "-use_fast_math", "-m64", "-maxrregcount=128", "-gencode", "arch=compute_100a,code=sm_100a",
+             "-w", "-Xptxas", "-v",
+             "-Xcompiler", "-fPIC", "-I" + os.path.join(out, "inc"), "-I" + out, "-I" + src]
+    units = [os.path.join(SHIM, "gpu_bridge.cu")] + [os.path.join(src, u) for u in
+                                                    ("gpu_type.cu", "gpu_get2e.cu", "gpu_getxc.cu")]
+
+    def cc(u):
+        o = os.path.join(out, os.path.basename(u).replace(".cu", ".o"))
+        with open(o.replace(".o", ".ptxas.txt"), "w") as log:   # resource usage per kernel
+            subprocess.run([nvcc] + flags + ["-c", u, "-o", o], check=True, stderr=log)
+        return o
+
+    with ThreadPoolExecutor(jobs) as ex:
+        objs = list(ex.map(cc, units))
+    lib = os.path.join(out, "libquickref.so")
+    subprocess.run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-Xlinker", "-Bsymbolic",
+                    "-o", lib] + objs, check=True)
+    return lib
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick-root", default=None)
     ap.add_argument("--spdf", action="store_true")
     ap.add_argument("--accurate-boys", action="store_true")
+    ap.add_argument("--gpu", action="store_true")
     a = ap.parse_args()
+    if a.gpu:
+        print(build_gpu(a.quick_root or quick_root()))
+        sys.exit(0)
     print(build(a.quick_root or quick_root(), a.spdf or a.accurate_boys, a.accurate_boys))
