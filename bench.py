@@ -214,13 +214,42 @@ def gpu_reference(steps, warmup, device=0):
         walls.append(wall)
         kerns.append(kern)
     z = np.load(os.path.join(ROOT, "tests", "golden", "config1_water32_631gss.npz"))
-    nq = int(z["unique_quartets"])
-    par = quick_parity(np.ascontiguousarray(O.T), nq, b.nbasis) or {}
+    full = WORKLOAD["grid"] == (4, 4, 2)
+    nq = int(z["unique_quartets"]) if full else None     # QUICK's own count of this workload
+    par = (quick_parity(np.ascontiguousarray(O.T), nq, b.nbasis) or {}) if full else {}
     wall, kern = float(np.mean(walls)), float(np.mean(kerns))
+    # QUICK's two-electron gradient (src/gradient.f90:279-286) on the same
+    # density: one warm-up call, two timed
+    gw, gk = [], []
+    for i in range(3):
+        g, w, k = oracle.ref_grad_gpu_timed(3 * m.natom, D, cm, cut, plim)
+        if i:
+            gw.append(w)
+            gk.append(k)
+    # QUICK's B3LYP XC quadrature on its SG1 grid (gpu_getxc_), the density of the xc line
+    from quick_b200.basis import sigrad2
+    rng = np.random.default_rng(WORKLOAD["seed"])
+    Cx = rng.standard_normal((b.nbasis, m.n_electrons // 2)) * 0.05
+    Dx = np.asfortranarray(2.0 * Cx @ Cx.T)
+    xw = []
+    for i in range(3):
+        _, exc, nel, w = oracle.ref_getxc_gpu_timed(Dx, sigrad2(b), method=1)
+        if i:
+            xw.append(w)
+    if not full:
+        return {"workload": WORKLOAD["name"], "ms_per_step": wall * 1e3, "kernel_ms": kern,
+                "gradient_kernel_ms": float(np.mean(gk)), "xc_ms_per_call": float(np.mean(xw)) * 1e3}
     return {"value": nq / wall, "unit": "quartets/s", "ms_per_step": wall * 1e3,
             "kernel_ms": kern, "kernel_quartets_per_s": nq / (kern * 1e-3), "quartets_per_step": nq,
             "steps": steps, "warmup": warmup,
             "max_abs_dF_vs_quick_host_sampled": par.get("max_abs_dF_sampled"),
+            "gradient": {"ms_per_call": float(np.mean(gw)) * 1e3, "kernel_ms": float(np.mean(gk)),
+                         "max_abs_dg_vs_quick_host": float(np.abs(g - z["grad"]).max()), "calls": len(gw),
+                         "what": "gpu_upload_calculated_/gpu_upload_cutoff_/gpu_upload_grad_/gpu_grad_ wall time; "
+                                 "kernel_ms: QUICK's event timers around its gradient launches, summed"},
+            "xc": {"ms_per_call": float(np.mean(xw)) * 1e3, "exc": exc, "electrons": nel, "calls": len(xw),
+                   "what": "B3LYP, QUICK's SG1 grid: gpu_upload_method_/gpu_upload_calculated_/gpu_getxc_ wall "
+                           "time (its kernel launch has no event timer)"},
             "what": "QUICK's own CUDA (gpu.cu bridge + get2e_kernel, spd build, -O3 -use_fast_math, QUICK's "
                     "config.cuda.h) built unchanged for sm_100a and run on this GPU on %s; value: the whole "
                     "gpu_upload_calculated_/gpu_upload_cutoff_/gpu_get2e_ sequence from host buffers (its e2e), "
@@ -801,7 +830,14 @@ def main():
                          "scf: the SCF+gradient line only; batch: the many-small-molecules line only; "
                          "quick-gpu (with --impl reference): QUICK's own GPU path on the Fock-build workload")
     ap.add_argument("--no-quick-gpu", action="store_true", help="skip the reference_gpu object")
+    ap.add_argument("--grid", default=None,
+                    help="water-cluster grid of the workload, e.g. 2,2,2 for (H2O)8 (default 4,4,2: (H2O)32); "
+                         "smaller cases are for profiling only")
     args = ap.parse_args()
+    if args.grid:
+        g = tuple(int(x) for x in args.grid.split(","))
+        WORKLOAD["grid"] = g
+        WORKLOAD["name"] = "(H2O)%d 6-31G** RHF Fock build" % (g[0] * g[1] * g[2])
     threads = os.cpu_count() or 1
     if args.impl == "reference" and args.part == "quick-gpu":
         # QUICK's own GPU path only (run by the default line in a process of its own)
@@ -858,6 +894,13 @@ def main():
             rg = out["reference_gpu"]
             rg["e2e_speedup_of_this_build"] = out["e2e"]["value"] / rg["value"]
             rg["kernel_speedup_of_this_build"] = out["value"] / rg["kernel_quartets_per_s"]
+            gr = out.get("gradient", {})
+            if "e2e_ms_per_call" in gr:
+                rg["gradient"]["e2e_speedup_of_this_build"] = rg["gradient"]["ms_per_call"] / gr["e2e_ms_per_call"]
+                rg["gradient"]["kernel_speedup_of_this_build"] = rg["gradient"]["kernel_ms"] / gr["kernel_ms"]
+            if "xc" in out and "e2e" in out["xc"]:
+                rg["xc"]["e2e_speedup_of_this_build"] = rg["xc"]["ms_per_call"] / out["xc"]["e2e"]["ms_per_call"]
+                rg["xc"]["abs_dExc_vs_this_build"] = abs(rg["xc"]["exc"] - out["xc"]["exc"])
     if rank == 0:
         print(json.dumps(out))
     if ws > 1:

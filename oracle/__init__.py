@@ -333,6 +333,56 @@ def ref_get2e_gpu_timed(O, dense, cutMatrix, integral_cutoff, prim_limit, method
     return o, wall, kern[0]
 
 
+def ref_grad_gpu_timed(ngrad, dense, cutMatrix, integral_cutoff, prim_limit, grad_cutoff=1e-7):
+    """QUICK's two-electron gradient through its GPU build, the sequence of
+    ref_grad.  Returns (gradient, wall seconds of the four bridge calls, the
+    sum of QUICK's own event times of its gradient launches in ms:
+    getGrad_kernel and, with d shells, getGrad_kernel_spdf and _spdf2,
+    src/cuda/gpu_get2e.cu:336-350)."""
+    import time
+    r = ref_lib("gpu")
+    n = dense.shape[0]
+    o = np.zeros((n, n), order="F")
+    co = np.zeros((n, n), order="F")
+    d = np.array(dense, order="F", dtype=np.float64)
+    cm = np.array(cutMatrix, order="F", dtype=np.float64)
+    g = np.zeros(ngrad)
+    lines = []
+    with _capture(lines):
+        t0 = time.perf_counter()
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(co), _ptr(d))
+        r.gpu_upload_cutoff_(_ptr(cm), _d(integral_cutoff), _d(prim_limit), None)
+        r.gpu_upload_grad_(_ptr(g), _d(grad_cutoff))
+        r.gpu_grad_(_ptr(g))
+        wall = time.perf_counter() - t0
+    kern = [float(x.split("this cycle:")[1].split("ms")[0]) for x in lines if "this cycle:" in x]
+    return g, wall, float(sum(kern))
+
+
+def ref_getxc_gpu_timed(dense, sigrad2, method=1, isg=1):
+    """One XC quadrature through QUICK's GPU build, the sequence of
+    ref_getxc.  Returns (O', Eelxc, aelec, wall seconds of the three bridge
+    calls; gpu_getxc_ returns after its download)."""
+    import time
+    r = ref_lib("gpu")
+    n = dense.shape[0]
+    o = np.zeros((n, n), order="F")
+    co = np.zeros((n, n), order="F")
+    vec = np.zeros((n, n), order="F")
+    d = np.array(dense, order="F", dtype=np.float64)
+    sg = np.ascontiguousarray(sigrad2, dtype=np.float64)
+    e, a, b = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0)
+    cm = np.zeros((max(_ref_nshell, 1),) * 2, order="F")
+    with _quiet():
+        r.gpu_upload_cutoff_(_ptr(cm), _d(1e-10), _d(1e-20), None)
+        t0 = time.perf_counter()
+        r.gpu_upload_method_(_i(method))
+        r.gpu_upload_calculated_(_ptr(o), _ptr(co), _ptr(vec), _ptr(d))
+        r.gpu_getxc_(_i(isg), _ptr(sg), C.byref(e), C.byref(a), C.byref(b), _ptr(o))
+        wall = time.perf_counter() - t0
+    return o, e.value, a.value, wall
+
+
 def _i(v):
     return C.byref(C.c_int(int(v)))
 
