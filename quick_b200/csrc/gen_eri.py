@@ -199,6 +199,16 @@ def group_sizes(la, lb, lc, ld):
     return [1]
 
 
+# One lane per quartet walks its primitive quartets ket-outer, bra-inner
+# for the classes up to this total angular momentum (gradient: of the
+# underlying class): the list is grouped by bra pair, so the inner loop's
+# primitive-pair loads are the same address across the warp (one broadcast
+# wavefront) where the bra-inner order made each lane load its own ket's
+# records once per bra primitive.  The heavier classes, bound by their
+# recurrences and register spills, keep bra-outer.
+KET_OUTER_MAX_L = 4
+
+
 SB_FLAG = 256     # kSbFlag of eri_common.cuh
 SB_MAX_L = 2      # kSbMaxL of eri_common.cuh
 
@@ -295,14 +305,25 @@ def gen_class(la, lb, lc, ld, prec="double", list32_launcher=False):
         b("c_%s_%s += %s;" % (nm(e), nm(f), v))
     # G == 1: one lane walks the bra x ket primitive double loop
     w("    if constexpr (G == 1) {")
-    w("    for (int ib = 0; ib < q.nbra; ib++) {")
-    for ln in bra_load:
-        w("        " + ln)
-    w("        for (int ik = 0; ik < q.nket; ik++) {")
-    for ln in body:
-        w("            " + ln)
-    w("        }")
-    w("    }")
+    nkl = 1 if f32 else 2          # the ket record loads that open the body
+    if L <= KET_OUTER_MAX_L:
+        w("    for (int ik = 0; ik < q.nket; ik++) {")
+        for ln in body[:nkl]:
+            w("        " + ln)
+        w("        for (int ib = 0; ib < q.nbra; ib++) {")
+        for ln in bra_load + body[nkl:]:
+            w("            " + ln)
+        w("        }")
+        w("    }")
+    else:
+        w("    for (int ib = 0; ib < q.nbra; ib++) {")
+        for ln in bra_load:
+            w("        " + ln)
+        w("        for (int ik = 0; ik < q.nket; ik++) {")
+        for ln in body:
+            w("            " + ln)
+        w("        }")
+        w("    }")
     # G > 1: the G lanes of a group stride over the flattened primitive
     # quartets (ket fastest); a lane keeps its bra record until its bra
     # primitive changes
@@ -621,14 +642,28 @@ def gen_grad_class(la, lb, lc, ld, part=0, prec="double"):
     # record read once); GS lanes: they stride over the flattened primitive
     # quartets
     w("    if constexpr (GS == 1) {")
-    w("    for (int ib = 0; ib < q.nbra; ib++) {")
-    for ln in bra:
-        w("        " + ln)
-    w("        for (int ik = 0; ik < q.nket; ik++) {")
-    for ln in ket + inner:
-        w("            " + ln)
-    w("        }")
-    w("    }")
+    if L - 1 <= KET_OUTER_MAX_L:
+        # ket-outer (KET_OUTER_MAX_L): the screen needs both records, so it
+        # moves into the inner loop
+        kload = [ln for ln in ket if "prim_survives" not in ln]
+        screen = [ln for ln in ket if "prim_survives" in ln]
+        w("    for (int ik = 0; ik < q.nket; ik++) {")
+        for ln in kload:
+            w("        " + ln)
+        w("        for (int ib = 0; ib < q.nbra; ib++) {")
+        for ln in bra + screen + inner:
+            w("            " + ln)
+        w("        }")
+        w("    }")
+    else:
+        w("    for (int ib = 0; ib < q.nbra; ib++) {")
+        for ln in bra:
+            w("        " + ln)
+        w("        for (int ik = 0; ik < q.nket; ik++) {")
+        for ln in ket + inner:
+            w("            " + ln)
+        w("        }")
+        w("    }")
     w("    } else {")
     w("    const int nk = q.nket, npq = q.nbra * nk;")
     w("    for (int t = sub; t < npq; t += GS) {")
