@@ -333,7 +333,10 @@ def run_ours(args, ws, rank, local):
     lib.qb_count_prim_quartets(capi._ptr(npq), 128)
     capi.check()
     k = ncls.value
-    alg_flops = flops.fock_flops(cl[:4 * k].reshape(k, 4), cq[:k], npq[:k], exchange=True)
+    # per class the smaller of the generator-graph and the definition count
+    alg_flops = flops.fock_flops(cl[:4 * k].reshape(k, 4), cq[:k], npq[:k], exchange=True, table="min")
+    alg_flops_tables = {t: flops.fock_flops(cl[:4 * k].reshape(k, 4), cq[:k], npq[:k], exchange=True, table=t)
+                        for t in ("generator", "definition")}
     peak64 = capi.C.c_double(0)
     lib.qb_fma_peak(1, capi.C.byref(peak64))
 
@@ -512,7 +515,12 @@ def run_ours(args, ws, rank, local):
                                        "profiles/fock_class_kernels_water32_631gss.md",
                      "kernel": "fock_class_kernel<LA,LB,LC,LD> (all classes of one build)",
                      "peak_source": "measured: FP64 FMA-chain probe run in this process (qb_fma_peak)",
-                     "flops_per_step": alg_flops, "kernel_ms": mean_eri,
+                     "flops_per_step": alg_flops,
+                     "flops_per_step_by_table": alg_flops_tables,
+                     "flops_note": "per class the smaller of two counts, both from the recurrences and not from "
+                                   "the kernels: the generator's dependency graph and the recurrence definitions "
+                                   "(quick_b200/flops.py definition_class)",
+                     "kernel_ms": mean_eri,
                      "screen_ms": float(np.mean(scr_ms))},
         "gpu_launches": int(launches),
         "cuda_graph": {"ms_per_step": graph_ms, "value": quartets * ws / (graph_ms * 1e-3), "unit": "quartets/s",
