@@ -214,7 +214,7 @@ def gpu_reference(steps, warmup, device=0):
         walls.append(wall)
         kerns.append(kern)
     z = np.load(os.path.join(ROOT, "tests", "golden", "config1_water32_631gss.npz"))
-    full = WORKLOAD["grid"] == (4, 4, 2)
+    full = WORKLOAD["grid"] == (4, 4, 2) and WORKLOAD["basis"] == "6-31G**"
     nq = int(z["unique_quartets"]) if full else None     # QUICK's own count of this workload
     par = (quick_parity(np.ascontiguousarray(O.T), nq, b.nbasis) or {}) if full else {}
     wall, kern = float(np.mean(walls)), float(np.mean(kerns))
@@ -263,7 +263,7 @@ def quick_parity(G, quartets, n):
     kernel compiled for the host on this workload and density).  G is
     row-major here; it is symmetric."""
     path = os.path.join(ROOT, "tests", "golden", "config1_water32_631gss.npz")
-    if not os.path.exists(path) or WORKLOAD["grid"] != (4, 4, 2):
+    if not os.path.exists(path) or WORKLOAD["grid"] != (4, 4, 2) or WORKLOAD["basis"] != "6-31G**":
         return None
     z = np.load(path)
     if int(z["nbasis"]) != n:
@@ -841,11 +841,14 @@ def main():
     ap.add_argument("--grid", default=None,
                     help="water-cluster grid of the workload, e.g. 2,2,2 for (H2O)8 (default 4,4,2: (H2O)32); "
                          "smaller cases are for profiling only")
+    ap.add_argument("--basis", default=None,
+                    help="basis set of the workload (default 6-31G**); others, e.g. cc-pVTZ, are for profiling only")
     args = ap.parse_args()
-    if args.grid:
-        g = tuple(int(x) for x in args.grid.split(","))
+    if args.grid or args.basis:
+        g = tuple(int(x) for x in args.grid.split(",")) if args.grid else WORKLOAD["grid"]
         WORKLOAD["grid"] = g
-        WORKLOAD["name"] = "(H2O)%d 6-31G** RHF Fock build" % (g[0] * g[1] * g[2])
+        WORKLOAD["basis"] = args.basis or WORKLOAD["basis"]
+        WORKLOAD["name"] = "(H2O)%d %s RHF Fock build" % (g[0] * g[1] * g[2], WORKLOAD["basis"])
     threads = os.cpu_count() or 1
     if args.impl == "reference" and args.part == "quick-gpu":
         # QUICK's own GPU path only (run by the default line in a process of its own)
