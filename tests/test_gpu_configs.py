@@ -4,8 +4,7 @@
 Fock-build benchmark), seeded clusters, the bench's model density: the GPU's
 Fock matrix, two-electron gradient and shell-quartet count against QUICK's
 get2e and gradient kernels compiled for the host (fixtures written by
-tests/golden/make_config_golden.py from oracle/_ref/libquickref.so); and the
-f-shell workload's basis (cc-pVTZ) on (H2O)8 against the C oracle.
+tests/golden/make_config_golden.py from oracle/_ref/libquickref.so).
 
 Tolerances: Fock elements 1e-8 (for the 800-function matrix on 20000 sampled
 elements and the diagonal; the projections G R within the bound that an
@@ -71,25 +70,3 @@ def test_config_matches_quick(session, oracle_lib, k):
     g = session.grad(np.zeros(3 * m.natom), D, cm, 1e-10, 1e-20)
     assert np.abs(g - z["grad"]).max() < TOL_G
 
-
-def test_fshell_workload_matches_oracle(session, oracle_lib):
-    """The f-shell workload's basis, cc-pVTZ, on (H2O)8 (520 functions, the
-    largest cluster the C oracle builds in about a minute; fixture written by
-    make_config_golden.py --only 4): the GPU's Fock matrix against the
-    oracle's on 20000 sampled elements, the diagonal and 8 projections
-    (tolerances as for config 1)."""
-    z = np.load(os.path.join(GOLDEN, "config4s_water8_ccpvtz.npz"))
-    m = water_cluster((2, 2, 2), seed=0)
-    b = build_basis(m.symbols, "cc-pVTZ")
-    n = b.nbasis
-    assert n == int(z["nbasis"])
-    Y, cp = oracle_lib.schwarz(b, m.xyz_bohr)
-    session.upload_molecule(m, b, Y, cp)
-    D = model_density(m, b, seed=0)
-    cm = shell_cut_matrix(b, D)
-    G = session.get2e(np.zeros((n, n), order="F"), D, cm, 1e-10, 1e-20, method=0)
-    R, idx = _probes(n)
-    assert np.abs(G[idx[:, 0], idx[:, 1]] - z["sample"]).max() < TOL_F
-    assert np.abs(np.diag(G) - z["diag"]).max() < TOL_F
-    bound = TOL_F * np.abs(R).sum(axis=0)
-    assert np.all(np.abs(G @ R - z["GR"]).max(axis=0) < bound)
