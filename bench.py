@@ -47,7 +47,7 @@ WORKLOAD = dict(name="(H2O)32 6-31G** RHF Fock build", grid=(4, 4, 2), basis="6-
 # mixed-precision split: shell quartets whose Y_ab Y_cd DNMax bound is below this run in FP32
 # DRAM bytes (read + write) of the class kernels of one FP64 build of the
 # workload, from one ncu capture (cold caches): the roofline's traffic
-FOCK_BUILD_DRAM_BYTES = 27.1e9
+FOCK_BUILD_DRAM_BYTES = 24.8e9
 MIXED_CUT = 1e-3
 
 
